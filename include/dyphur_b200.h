@@ -1,0 +1,236 @@
+/* dyphur_b200.h — C ABI of the B200-native dyphur frame step.
+ *
+ * The frame step is integrate -> Morton/LBVH broadphase -> (a, b) pair order
+ * -> SAT narrowphase -> XPBD contact solve -> FNV-1a state hash, as the
+ * reference drives it in examples/stress_test_blocks/main.cpp:264-279.
+ *
+ * Conventions
+ *   - Every pointer inside a view struct is a DEVICE pointer (cudaMalloc or
+ *     torch storage) unless the name says host. Counts that the GPU produces
+ *     stay on the device (uint32_t* d_*).
+ *   - Every entry point returns dyph_status (0 = OK) and never throws.
+ *   - Work is queued on the given stream (a cudaStream_t; NULL = legacy
+ *     default stream). Nothing synchronises the host unless its name says
+ *     "download".
+ *   - The view structs have the field order and meaning of the reference's
+ *     kernel views, so a BodyView / ShapeView / ContactView can be passed by
+ *     reinterpret_cast.
+ */
+#ifndef DYPHUR_B200_H
+#define DYPHUR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dyph_stream;
+
+typedef enum dyph_status {
+    DYPH_OK = 0,
+    DYPH_ERR_INVALID = 1,          /* bad argument (null pointer, size, mode) */
+    DYPH_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    DYPH_ERR_PAIR_OVERFLOW = 3,    /* more candidate pairs than capacity (sorted prefix kept) */
+    DYPH_ERR_CONTACT_OVERFLOW = 4, /* more contacts than capacity (ordered prefix kept) */
+    DYPH_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
+    DYPH_ERR_NO_DEVICE = 6,        /* no CUDA device / not an sm_100 device */
+    DYPH_ERR_NOMEM = 7,            /* device allocation failed */
+    DYPH_ERR_NOT_FINITE = 8        /* NaN / Inf found in body state */
+} dyph_status;
+
+/* Mirrors BodyView (core/include/core/body.hpp:30-46). */
+typedef struct dyph_bodies {
+    float *pos_x, *pos_y, *pos_z;
+    float *rot_w, *rot_x, *rot_y, *rot_z;
+    float *vel_x, *vel_y, *vel_z;
+    float *ang_x, *ang_y, *ang_z;
+    float* inv_mass;
+    float *iI_xx, *iI_yy, *iI_zz;
+    float *iI_xy, *iI_xz, *iI_yz;
+    uint32_t* shape;
+    uint32_t* flags;
+    uint32_t n;
+} dyph_bodies;
+
+/* Mirrors ShapeView (core/include/core/shapes.hpp:22-29). type: 0 box, 1 sphere. */
+typedef struct dyph_shapes {
+    const uint32_t* type;
+    const float* half_x;
+    const float* half_y;
+    const float* half_z;
+    const uint32_t* ext_id;
+    uint32_t n;
+} dyph_shapes;
+
+/* Mirrors ContactView (core/include/core/contact.hpp:8-20). Normal points from B toward A. */
+typedef struct dyph_contacts {
+    uint32_t* body_a;
+    uint32_t* body_b;
+    float *pos_x, *pos_y, *pos_z;
+    float *norm_x, *norm_y, *norm_z;
+    float* depth;
+    uint32_t* n; /* device: live contact count */
+    uint32_t capacity;
+} dyph_contacts;
+
+/* Mirrors AABB (core/include/core/aabb.hpp:7-9). */
+typedef struct dyph_aabb {
+    float min_x, min_y, min_z, max_x, max_y, max_z;
+} dyph_aabb;
+
+/* Mirrors ContactPair (core/include/core/broadphase.hpp:12-14): a < b. */
+typedef struct dyph_pair {
+    uint32_t a, b;
+} dyph_pair;
+
+/* Mirrors NodeBox (core/include/core/broadphase.hpp:21-25): raw fp16 bits. */
+typedef struct dyph_node_box {
+    uint16_t mn_x, mn_y, mn_z, mx_x, mx_y, mx_z, pad0, pad1;
+} dyph_node_box;
+
+/* Mirrors BvhView (core/include/core/broadphase.hpp:30-38), plus the sorted
+ * 64-bit Morton keys (morton30 << 32 | body) the tree was built from. */
+typedef struct dyph_bvh_view {
+    const int32_t* left;
+    const int32_t* right;
+    const int32_t* parent;
+    const int32_t* root;
+    const uint32_t* sorted_idx;
+    const dyph_node_box* aabb;
+    const uint64_t* sorted_keys;
+    uint32_t n;
+} dyph_bvh_view;
+
+/* Mirrors IntegratorParams (core/include/core/integrator.hpp:7-11). */
+typedef struct dyph_integrator_params {
+    float gravity[3];
+    float dt;
+    int32_t n_substeps;
+} dyph_integrator_params;
+
+/* Solver order modes. */
+typedef enum dyph_solver_mode {
+    /* XpbdSolver default (core/src/xpbd_solver.cpp:620-733): sequential order
+     * when n_con <= 256, else Jones–Plassmann colours processed in ascending
+     * colour order. Bit-identical to the reference. */
+    DYPH_SOLVER_REFERENCE = 0,
+    /* XpbdSolver::set_force_serial(true) (core/include/core/xpbd_solver.hpp:48):
+     * sorted contact order, run as a level schedule (bit-identical). */
+    DYPH_SOLVER_SEQUENTIAL = 1
+} dyph_solver_mode;
+
+/* ── library ──────────────────────────────────────────────────────────────── */
+
+const char* dyph_status_string(int status);
+/* Returns DYPH_OK when a CUDA device of compute capability 10.x is current. */
+dyph_status dyph_device_check(void);
+/* Sticky device-side error word of the library (DYPH_ERR_TIMEOUT etc.), read
+ * and cleared. Blocks on the stream. */
+dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code);
+
+/* ── integrate — replaces integrate(Stream&, BodyView, const IntegratorParams&)
+ *    (core/include/core/integrator.hpp:25, core/src/integrator.cpp:7-71) ──── */
+dyph_status dyph_integrate(const dyph_bodies* bodies, const dyph_integrator_params* params, dyph_stream s);
+
+/* ── sort — replaces sort_by_key<K,V> / sort<K>
+ *    (compute/include/compute/sort.hpp:29-137). Ascending, stable LSD radix
+ *    sort; unlike the reference n need not be a power of two. ──────────── */
+size_t dyph_sort_workspace_bytes(size_t n);
+dyph_status dyph_sort_by_key_u64_u32(uint64_t* keys, uint32_t* values, size_t n, void* workspace,
+                                     size_t workspace_bytes, dyph_stream s);
+dyph_status dyph_sort_u64(uint64_t* keys, size_t n, void* workspace, size_t workspace_bytes, dyph_stream s);
+dyph_status dyph_sort_by_key_u32_u32(uint32_t* keys, uint32_t* values, size_t n, int key_bits, void* workspace,
+                                     size_t workspace_bytes, dyph_stream s);
+
+/* ── broadphase — replaces class Broadphase
+ *    (core/include/core/broadphase.hpp:50-111, core/src/broadphase.cpp:82-377).
+ *    Pairs come out already in ascending (a << 32 | b) order, so
+ *    dyph_broadphase_sort_pairs is a no-op kept for the call sequence. ───── */
+typedef struct dyph_broadphase dyph_broadphase;
+dyph_status dyph_broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broadphase** out);
+void dyph_broadphase_destroy(dyph_broadphase* bp);
+dyph_status dyph_broadphase_build_and_query(dyph_broadphase* bp, const dyph_bodies* bodies,
+                                            const dyph_shapes* shapes, const dyph_aabb* scene_bounds,
+                                            dyph_stream s);
+dyph_status dyph_broadphase_sort_pairs(dyph_broadphase* bp, uint32_t n_pairs, dyph_stream s);
+/* Blocking: true candidate-pair count of the last build (may exceed max_pairs). */
+dyph_status dyph_broadphase_download_count(dyph_broadphase* bp, dyph_stream s, uint32_t* out);
+const dyph_pair* dyph_broadphase_pairs(const dyph_broadphase* bp);
+/* Device count of pairs stored (min(true count, max_pairs)). */
+const uint32_t* dyph_broadphase_count_ptr(const dyph_broadphase* bp);
+uint32_t dyph_broadphase_max_pairs(const dyph_broadphase* bp);
+dyph_status dyph_broadphase_bvh_view(const dyph_broadphase* bp, uint32_t n_active, dyph_bvh_view* out);
+
+/* ── narrowphase — replaces class Narrowphase
+ *    (core/include/core/narrowphase.hpp:26-73, core/src/narrowphase.cpp:1053-1144).
+ *    One thread per pair; contacts are compacted in pair order, which is the
+ *    order the reference's (pair_idx << 32 | sub) key sort restores. ────── */
+typedef struct dyph_narrowphase dyph_narrowphase;
+dyph_status dyph_narrowphase_create(uint32_t max_contacts, dyph_narrowphase** out);
+void dyph_narrowphase_destroy(dyph_narrowphase* np);
+/* Pair count read from device memory (no host sync). */
+dyph_status dyph_narrowphase_run(dyph_narrowphase* np, const dyph_pair* pairs, const uint32_t* d_n_pairs,
+                                 const dyph_bodies* bodies, const dyph_shapes* shapes, dyph_stream s);
+/* Pair count given on the host. */
+dyph_status dyph_narrowphase_run_host_count(dyph_narrowphase* np, const dyph_pair* pairs, uint32_t n_pairs,
+                                            const dyph_bodies* bodies, const dyph_shapes* shapes,
+                                            dyph_stream s);
+dyph_status dyph_narrowphase_contacts(dyph_narrowphase* np, dyph_contacts* out);
+dyph_status dyph_narrowphase_download_count(dyph_narrowphase* np, dyph_stream s, uint32_t* stored,
+                                            uint32_t* true_count);
+
+/* ── XPBD solver — replaces class XpbdSolver : IConstraintSolver
+ *    (core/include/core/solver.hpp:11-22, core/include/core/xpbd_solver.hpp:29-70,
+ *    core/src/xpbd_solver.cpp:593-733). Contacts only (JointView{} with n = 0). */
+typedef struct dyph_xpbd dyph_xpbd;
+dyph_status dyph_xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bodies, float friction,
+                             dyph_xpbd** out);
+void dyph_xpbd_destroy(dyph_xpbd* sv);
+dyph_status dyph_xpbd_set_mode(dyph_xpbd* sv, dyph_solver_mode mode);
+dyph_status dyph_xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_bodies* bodies, float dt,
+                            dyph_stream s);
+/* Colours of the last coloured solve (UINT32_MAX for the sequential path) and
+ * the colour count (0 = sequential). Blocking. */
+dyph_status dyph_xpbd_download_colors(dyph_xpbd* sv, dyph_stream s, uint32_t* host_colors, uint32_t cap,
+                                      uint32_t* n_colors);
+
+/* ── state hash — replaces the host FNV-1a-64 loop
+ *    (examples/stress_test_blocks/main.cpp:34-41, 301-311) ───────────────── */
+dyph_status dyph_fnv1a64_state(const dyph_bodies* bodies, uint64_t* d_hash, dyph_stream s);
+
+/* ── world: the whole frame step behind one handle. Replaces the open-coded
+ *    loop examples/stress_test_blocks/main.cpp:264-279 (integrate,
+ *    build_and_query, download_count, sort_pairs, Narrowphase::run,
+ *    XpbdSolver::solve) with a sync-free, CUDA-graph-replayed sequence. ─── */
+typedef struct dyph_world_desc {
+    dyph_bodies bodies;       /* device SoA, updated in place */
+    dyph_shapes shapes;       /* device SoA */
+    dyph_aabb scene_bounds;
+    dyph_integrator_params integrator;
+    uint32_t max_pairs;
+    uint32_t max_contacts;
+    int32_t n_iters;
+    float friction;
+    dyph_solver_mode mode;
+} dyph_world_desc;
+
+typedef struct dyph_world dyph_world;
+dyph_status dyph_world_create(const dyph_world_desc* desc, dyph_stream s, dyph_world** out);
+void dyph_world_destroy(dyph_world* w);
+/* Queue n_frames frame steps (graph-replayed after the first call). */
+dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_stream s);
+/* Blocking: peak pair / contact counts and the sticky status of the frames
+ * stepped so far (overflow or timeout). */
+dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* last_pairs,
+                                      uint32_t* last_contacts, uint32_t* peak_pairs, uint32_t* peak_contacts,
+                                      uint32_t* status);
+dyph_status dyph_world_broadphase(dyph_world* w, dyph_broadphase** out);
+dyph_status dyph_world_narrowphase(dyph_world* w, dyph_narrowphase** out);
+dyph_status dyph_world_solver(dyph_world* w, dyph_xpbd** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DYPHUR_B200_H */

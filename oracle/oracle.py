@@ -1,0 +1,192 @@
+"""ctypes access to the two CPU checkers (test infrastructure only).
+
+``Checker("oracle")`` loads the plain-C restatement (oracle/_build), and
+``Checker("ref")`` loads the reference's own sources built on the host SYCL
+shim (oracle/_ref). Both expose the interface of oracle/oracle_api.h.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libdyphur_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libdyphur_ref.so")
+
+STAGE_INTEGRATE, STAGE_BROADPHASE, STAGE_NARROWPHASE, STAGE_SOLVE = 1, 2, 3, 4
+SOLVER_REFERENCE, SOLVER_SERIAL = 0, 1
+
+
+class _Scene(ctypes.Structure):
+    _fields_ = [
+        ("n_bodies", ctypes.c_uint32), ("pos", ctypes.c_void_p), ("rot", ctypes.c_void_p),
+        ("vel", ctypes.c_void_p), ("ang", ctypes.c_void_p), ("mass", ctypes.c_void_p),
+        ("inertia", ctypes.c_void_p), ("shape", ctypes.c_void_p), ("flags", ctypes.c_void_p),
+        ("n_shapes", ctypes.c_uint32), ("shape_type", ctypes.c_void_p), ("shape_half", ctypes.c_void_p),
+        ("max_pairs", ctypes.c_uint32), ("max_contacts", ctypes.c_uint32), ("n_iters", ctypes.c_int32),
+        ("friction", ctypes.c_float), ("bounds", ctypes.c_float * 6), ("gravity", ctypes.c_float * 3),
+        ("dt", ctypes.c_float), ("n_substeps", ctypes.c_int32),
+    ]
+
+
+def build_oracle() -> str:
+    """Compile the C restatement if needed (gcc only; works on any host)."""
+    src = os.path.join(HERE, "dyphur_oracle.c")
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return ORACLE_SO
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+class Checker:
+    def __init__(self, which: str = "oracle"):
+        if which == "oracle":
+            self.lib = ctypes.CDLL(build_oracle())
+            p = "dyo_"
+        elif which == "ref":
+            if not ref_available():
+                raise FileNotFoundError(REF_SO)
+            self.lib = ctypes.CDLL(REF_SO)
+            p = "dyr_"
+        else:
+            raise ValueError(which)
+        self.which = which
+        L = self.lib
+        vp, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+        self.f_create = getattr(L, p + "create"); self.f_create.restype = vp
+        self.f_create.argtypes = [ctypes.POINTER(_Scene)]
+        self.f_destroy = getattr(L, p + "destroy"); self.f_destroy.argtypes = [vp]
+        self.f_stage = getattr(L, p + "run_stage"); self.f_stage.argtypes = [vp, i32, i32]
+        self.f_step = getattr(L, p + "step"); self.f_step.argtypes = [vp, i32, i32]
+        self.f_get_state = getattr(L, p + "get_state"); self.f_get_state.argtypes = [vp, vp]
+        self.f_set_state = getattr(L, p + "set_state"); self.f_set_state.argtypes = [vp, vp]
+        self.f_get_inv = getattr(L, p + "get_inv"); self.f_get_inv.argtypes = [vp, vp, vp]
+        self.f_hash = getattr(L, p + "hash"); self.f_hash.restype = ctypes.c_uint64
+        self.f_hash.argtypes = [vp]
+        self.f_pairs = getattr(L, p + "get_pairs"); self.f_pairs.restype = u32
+        self.f_pairs.argtypes = [vp, vp, u32]
+        self.f_contacts = getattr(L, p + "get_contacts"); self.f_contacts.restype = u32
+        self.f_contacts.argtypes = [vp, vp, vp, u32]
+        self.f_bvh = getattr(L, p + "get_bvh"); self.f_bvh.argtypes = [vp] * 7
+        self.f_colors = getattr(L, p + "get_colors"); self.f_colors.restype = u32
+        self.f_colors.argtypes = [vp, vp, u32]
+
+
+class World:
+    """One scene stepped by a CPU checker."""
+
+    def __init__(self, scene, which: str = "oracle", max_pairs: int | None = None,
+                 max_contacts: int | None = None):
+        self.ck = Checker(which)
+        s = scene
+        self.n = s.n_bodies
+        self._keep = [np.ascontiguousarray(a) for a in (
+            s.pos.astype(np.float32), s.rot.astype(np.float32), s.vel.astype(np.float32),
+            s.ang.astype(np.float32), s.mass.astype(np.float32), s.inertia.astype(np.float32),
+            s.shape.astype(np.uint32), s.flags.astype(np.uint32), s.shape_type.astype(np.uint32),
+            s.shape_half.astype(np.float32))]
+        d = _Scene()
+        d.n_bodies = self.n
+        for name, a in zip(("pos", "rot", "vel", "ang", "mass", "inertia", "shape", "flags"), self._keep[:8]):
+            setattr(d, name, a.ctypes.data)
+        d.n_shapes = int(s.shape_type.shape[0])
+        d.shape_type = self._keep[8].ctypes.data
+        d.shape_half = self._keep[9].ctypes.data
+        self.max_pairs = int(max_pairs or s.max_pairs)
+        self.max_contacts = int(max_contacts or s.max_contacts)
+        d.max_pairs, d.max_contacts = self.max_pairs, self.max_contacts
+        d.n_iters, d.friction = int(s.n_iters), float(s.friction)
+        d.bounds[:] = [float(x) for x in np.asarray(s.bounds).reshape(-1)[:6]]
+        d.gravity[:] = [float(x) for x in s.gravity]
+        d.dt, d.n_substeps = float(s.dt), int(s.n_substeps)
+        self._desc = d
+        self.h = self.ck.f_create(ctypes.byref(d))
+        if not self.h:
+            raise RuntimeError(f"{which}: create failed")
+
+    def close(self):
+        if self.h:
+            self.ck.f_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stage(self, st: int, mode: int = SOLVER_REFERENCE) -> int:
+        return int(self.ck.f_stage(self.h, st, mode))
+
+    def step(self, frames: int, mode: int = SOLVER_REFERENCE) -> int:
+        return int(self.ck.f_step(self.h, frames, mode))
+
+    def state(self) -> np.ndarray:
+        out = np.empty((13, self.n), np.float32)
+        self.ck.f_get_state(self.h, out.ctypes.data)
+        return out
+
+    def set_state(self, st: np.ndarray) -> None:
+        st = np.ascontiguousarray(st, dtype=np.float32).reshape(13, self.n)
+        self.ck.f_set_state(self.h, st.ctypes.data)
+
+    def inv(self):
+        im = np.empty(self.n, np.float32)
+        ii = np.empty((6, self.n), np.float32)
+        self.ck.f_get_inv(self.h, im.ctypes.data, ii.ctypes.data)
+        return im, ii
+
+    def hash(self) -> int:
+        return int(self.ck.f_hash(self.h))
+
+    def pairs(self):
+        cap = self.max_pairs
+        buf = np.empty((cap, 2), np.uint32)
+        n = int(self.ck.f_pairs(self.h, buf.ctypes.data, cap))
+        return buf[:min(n, cap)].copy(), n
+
+    def contacts(self):
+        cap = self.max_contacts
+        ab = np.empty((cap, 2), np.uint32)
+        p7 = np.empty((cap, 7), np.float32)
+        n = int(self.ck.f_contacts(self.h, ab.ctypes.data, p7.ctypes.data, cap))
+        m = min(n, cap)
+        return ab[:m].copy(), p7[:m].copy()
+
+    def bvh(self):
+        n = self.n
+        keys = np.zeros(n, np.uint64)
+        si = np.zeros(n, np.uint32)
+        left = np.zeros(max(n - 1, 1), np.int32)
+        right = np.zeros(max(n - 1, 1), np.int32)
+        parent = np.zeros(max(2 * n - 1, 1), np.int32)
+        aabb = np.zeros((max(2 * n - 1, 1), 8), np.uint16)
+        self.ck.f_bvh(self.h, keys.ctypes.data, si.ctypes.data, left.ctypes.data, right.ctypes.data,
+                      parent.ctypes.data, aabb.ctypes.data)
+        return dict(keys=keys, sorted_idx=si, left=left[:n - 1], right=right[:n - 1],
+                    parent=parent[:2 * n - 1], aabb=aabb[:2 * n - 1])
+
+    def colors(self):
+        cap = self.max_contacts
+        buf = np.empty(cap, np.uint32)
+        n = int(self.ck.f_colors(self.h, buf.ctypes.data, cap))
+        return buf[:min(n, cap)].copy()
+
+
+def fnv1a64_state(state13: np.ndarray) -> int:
+    """FNV-1a-64 of pos_x..rot_z (examples/stress_test_blocks/main.cpp:34-41, 301-311)."""
+    data = np.ascontiguousarray(state13[:7], dtype=np.float32).tobytes()
+    h = 0xcbf29ce484222325
+    for b in data:
+        h ^= b
+        h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
