@@ -1,0 +1,337 @@
+// LBVH broadphase: Morton codes -> radix sort -> one-pass bottom-up Karras
+// tree with fp16 boxes -> stackless traversal emitting (a, b) pairs already in
+// ascending (a << 32 | b) order.
+//
+// Replaces Broadphase::build_and_query / sort_pairs (core/src/broadphase.cpp:
+// 101-359). The tree is the reference's Karras tree node for node (same
+// left / right / parent / NodeBox arrays, broadphase.cpp:158-288); it is built
+// in a single kernel by letting each leaf walk up and the second child to
+// arrive at a node merge the boxes (atomic rendezvous with release / acquire
+// fences), instead of the reference's host-synchronised refit rounds.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+
+#include "internal.cuh"
+
+namespace dyph {
+namespace {
+
+constexpr int kBpThreads = 256;
+constexpr int kMaxPartners = 32;  // per-thread sorted partner window (larger lists take extra passes)
+
+__global__ void __launch_bounds__(kBpThreads) morton_kernel(GlobalBodies B, uint32_t n, dyph_aabb bounds,
+                                                            uint32_t* __restrict__ codes,
+                                                            uint32_t* __restrict__ sorted_idx,
+                                                            uint32_t* __restrict__ counts,
+                                                            uint32_t* __restrict__ tstatus, uint32_t n_tiles) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = tid; i < n; i += stride) {
+        codes[i] = morton_code(B.px(i), B.py(i), B.pz(i), bounds);
+        sorted_idx[i] = i;
+    }
+    for (uint32_t t = tid; t < n_tiles; t += stride) tstatus[t] = 0u;
+    if (tid == 0) {
+        counts[0] = 0u;
+        counts[1] = 0u;
+        counts[2] = 0u;
+    }
+}
+
+__device__ __forceinline__ uint64_t key64(const uint32_t* codes, const uint32_t* si, int i) {
+    return (static_cast<uint64_t>(codes[i]) << 32) | static_cast<uint64_t>(si[i]);
+}
+
+// Common-prefix length between sorted positions i and i+1 (lbvh_delta,
+// broadphase.cpp:38-41); -1 outside [0, n-1).
+__device__ __forceinline__ int boundary_delta(const uint32_t* codes, const uint32_t* si, int i, int n) {
+    if (i < 0 || i >= n - 1) return -1;
+    return __clzll(static_cast<long long>(key64(codes, si, i) ^ key64(codes, si, i + 1)));
+}
+
+__global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, GlobalShapes S, uint32_t n_u,
+                                                           const uint32_t* __restrict__ codes,
+                                                           const uint32_t* __restrict__ si, BvhBuffers T) {
+    const int n = static_cast<int>(n_u);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t body = si[k];
+    T.sorted_keys[k] = key64(codes, si, k);
+    T.inv_sorted[body] = static_cast<uint32_t>(k);
+    const uint32_t sh = B.shape(body);
+    uint4 box = leaf_box(S.type(sh), B.px(body), B.py(body), B.pz(body), B.qw(body), B.qx(body), B.qy(body),
+                         B.qz(body), S.hx(sh), S.hy(sh), S.hz(sh));
+    int node = n - 1 + k;
+    T.aabb[node] = box;
+    if (k == 0) {
+        T.parent[0] = -1;
+        T.root[0] = 0;
+    }
+    if (n == 1) {
+        T.parent[0] = -1;
+        return;
+    }
+    int l = k, r = k;
+    while (true) {
+        if (l == 0 && r == n - 1) return;  // this thread completed the root
+        const int dl = boundary_delta(codes, si, l - 1, n);
+        const int dr = boundary_delta(codes, si, r, n);
+        const bool is_left = dr > dl;  // merge across boundary r: we are the left child
+        const int s = is_left ? r : l - 1;
+        // Publish our far end and box, then rendezvous at split s.
+        T.slot[s] = static_cast<uint32_t>(is_left ? l : r);
+        __threadfence();
+        const uint32_t old = atomicAdd(&T.flags[s], 1u);
+        if ((old & 1u) == 0u) return;  // first arrival: the sibling carries on
+        __threadfence();
+        // L2 loads (ld.global.cg): the sibling's writes were made on another SM.
+        const int other = static_cast<int>(__ldcg(&T.slot[s]));
+        const int L = is_left ? l : other;
+        const int R = is_left ? other : r;
+        const int lidx = (L == s) ? (n - 1 + L) : s;
+        const int ridx = (s + 1 == R) ? (n - 1 + R) : (s + 1);
+        int pidx;
+        if (L == 0 && R == n - 1) {
+            pidx = 0;
+        } else {
+            const int pdl = boundary_delta(codes, si, L - 1, n);
+            const int pdr = boundary_delta(codes, si, R, n);
+            pidx = (pdr > pdl) ? R : L;
+        }
+        const uint4 sib = __ldcg(&T.aabb[is_left ? ridx : lidx]);
+        box = is_left ? merge_box(box, sib) : merge_box(sib, box);
+        T.aabb[pidx] = box;
+        T.left[pidx] = lidx;
+        T.right[pidx] = ridx;
+        T.parent[lidx] = pidx;
+        T.parent[ridx] = pidx;
+        T.range_hi[pidx] = R;
+        T.rsplit[s] = ridx;
+        l = L;
+        r = R;
+        node = pidx;
+    }
+}
+
+struct Partners {
+    uint32_t v[kMaxPartners];
+    int m;
+};
+
+__device__ __forceinline__ void partner_insert(Partners& p, uint32_t b) {
+    int pos = p.m;
+    if (pos == kMaxPartners) {
+        if (b >= p.v[kMaxPartners - 1]) return;
+        pos = kMaxPartners - 1;
+    } else {
+        p.m++;
+    }
+    while (pos > 0 && p.v[pos - 1] > b) {
+        p.v[pos] = p.v[pos - 1];
+        --pos;
+    }
+    p.v[pos] = b;
+}
+
+// Stackless pre-order traversal with escape links: on a hit at an internal
+// node go to its left child, otherwise jump to the right child of the split
+// at the node's range end. Collects leaves whose body index exceeds `lo`.
+// Returns the number of such leaves; keeps the kMaxPartners smallest.
+__device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const BoxF& q, uint32_t lo, Partners& p) {
+    uint32_t count = 0;
+    p.m = 0;
+    int node = 0;
+    while (node >= 0) {
+        const BoxF nb = unpack_box(__ldg(&T.aabb[node]));
+        int r;
+        if (box_overlap(nb, q)) {
+            if (node >= n - 1) {
+                const int leaf = node - (n - 1);
+                const uint32_t b = __ldg(&T.sorted_idx[leaf]);
+                if (b > lo) {
+                    ++count;
+                    partner_insert(p, b);
+                }
+                r = leaf;
+            } else {
+                node = __ldg(&T.left[node]);
+                continue;
+            }
+        } else {
+            r = (node >= n - 1) ? node - (n - 1) : __ldg(&T.range_hi[node]);
+        }
+        node = (r == n - 1) ? -1 : __ldg(&T.rsplit[r]);
+    }
+    return count;
+}
+
+__global__ void __launch_bounds__(kBpThreads) traverse_kernel(uint32_t n_u, BvhBuffers T, uint2* __restrict__ pairs,
+                                                              uint32_t max_pairs, uint32_t* __restrict__ counts,
+                                                              uint32_t* __restrict__ tstatus) {
+    __shared__ uint32_t s_tile, s_excl;
+    __shared__ uint32_t s_scan[kBpThreads / 32];
+    const int n = static_cast<int>(n_u);
+    if (threadIdx.x == 0) s_tile = atomicAdd(&counts[2], 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t a = tile * kBpThreads + threadIdx.x;
+    Partners P;
+    uint32_t cnt = 0;
+    BoxF q{};
+    if (a < n_u) {
+        const uint32_t leaf = __ldg(&T.inv_sorted[a]);
+        q = unpack_box(__ldg(&T.aabb[n - 1 + static_cast<int>(leaf)]));
+        cnt = traverse(T, n, q, a, P);
+    } else {
+        P.m = 0;
+    }
+    uint32_t total;
+    const uint32_t excl_block = block_exclusive_scan<kBpThreads>(cnt, s_scan, total);
+    if (threadIdx.x < 32) {
+        const uint32_t e = lookback_warp(tstatus, tile, total);
+        if (threadIdx.x == 0) {
+            s_excl = e;
+            const uint32_t last_tile = (n_u - 1) / kBpThreads;
+            if (tile == last_tile) {
+                const uint32_t all = e + total;
+                counts[1] = all;
+                counts[0] = all < max_pairs ? all : max_pairs;
+            }
+        }
+    }
+    __syncthreads();
+    if (a >= n_u || cnt == 0) return;
+    uint32_t off = s_excl + excl_block;
+    uint32_t written = 0;
+    while (true) {
+        for (int i = 0; i < P.m; ++i) {
+            const uint32_t pos = off + written + static_cast<uint32_t>(i);
+            if (pos < max_pairs) pairs[pos] = make_uint2(a, P.v[i]);
+        }
+        written += static_cast<uint32_t>(P.m);
+        if (written >= cnt || P.m == 0) break;
+        const uint32_t last = P.v[P.m - 1];
+        traverse(T, n, q, last, P);
+    }
+}
+
+template <typename T>
+cudaError_t dev_alloc(T** p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+dyph_status broadphase_build(dyph_broadphase* bp, const dyph_bodies* bodies, const dyph_shapes* shapes,
+                             const dyph_aabb* bounds, cudaStream_t s) {
+    if (!bp || !bodies || !shapes || !bounds) return DYPH_ERR_INVALID;
+    const uint32_t n = bodies->n;
+    if (n > bp->max_bodies) return DYPH_ERR_INVALID;
+    const uint32_t n_tiles = (std::max(n, 1u) + kBpThreads - 1) / kBpThreads;
+    GlobalBodies B{*bodies};
+    GlobalShapes S{*shapes};
+    const uint32_t mblocks = std::max(1u, std::min((n + kBpThreads - 1) / kBpThreads, 2048u));
+    morton_kernel<<<mblocks, kBpThreads, 0, s>>>(B, n, *bounds, bp->codes, bp->bvh.sorted_idx, bp->counts,
+                                                 bp->tstatus, n_tiles);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    bp->last_n = n;
+    if (n < 2) return DYPH_OK;
+    dyph_status st = sort_u32_u32(bp->codes, bp->bvh.sorted_idx, n, 30, bp->sort_ws, bp->sort_ws_bytes, s);
+    if (st != DYPH_OK) return st;
+    build_kernel<<<(n + kBpThreads - 1) / kBpThreads, kBpThreads, 0, s>>>(B, S, n, bp->codes, bp->bvh.sorted_idx,
+                                                                         bp->bvh);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    traverse_kernel<<<n_tiles, kBpThreads, 0, s>>>(n, bp->bvh, reinterpret_cast<uint2*>(bp->pairs), bp->max_pairs,
+                                                   bp->counts, bp->tstatus);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    return DYPH_OK;
+}
+
+dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broadphase** out) {
+    if (!out || max_bodies == 0 || max_pairs == 0 || max_bodies >= (1u << 30)) return DYPH_ERR_INVALID;
+    auto* bp = new (std::nothrow) dyph_broadphase();
+    if (!bp) return DYPH_ERR_NOMEM;
+    bp->max_bodies = max_bodies;
+    bp->max_pairs = max_pairs;
+    const size_t nb = max_bodies, ni = max_bodies > 1 ? max_bodies - 1 : 1, nn = 2 * nb - 1;
+    bool ok = dev_alloc(&bp->codes, nb) == cudaSuccess && dev_alloc(&bp->bvh.sorted_idx, nb) == cudaSuccess &&
+              dev_alloc(&bp->bvh.sorted_keys, nb) == cudaSuccess &&
+              dev_alloc(&bp->bvh.inv_sorted, nb) == cudaSuccess && dev_alloc(&bp->bvh.left, ni) == cudaSuccess &&
+              dev_alloc(&bp->bvh.right, ni) == cudaSuccess && dev_alloc(&bp->bvh.parent, nn) == cudaSuccess &&
+              dev_alloc(&bp->bvh.root, 1) == cudaSuccess && dev_alloc(&bp->bvh.aabb, nn) == cudaSuccess &&
+              dev_alloc(&bp->bvh.range_hi, ni) == cudaSuccess && dev_alloc(&bp->bvh.rsplit, ni) == cudaSuccess &&
+              dev_alloc(&bp->bvh.slot, ni) == cudaSuccess && dev_alloc(&bp->bvh.flags, ni) == cudaSuccess &&
+              dev_alloc(&bp->pairs, max_pairs) == cudaSuccess && dev_alloc(&bp->counts, 4) == cudaSuccess &&
+              dev_alloc(&bp->tstatus, (nb + kBpThreads - 1) / kBpThreads) == cudaSuccess;
+    if (ok) {
+        bp->sort_ws_bytes = sort_workspace_bytes(nb, 4);
+        ok = cudaMalloc(&bp->sort_ws, bp->sort_ws_bytes) == cudaSuccess;
+    }
+    // Arrival counters start even; every build adds exactly two per internal node.
+    if (ok) ok = cudaMemset(bp->bvh.flags, 0, ni * sizeof(uint32_t)) == cudaSuccess;
+    if (ok) ok = cudaMemset(bp->counts, 0, 4 * sizeof(uint32_t)) == cudaSuccess;
+    if (ok) ok = sort_prepare() == DYPH_OK;
+    if (!ok) {
+        broadphase_destroy(bp);
+        return DYPH_ERR_NOMEM;
+    }
+    *out = bp;
+    return DYPH_OK;
+}
+
+void broadphase_destroy(dyph_broadphase* bp) {
+    if (!bp) return;
+    void* ptrs[] = {bp->codes, bp->bvh.sorted_idx, bp->bvh.sorted_keys, bp->bvh.inv_sorted, bp->bvh.left,
+                    bp->bvh.right, bp->bvh.parent, bp->bvh.root, bp->bvh.aabb, bp->bvh.range_hi, bp->bvh.rsplit,
+                    bp->bvh.slot, bp->bvh.flags, bp->pairs, bp->counts, bp->tstatus, bp->sort_ws};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete bp;
+}
+
+}  // namespace dyph
+
+using namespace dyph;
+
+extern "C" dyph_status dyph_broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broadphase** out) {
+    return broadphase_create(max_bodies, max_pairs, out);
+}
+
+extern "C" void dyph_broadphase_destroy(dyph_broadphase* bp) { broadphase_destroy(bp); }
+
+extern "C" dyph_status dyph_broadphase_build_and_query(dyph_broadphase* bp, const dyph_bodies* bodies,
+                                                       const dyph_shapes* shapes, const dyph_aabb* bounds,
+                                                       dyph_stream s) {
+    return broadphase_build(bp, bodies, shapes, bounds, reinterpret_cast<cudaStream_t>(s));
+}
+
+extern "C" dyph_status dyph_broadphase_sort_pairs(dyph_broadphase* bp, uint32_t, dyph_stream) {
+    return bp ? DYPH_OK : DYPH_ERR_INVALID;  // pairs are emitted in sorted order
+}
+
+extern "C" dyph_status dyph_broadphase_download_count(dyph_broadphase* bp, dyph_stream s, uint32_t* out) {
+    if (!bp || !out) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaMemcpyAsync(out, bp->counts + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    return DYPH_OK;
+}
+
+extern "C" const dyph_pair* dyph_broadphase_pairs(const dyph_broadphase* bp) { return bp ? bp->pairs : nullptr; }
+extern "C" const uint32_t* dyph_broadphase_count_ptr(const dyph_broadphase* bp) { return bp ? bp->counts : nullptr; }
+extern "C" uint32_t dyph_broadphase_max_pairs(const dyph_broadphase* bp) { return bp ? bp->max_pairs : 0u; }
+
+extern "C" dyph_status dyph_broadphase_bvh_view(const dyph_broadphase* bp, uint32_t n_active, dyph_bvh_view* out) {
+    if (!bp || !out) return DYPH_ERR_INVALID;
+    out->left = bp->bvh.left;
+    out->right = bp->bvh.right;
+    out->parent = bp->bvh.parent;
+    out->root = bp->bvh.root;
+    out->sorted_idx = bp->bvh.sorted_idx;
+    out->aabb = reinterpret_cast<const dyph_node_box*>(bp->bvh.aabb);
+    out->sorted_keys = bp->bvh.sorted_keys;
+    out->n = n_active;
+    return DYPH_OK;
+}

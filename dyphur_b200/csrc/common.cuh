@@ -1,0 +1,165 @@
+// Shared device helpers for the sm_100a frame-step kernels.
+//
+// Numerics: the library is compiled with --fmad=false, -prec-div=true and
+// -prec-sqrt=true, so every a*b+c is two correctly rounded operations and
+// division / square root are IEEE. That makes each kernel's float results
+// identical to the reference's host build for the same inputs.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/dyphur_b200.h"
+
+namespace dyph {
+
+constexpr uint32_t kFlagStatic = 1u;    // BodyFlag::Static (core/include/core/body.hpp:9)
+constexpr uint32_t kFlagSleeping = 4u;  // BodyFlag::Sleeping (core/include/core/body.hpp:11)
+constexpr uint32_t kShapeBox = 0u;
+constexpr uint32_t kShapeSphere = 1u;
+
+// Iteration limit for every device-side spin (look-back, grid barrier). With
+// the nanosleep back-off this is well over a second of waiting.
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+// Sticky device error word (DYPH_ERR_TIMEOUT ...), read by dyph_download_device_error.
+// Defined here: the library is compiled as one translation unit (dyphur_b200.cu).
+__device__ uint32_t g_device_error = 0u;
+
+__device__ __forceinline__ void raise_error(uint32_t code) { atomicCAS(&g_device_error, 0u, code); }
+
+__device__ __forceinline__ float rsqrt_ieee(float x) { return __fdiv_rn(1.0f, __fsqrt_rn(x)); }
+
+__device__ __forceinline__ uint16_t f2h_bits(float f) { return __half_as_ushort(__float2half_rn(f)); }
+__device__ __forceinline__ float h2f_bits(uint16_t h) { return __half2float(__ushort_as_half(h)); }
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ── block-wide exclusive scan of one uint32 per thread ──────────────────────
+// BLOCK threads; `smem` holds BLOCK/32 words. Returns the exclusive prefix and
+// writes the block total.
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) smem[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int NW = BLOCK / 32;
+        uint32_t w = lane < NW ? smem[lane] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= d) w += y;
+        }
+        if (lane < NW) smem[lane] = w;
+    }
+    __syncthreads();
+    uint32_t warp_prefix = warp > 0 ? smem[warp - 1] : 0u;
+    total = smem[BLOCK / 32 - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+// ── decoupled look-back over tiles ──────────────────────────────────────────
+// status[t]: 0 = not ready, (1 << 30) | v = tile aggregate v,
+// (2 << 30) | v = inclusive prefix v. Values must stay below 2^30.
+constexpr uint32_t kLbAgg = 1u << 30;
+constexpr uint32_t kLbPrefix = 2u << 30;
+constexpr uint32_t kLbMask = (1u << 30) - 1u;
+
+// Called by one full warp. Publishes the tile aggregate, looks back, publishes
+// the inclusive prefix and returns the exclusive prefix (valid in all lanes).
+// On a timeout it raises DYPH_ERR_TIMEOUT and returns 0.
+__device__ __forceinline__ uint32_t lookback_warp(uint32_t* status, uint32_t tile, uint32_t aggregate) {
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st_release(&status[0], kLbPrefix | aggregate);
+        return 0u;
+    }
+    if (lane == 0) st_release(&status[tile], kLbAgg | aggregate);
+    uint32_t exclusive = 0;
+    int64_t base = static_cast<int64_t>(tile) - 1;
+    uint32_t spins = 0;
+    while (true) {
+        int64_t t = base - lane;
+        uint32_t s = (t >= 0) ? ld_acquire(&status[t]) : kLbPrefix;
+        uint32_t flag = s & ~kLbMask;
+        // Lane j looks at tile base - j. Everything from lane 0 up to the
+        // closest tile holding an inclusive prefix must be ready.
+        unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0u);
+        unsigned is_prefix = __ballot_sync(0xffffffffu, flag == kLbPrefix);
+        unsigned first_prefix = is_prefix ? static_cast<unsigned>(__ffs(is_prefix) - 1) : 32u;
+        unsigned need = (first_prefix >= 31u) ? 0xffffffffu : ((1u << (first_prefix + 1u)) - 1u);
+        if (not_ready & need) {
+            if (++spins > kSpinLimit) {
+                raise_error(DYPH_ERR_TIMEOUT);
+                return 0u;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        uint32_t contrib = (static_cast<unsigned>(lane) <= first_prefix) ? (s & kLbMask) : 0u;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, d);
+        exclusive += contrib;
+        if (first_prefix < 32) break;
+        base -= 32;
+    }
+    if (lane == 0) st_release(&status[tile], kLbPrefix | ((exclusive + aggregate) & kLbMask));
+    return exclusive;
+}
+
+// ── bounded grid barrier for cooperative launches ───────────────────────────
+// bar[0] = arrival count, bar[1] = generation. Returns false (and raises
+// DYPH_ERR_TIMEOUT) if the wait gave up; the caller must then leave the kernel.
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t n_blocks) {
+    __shared__ int ok_flag;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        uint32_t gen = ld_acquire(&bar[1]);
+        __threadfence();
+        uint32_t arrived = atomicAdd(&bar[0], 1u);
+        if (arrived == n_blocks - 1) {
+            bar[0] = 0u;
+            __threadfence();
+            st_release(&bar[1], gen + 1u);
+        } else {
+            uint32_t spins = 0;
+            while (ld_acquire(&bar[1]) == gen) {
+                if (++spins > kSpinLimit || ld_acquire(&g_device_error) == DYPH_ERR_TIMEOUT) {
+                    raise_error(DYPH_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_flag = ok;
+    }
+    __syncthreads();
+    return ok_flag != 0;
+}
+
+}  // namespace dyph
+
+#define DYPH_CUDA_TRY(expr)                                   \
+    do {                                                      \
+        cudaError_t _e = (expr);                              \
+        if (_e != cudaSuccess) return DYPH_ERR_CUDA;          \
+    } while (0)

@@ -1,0 +1,104 @@
+// Symplectic Euler integration (core/src/integrator.cpp:7-71) and the
+// library-level C entry points (status strings, device check, error word).
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace dyph {
+namespace {
+
+constexpr int kIntThreads = 256;
+
+// One body per thread; the substep loop stays in registers, which gives the
+// same values as the reference's one launch per substep.
+__global__ void __launch_bounds__(kIntThreads) integrate_kernel(GlobalBodies B, float gx, float gy, float gz,
+                                                                float sub_dt, float half_dt, int n_substeps) {
+    const uint32_t n = B.v.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (B.im(i) == 0.f) continue;
+        if (B.v.flags[i] & kFlagSleeping) continue;
+        Pose s{B.px(i), B.py(i), B.pz(i), B.qw(i), B.qx(i), B.qy(i), B.qz(i), B.vx(i), B.vy(i), B.vz(i)};
+        const float ox = B.wx(i), oy = B.wy(i), oz = B.wz(i);
+        for (int k = 0; k < n_substeps; ++k) integrate_body(s, ox, oy, oz, gx, gy, gz, sub_dt, half_dt);
+        B.px(i) = s.px; B.py(i) = s.py; B.pz(i) = s.pz;
+        B.qw(i) = s.qw; B.qx(i) = s.qx; B.qy(i) = s.qy; B.qz(i) = s.qz;
+        B.vx(i) = s.vx; B.vy(i) = s.vy; B.vz(i) = s.vz;
+    }
+}
+
+}  // namespace
+
+dyph_status integrate_launch(const dyph_bodies* bodies, const dyph_integrator_params* p, cudaStream_t s) {
+    if (!bodies || !p || p->n_substeps <= 0) return DYPH_ERR_INVALID;
+    if (bodies->n == 0) return DYPH_OK;
+    const float sub_dt = p->dt / static_cast<float>(p->n_substeps);
+    const float half_dt = 0.5f * sub_dt;
+    const unsigned blocks = (bodies->n + kIntThreads - 1) / kIntThreads;
+    integrate_kernel<<<blocks, kIntThreads, 0, s>>>(GlobalBodies{*bodies}, p->gravity[0], p->gravity[1],
+                                                    p->gravity[2], sub_dt, half_dt, p->n_substeps);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    return DYPH_OK;
+}
+
+}  // namespace dyph
+
+extern "C" dyph_status dyph_integrate(const dyph_bodies* bodies, const dyph_integrator_params* params,
+                                      dyph_stream s) {
+    return dyph::integrate_launch(bodies, params, reinterpret_cast<cudaStream_t>(s));
+}
+
+extern "C" const char* dyph_status_string(int status) {
+    switch (status) {
+        case DYPH_OK: return "ok";
+        case DYPH_ERR_INVALID: return "invalid argument";
+        case DYPH_ERR_CUDA: return "CUDA runtime error";
+        case DYPH_ERR_PAIR_OVERFLOW: return "candidate pairs exceeded capacity";
+        case DYPH_ERR_CONTACT_OVERFLOW: return "contacts exceeded capacity";
+        case DYPH_ERR_TIMEOUT: return "bounded device wait timed out";
+        case DYPH_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+        case DYPH_ERR_NOMEM: return "device allocation failed";
+        case DYPH_ERR_NOT_FINITE: return "non-finite body state";
+        default: return "unknown status";
+    }
+}
+
+extern "C" dyph_status dyph_device_check(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return DYPH_ERR_NO_DEVICE;
+    }
+    int dev = 0, major = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DYPH_ERR_NO_DEVICE;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess)
+        return DYPH_ERR_NO_DEVICE;
+    return major == 10 ? DYPH_OK : DYPH_ERR_NO_DEVICE;
+}
+
+extern "C" dyph_status dyph_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, dyph_stream s) {
+    if (bytes == 0) return DYPH_OK;
+    if (!host_dst || !dev_src) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_copy_to_device(void* dev_dst, const void* host_src, size_t bytes, dyph_stream s) {
+    if (bytes == 0) return DYPH_OK;
+    if (!dev_dst || !host_src) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaMemcpyAsync(dev_dst, host_src, bytes, cudaMemcpyHostToDevice, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code) {
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    uint32_t h = 0, zero = 0;
+    DYPH_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h, dyph::g_device_error, sizeof(h), 0, cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaMemcpyToSymbolAsync(dyph::g_device_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    if (out_code) *out_code = h;
+    return DYPH_OK;
+}

@@ -1,0 +1,93 @@
+// Handle layouts and cross-file entry points of the native library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "contact_math.cuh"
+#include "sort.cuh"
+
+namespace dyph {
+
+// Device arrays of one LBVH (Karras indexing: internal nodes [0, n-2], leaf k
+// at n-1+k; core/include/core/broadphase.hpp:95-106).
+struct BvhBuffers {
+    uint32_t* sorted_idx;   // leaf k -> body
+    uint64_t* sorted_keys;  // (morton30 << 32 | body) of leaf k
+    uint32_t* inv_sorted;   // body -> leaf k
+    int32_t* left;          // [n-1]
+    int32_t* right;         // [n-1]
+    int32_t* parent;        // [2n-1]
+    int32_t* root;          // [1] (always 0 for distinct keys)
+    uint4* aabb;            // [2n-1] NodeBox (6 x fp16 + 2 pad)
+    int32_t* range_hi;      // [n-1] last leaf covered by internal node i
+    int32_t* rsplit;        // [n-1] right child of the node whose split is s
+    uint32_t* slot;         // [n-1] build rendezvous: far end of the first child
+    uint32_t* flags;        // [n-1] build arrival counters (two per build)
+};
+
+}  // namespace dyph
+
+struct dyph_broadphase {
+    uint32_t max_bodies = 0, max_pairs = 0, last_n = 0;
+    uint32_t* codes = nullptr;   // Morton codes, sorted in place
+    dyph::BvhBuffers bvh{};
+    dyph_pair* pairs = nullptr;  // [max_pairs]
+    uint32_t* counts = nullptr;  // [0] stored pairs, [1] true pairs, [2] traversal tile counter
+    uint32_t* tstatus = nullptr; // traversal look-back status, one word per 256 bodies
+    void* sort_ws = nullptr;
+    size_t sort_ws_bytes = 0;
+};
+
+struct dyph_narrowphase {
+    uint32_t max_contacts = 0;
+    dyph_contacts view{};         // store (count = stored contacts)
+    uint32_t* counts = nullptr;   // [0] stored (== view.n), [1] true count, [2] tile counter
+    uint32_t* status = nullptr;   // look-back status per 256-pair tile
+    uint32_t status_words = 0;    // words cleared before a run
+    uint32_t max_pairs_seen = 0;  // status capacity in tiles * 256
+};
+
+struct dyph_xpbd {
+    int32_t n_iters = 10;
+    float friction = 0.5f;
+    uint32_t max_contacts = 0, max_bodies = 0;
+    dyph_solver_mode mode = DYPH_SOLVER_REFERENCE;
+    float* lambda = nullptr;        // [max_contacts]
+    uint32_t* color = nullptr;      // [max_contacts]
+    uint32_t* order = nullptr;      // [max_contacts] contacts grouped by colour / level
+    uint32_t* pred = nullptr;       // [2 max_contacts] predecessor contact on body a / b
+    uint32_t* done = nullptr;       // [max_contacts] wave in which a contact was solved
+    uint64_t* bpri = nullptr;       // [2 max_bodies] JP priorities (double-buffered)
+    uint64_t* bmask = nullptr;      // [max_bodies] JP used-colour masks
+    uint32_t* blast = nullptr;      // [max_bodies] last contact seen per body (sequential path)
+    uint32_t* meta = nullptr;       // solver control words (see solver.cu)
+    int coop_blocks = 0;            // co-resident blocks of the coloured kernel
+};
+
+namespace dyph {
+
+dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broadphase** out);
+void broadphase_destroy(dyph_broadphase* bp);
+dyph_status broadphase_build(dyph_broadphase* bp, const dyph_bodies* bodies, const dyph_shapes* shapes,
+                             const dyph_aabb* bounds, cudaStream_t s);
+
+dyph_status narrowphase_create(uint32_t max_contacts, dyph_narrowphase** out);
+void narrowphase_destroy(dyph_narrowphase* np);
+// Size the tile-status buffer for up to max_pairs pairs (allocates; call outside graph capture).
+dyph_status narrowphase_reserve(dyph_narrowphase* np, uint32_t max_pairs);
+dyph_status narrowphase_run(dyph_narrowphase* np, const dyph_pair* pairs, const uint32_t* d_n_pairs,
+                            uint32_t max_pairs, const dyph_bodies* bodies, const dyph_shapes* shapes,
+                            cudaStream_t s);
+
+dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bodies, float friction,
+                        dyph_xpbd** out);
+void xpbd_destroy(dyph_xpbd* sv);
+dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_bodies* bodies, float dt,
+                       cudaStream_t s);
+
+// Pre-set kernel attributes of the sort (call once, outside graph capture).
+dyph_status sort_prepare();
+
+dyph_status integrate_launch(const dyph_bodies* bodies, const dyph_integrator_params* p, cudaStream_t s);
+
+}  // namespace dyph

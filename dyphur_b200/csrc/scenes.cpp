@@ -270,6 +270,34 @@ extern "C" dyph_scene_set* dyph_scene_make(int kind, uint64_t seed, int32_t a0, 
     }
 }
 
+extern "C" void dyph_pack_bodies(uint32_t n, const float* pos, const float* rot, const float* vel,
+                                 const float* ang, const float* mass, const float* inertia,
+                                 const uint32_t* flags_in, float* st, float* inv_mass, float* iI6,
+                                 uint32_t* flags_out) {
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int k = 0; k < 3; ++k) st[static_cast<size_t>(k) * n + i] = pos[3 * i + k];
+        for (int k = 0; k < 4; ++k) st[static_cast<size_t>(3 + k) * n + i] = rot[4 * i + k];
+        for (int k = 0; k < 3; ++k) st[static_cast<size_t>(7 + k) * n + i] = vel[3 * i + k];
+        for (int k = 0; k < 3; ++k) st[static_cast<size_t>(10 + k) * n + i] = ang[3 * i + k];
+        const bool is_static = (flags_in[i] & 1u) || mass[i] <= 0.f;
+        inv_mass[i] = is_static ? 0.f : 1.f / mass[i];
+        float out[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (!is_static) {
+            const float* d = inertia + 9 * static_cast<size_t>(i);
+            const float det = d[0] * (d[4] * d[8] - d[5] * d[7]) - d[1] * (d[3] * d[8] - d[5] * d[6]) +
+                              d[2] * (d[3] * d[7] - d[4] * d[6]);
+            out[0] = (d[4] * d[8] - d[5] * d[7]) / det;   // (0,0)
+            out[1] = (d[0] * d[8] - d[2] * d[6]) / det;   // (1,1)
+            out[2] = (d[0] * d[4] - d[1] * d[3]) / det;   // (2,2)
+            out[3] = -(d[1] * d[8] - d[2] * d[7]) / det;  // (0,1)
+            out[4] = (d[1] * d[5] - d[2] * d[4]) / det;   // (0,2)
+            out[5] = -(d[0] * d[5] - d[2] * d[3]) / det;  // (1,2)
+        }
+        for (int k = 0; k < 6; ++k) iI6[static_cast<size_t>(k) * n + i] = out[k];
+        flags_out[i] = is_static ? (flags_in[i] | 1u) : flags_in[i];
+    }
+}
+
 extern "C" void dyph_scene_free(dyph_scene_set* s) {
     if (!s) return;
     void* p[] = {s->pos, s->rot, s->vel, s->ang, s->mass, s->inertia, s->shape, s->flags, s->shape_type,

@@ -63,6 +63,17 @@ typedef struct dyph_scene_set {
     float friction;
 } dyph_scene_set;
 
+/* BodyStore::add for n bodies (core/src/body_store.cpp:28-69): fills the
+ * host SoA rows of a BodyView — state13 = pos xyz, rot wxyz, vel xyz, ang xyz
+ * ([13][n]), inv_mass [n], iI6 = iI_xx, iI_yy, iI_zz, iI_xy, iI_xz, iI_yz
+ * ([6][n]) and flags [n]. A body is static when flagged Static or mass <= 0;
+ * a static body gets inv_mass 0, a zero inverse inertia and the Static flag;
+ * otherwise the inverse inertia is Mat3::inverse (adjugate / determinant,
+ * core/include/core/math/mat3.hpp:61-79) of the body-frame inertia. */
+void dyph_pack_bodies(uint32_t n, const float* pos, const float* rot, const float* vel, const float* ang,
+                      const float* mass, const float* inertia, const uint32_t* flags_in, float* state13,
+                      float* inv_mass, float* iI6, uint32_t* flags_out);
+
 /* Returns NULL on a bad kind or size. Free with dyph_scene_free. */
 dyph_scene_set* dyph_scene_make(int kind, uint64_t seed, int32_t a0, int32_t a1, int32_t a2, float spacing,
                                 float jitter);

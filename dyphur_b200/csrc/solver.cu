@@ -1,0 +1,405 @@
+// XPBD contact solver: Jones–Plassmann colouring + coloured Gauss–Seidel
+// sweeps (one cooperative kernel), and the sequential-order path (one thread
+// block running a level schedule that reproduces the serial order bit for bit).
+//
+// Replaces XpbdSolver::solve (core/src/xpbd_solver.cpp:603-733) for contacts.
+// Facts the schedule relies on:
+//   * solve_contact (:413-521) writes only its two bodies and never a body with
+//     inv_mass == 0, so two contacts sharing no dynamic body commute exactly;
+//   * lambda starts at 0 and a solved contact stores lambda = depth, so every
+//     later iteration returns at `remaining <= 1e-6` — only a contact that
+//     returned at `w_total < 1e-10` can act again, and that case is tracked;
+//   * every iteration ends with a renormalisation of every body, so the
+//     quaternion update q * rsqrt(|q|^2) is applied n_iters times per frame;
+//   * with no contacts at all nothing (not even the renormalisation) runs.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+
+#include "internal.cuh"
+
+namespace dyph {
+namespace {
+
+constexpr int kColorThreads = 256;
+constexpr int kSeqThreads = 1024;
+constexpr int kSeqWindow = 4;
+constexpr uint32_t kUncolored = 0xFFFFFFFFu;
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kSerialThreshold = 256u;  // XpbdSolver::kSerialThreshold (xpbd_solver.hpp:43)
+constexpr uint32_t kMaxRounds = 256u;        // MAX_ROUNDS (xpbd_solver.cpp:645)
+
+// meta words
+constexpr int kMetaDecision = 0;  // 1 = sequential fallback requested, 2 = coloured path finished
+constexpr int kMetaRemaining = 1;
+constexpr int kMetaOverflow = 2;
+constexpr int kMetaMaxColor = 3;
+constexpr int kMetaBarrier = 4;   // [4] count, [5] generation
+constexpr int kMetaDeferred = 6;
+constexpr int kMetaColorCount = 16;   // [16, 80)
+constexpr int kMetaColorCursor = 80;  // [80, 144)
+constexpr int kMetaWords = 160;
+
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {  // xpbd_solver.cpp:31-34
+    x ^= x >> 16; x *= 0x85ebca6bu; x ^= x >> 13; x *= 0xc2b2ae35u; x ^= x >> 16;
+    return x;
+}
+
+__device__ __forceinline__ Contact load_contact(const dyph_contacts& cv, uint32_t c) {
+    Contact ct;
+    ct.a = cv.body_a[c]; ct.b = cv.body_b[c];
+    ct.px = cv.pos_x[c]; ct.py = cv.pos_y[c]; ct.pz = cv.pos_z[c];
+    ct.nx = cv.norm_x[c]; ct.ny = cv.norm_y[c]; ct.nz = cv.norm_z[c];
+    ct.depth = cv.depth[c];
+    return ct;
+}
+
+__device__ __forceinline__ uint32_t contact_count(const dyph_contacts& cv) {
+    uint32_t nc = *cv.n;
+    return nc < cv.capacity ? nc : cv.capacity;
+}
+
+__device__ __forceinline__ bool wants_sequential(int mode, uint32_t nc) {
+    return mode == DYPH_SOLVER_SEQUENTIAL || (mode == DYPH_SOLVER_REFERENCE && nc <= kSerialThreshold);
+}
+
+__device__ __forceinline__ void renorm_body(const GlobalBodies& B, uint32_t i, int times) {
+    float qw = B.qw(i), qx = B.qx(i), qy = B.qy(i), qz = B.qz(i);
+    for (int t = 0; t < times; ++t) renormalize(qw, qx, qy, qz);
+    B.qw(i) = qw; B.qx(i) = qx; B.qy(i) = qy; B.qz(i) = qz;
+}
+
+// ── coloured path (cooperative launch) ──────────────────────────────────────
+__global__ void __launch_bounds__(kColorThreads) color_solve_kernel(dyph_contacts cv, GlobalBodies B, int mode,
+                                                                    int n_iters, float mu, float dt,
+                                                                    float* __restrict__ lambda,
+                                                                    uint32_t* __restrict__ color,
+                                                                    uint32_t* __restrict__ order,
+                                                                    uint64_t* __restrict__ bpri,
+                                                                    uint64_t* __restrict__ bmask,
+                                                                    uint32_t* __restrict__ meta) {
+    __shared__ uint32_t s_off[65];
+    const uint32_t nc = contact_count(cv);
+    if (nc == 0 || wants_sequential(mode, nc)) return;
+    const uint32_t nb = B.v.n;
+    const uint32_t nblk = gridDim.x;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gstride = gridDim.x * blockDim.x;
+    uint32_t* bar = meta + kMetaBarrier;
+
+    for (uint32_t k = gtid; k < nc; k += gstride) {
+        lambda[k] = 0.f;
+        color[k] = kUncolored;
+    }
+    for (uint32_t i = gtid; i < nb; i += gstride) {
+        bmask[i] = 0ull;
+        bpri[i] = 0ull;
+    }
+    if (gtid == 0) meta[kMetaRemaining] = nc;
+    if (!grid_barrier(bar, nblk)) return;
+
+    // Jones–Plassmann rounds (xpbd_solver.cpp:645-688).
+    uint32_t r = 0;
+    for (; r < kMaxRounds; ++r) {
+        uint64_t* pri = bpri + static_cast<size_t>(r & 1u) * nb;
+        uint64_t* pri_next = bpri + static_cast<size_t>((r + 1u) & 1u) * nb;
+        for (uint32_t k = gtid; k < nc; k += gstride) {
+            if (color[k] != kUncolored) continue;
+            const uint32_t a = cv.body_a[k], b = cv.body_b[k];
+            const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
+            if (B.im(a) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[a]), pk);
+            if (B.im(b) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[b]), pk);
+        }
+        if (!grid_barrier(bar, nblk)) return;
+        for (uint32_t k = gtid; k < nc; k += gstride) {
+            if (color[k] != kUncolored) continue;
+            const uint32_t a = cv.body_a[k], b = cv.body_b[k];
+            const bool da = B.im(a) != 0.f, db = B.im(b) != 0.f;
+            const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
+            if ((da && pri[a] != pk) || (db && pri[b] != pk)) continue;
+            const uint64_t used = (da ? bmask[a] : 0ull) | (db ? bmask[b] : 0ull);
+            const uint64_t freebits = ~used;
+            if (freebits == 0ull) {
+                meta[kMetaOverflow] = 1u;
+                continue;
+            }
+            const uint32_t col = static_cast<uint32_t>(__ffsll(static_cast<long long>(freebits)) - 1);
+            color[k] = col;
+            const uint64_t bit = 1ull << col;
+            if (da) atomicOr(reinterpret_cast<unsigned long long*>(&bmask[a]), bit);
+            if (db) atomicOr(reinterpret_cast<unsigned long long*>(&bmask[b]), bit);
+            atomicMax(&meta[kMetaMaxColor], col);
+            atomicSub(&meta[kMetaRemaining], 1u);
+        }
+        for (uint32_t i = gtid; i < nb; i += gstride) pri_next[i] = 0ull;
+        if (!grid_barrier(bar, nblk)) return;
+        const uint32_t rem = ld_acquire(&meta[kMetaRemaining]);
+        const uint32_t ovf = ld_acquire(&meta[kMetaOverflow]);
+        if (rem == 0u || ovf != 0u) break;
+    }
+    {
+        const uint32_t rem = ld_acquire(&meta[kMetaRemaining]);
+        const uint32_t ovf = ld_acquire(&meta[kMetaOverflow]);
+        if (rem != 0u || ovf != 0u) {  // >64 colours or not converged: serial (xpbd_solver.cpp:690-693)
+            if (gtid == 0) meta[kMetaDecision] = 1u;
+            return;
+        }
+    }
+    const uint32_t n_colors = ld_acquire(&meta[kMetaMaxColor]) + 1u;
+    // Group contacts by colour (order inside a colour is irrelevant: disjoint dynamic bodies).
+    for (uint32_t k = gtid; k < nc; k += gstride) atomicAdd(&meta[kMetaColorCount + color[k]], 1u);
+    if (!grid_barrier(bar, nblk)) return;
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (uint32_t c = 0; c < n_colors; ++c) {
+            s_off[c] = acc;
+            acc += ld_acquire(&meta[kMetaColorCount + c]);
+        }
+        s_off[n_colors] = acc;
+    }
+    __syncthreads();
+    for (uint32_t k = gtid; k < nc; k += gstride) {
+        const uint32_t c = color[k];
+        order[s_off[c] + atomicAdd(&meta[kMetaColorCursor + c], 1u)] = k;
+    }
+    if (!grid_barrier(bar, nblk)) return;
+    // Gauss–Seidel across colours, parallel within a colour (xpbd_solver.cpp:718-732).
+    bool deferred_any = false;
+    for (int iter = 0; iter < n_iters; ++iter) {
+        if (iter == 0 || deferred_any) {
+            for (uint32_t ci = 0; ci < n_colors; ++ci) {
+                for (uint32_t idx = s_off[ci] + gtid; idx < s_off[ci + 1]; idx += gstride) {
+                    const uint32_t k = order[idx];
+                    const Contact ct = load_contact(cv, k);
+                    float lc = lambda[k];
+                    const int res = solve_contact(B, ct, mu, lc, dt);
+                    lambda[k] = lc;
+                    if (res == kSolveDeferred) meta[kMetaDeferred] = 1u;
+                }
+                if (!grid_barrier(bar, nblk)) return;
+            }
+            deferred_any = ld_acquire(&meta[kMetaDeferred]) != 0u;
+        }
+        if (!deferred_any) {
+            // Remaining iterations only renormalise: apply them all now.
+            for (uint32_t i = gtid; i < nb; i += gstride) renorm_body(B, i, n_iters - iter);
+            break;
+        }
+        for (uint32_t i = gtid; i < nb; i += gstride) renorm_body(B, i, 1);
+        if (!grid_barrier(bar, nblk)) return;
+    }
+    if (gtid == 0) meta[kMetaDecision] = 2u;
+}
+
+// ── sequential path (one block) ─────────────────────────────────────────────
+// Predecessors: contacts are sorted by (a, b), so the contacts touching body x
+// are its b-side contacts (a < x, scattered) followed by its a-side run
+// (a == x, contiguous). pred_a(c) is c-1 inside an a-run, else the last b-side
+// contact of a; pred_b(c) is the previous b-side contact of b.
+__global__ void __launch_bounds__(kSeqThreads) sequential_solve_kernel(
+    dyph_contacts cv, GlobalBodies B, int mode, int n_iters, float mu, float dt, float* __restrict__ lambda,
+    uint32_t* __restrict__ pred, uint32_t* __restrict__ entries, uint32_t* __restrict__ done,
+    uint32_t* __restrict__ bcnt, uint32_t* __restrict__ boff, uint32_t* __restrict__ meta) {
+    __shared__ uint32_t s_scan[kSeqThreads / 32];
+    __shared__ uint32_t s_carry;
+    __shared__ int s_deferred;
+    const uint32_t nc = contact_count(cv);
+    if (nc == 0) return;
+    if (!wants_sequential(mode, nc) && ld_acquire(&meta[kMetaDecision]) != 1u) return;
+    const uint32_t nb = B.v.n;
+    const uint32_t t = threadIdx.x;
+    uint32_t* pred_a = pred;
+    uint32_t* pred_b = pred + cv.capacity;
+    // 1. b-side CSR: counts
+    for (uint32_t i = t; i < nb; i += kSeqThreads) bcnt[i] = 0u;
+    if (t == 0) s_deferred = 0;
+    __syncthreads();
+    for (uint32_t c = t; c < nc; c += kSeqThreads) {
+        const uint32_t b = cv.body_b[c];
+        if (B.im(b) != 0.f) atomicAdd(&bcnt[b], 1u);
+    }
+    __syncthreads();
+    // 2. exclusive scan of counts -> boff
+    if (t == 0) s_carry = 0u;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += kSeqThreads) {
+        const uint32_t i = base + t;
+        const uint32_t v = i < nb ? bcnt[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kSeqThreads>(v, s_scan, tot);
+        if (i < nb) {
+            boff[i] = s_carry + ex;
+            bcnt[i] = 0u;  // reused as the fill cursor
+        }
+        __syncthreads();
+        if (t == 0) s_carry += tot;
+        __syncthreads();
+    }
+    if (t == 0) boff[nb] = s_carry;
+    __syncthreads();
+    // 3. fill (unordered), 4. sort each body's list and link predecessors
+    for (uint32_t c = t; c < nc; c += kSeqThreads) {
+        const uint32_t b = cv.body_b[c];
+        if (B.im(b) != 0.f) entries[boff[b] + atomicAdd(&bcnt[b], 1u)] = c;
+        pred_b[c] = kNone;
+    }
+    __syncthreads();
+    for (uint32_t x = t; x < nb; x += kSeqThreads) {
+        const uint32_t lo = boff[x], hi = boff[x + 1];
+        for (uint32_t i = lo + 1; i < hi; ++i) {
+            uint32_t v = entries[i], j = i;
+            while (j > lo && entries[j - 1] > v) {
+                entries[j] = entries[j - 1];
+                --j;
+            }
+            entries[j] = v;
+        }
+        for (uint32_t i = lo + 1; i < hi; ++i) pred_b[entries[i]] = entries[i - 1];
+        bcnt[x] = (hi > lo) ? entries[hi - 1] : kNone;  // last b-side contact of x
+    }
+    __syncthreads();
+    for (uint32_t c = t; c < nc; c += kSeqThreads) {
+        const uint32_t a = cv.body_a[c];
+        uint32_t p = kNone;
+        if (B.im(a) != 0.f) p = (c > 0 && cv.body_a[c - 1] == a) ? c - 1 : bcnt[a];
+        pred_a[c] = p;
+    }
+    __syncthreads();
+    // 5. level-scheduled sweeps; done[c] = wave (>= 1) in which c was solved.
+    bool deferred = false;
+    for (int iter = 0; iter < n_iters; ++iter) {
+        if (iter == 0 || deferred) {
+            for (uint32_t c = t; c < nc; c += kSeqThreads) {
+                done[c] = 0u;
+                if (iter == 0) lambda[c] = 0.f;
+            }
+            __syncthreads();
+            const uint32_t mine = (nc > t) ? (nc - t + kSeqThreads - 1) / kSeqThreads : 0u;
+            uint32_t cursor = 0;
+            uint32_t wave = 1;
+            while (true) {
+                int left = cursor < mine;
+                if (!__syncthreads_or(left)) break;
+                for (uint32_t j = cursor; j < mine && j < cursor + kSeqWindow; ++j) {
+                    const uint32_t c = t + j * kSeqThreads;
+                    if (done[c] != 0u) continue;
+                    const uint32_t pa = pred_a[c], pb = pred_b[c];
+                    const uint32_t da = (pa == kNone) ? 1u : done[pa];
+                    const uint32_t db = (pb == kNone) ? 1u : done[pb];
+                    const bool ready = (pa == kNone || (da != 0u && da < wave)) && (pb == kNone || (db != 0u && db < wave));
+                    if (!ready) continue;
+                    const Contact ct = load_contact(cv, c);
+                    float lc = lambda[c];
+                    if (solve_contact(B, ct, mu, lc, dt) == kSolveDeferred) s_deferred = 1;
+                    lambda[c] = lc;
+                    done[c] = wave;
+                }
+                while (cursor < mine && done[t + cursor * kSeqThreads] != 0u) ++cursor;
+                __syncthreads();
+                ++wave;
+                if (wave > kSpinLimit) {
+                    raise_error(DYPH_ERR_TIMEOUT);
+                    return;
+                }
+            }
+            __syncthreads();
+            deferred = s_deferred != 0;
+        }
+        if (!deferred) {
+            for (uint32_t i = t; i < nb; i += kSeqThreads) renorm_body(B, i, n_iters - iter);
+            break;
+        }
+        for (uint32_t i = t; i < nb; i += kSeqThreads) renorm_body(B, i, 1);
+        __syncthreads();
+    }
+}
+
+int coop_block_count() {
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, color_solve_kernel, kColorThreads, 0);
+        blocks = sms * std::max(1, std::min(per_sm, 2));
+    }
+    return blocks;
+}
+
+}  // namespace
+
+dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bodies, float friction,
+                        dyph_xpbd** out) {
+    if (!out || n_iters < 0 || max_contacts == 0 || max_bodies == 0) return DYPH_ERR_INVALID;
+    auto* sv = new (std::nothrow) dyph_xpbd();
+    if (!sv) return DYPH_ERR_NOMEM;
+    sv->n_iters = n_iters;
+    sv->friction = friction;
+    sv->max_contacts = max_contacts;
+    sv->max_bodies = max_bodies;
+    const size_t mc = max_contacts, mb = max_bodies;
+    bool ok = cudaMalloc(&sv->lambda, mc * 4) == cudaSuccess && cudaMalloc(&sv->color, mc * 4) == cudaSuccess &&
+              cudaMalloc(&sv->order, mc * 4) == cudaSuccess && cudaMalloc(&sv->pred, 2 * mc * 4) == cudaSuccess &&
+              cudaMalloc(&sv->done, mc * 4) == cudaSuccess && cudaMalloc(&sv->bpri, 2 * mb * 8) == cudaSuccess &&
+              cudaMalloc(&sv->bmask, mb * 8) == cudaSuccess && cudaMalloc(&sv->blast, 2 * (mb + 1) * 4) == cudaSuccess &&
+              cudaMalloc(&sv->meta, kMetaWords * 4) == cudaSuccess;
+    if (!ok) {
+        xpbd_destroy(sv);
+        return DYPH_ERR_NOMEM;
+    }
+    sv->coop_blocks = coop_block_count();
+    *out = sv;
+    return DYPH_OK;
+}
+
+void xpbd_destroy(dyph_xpbd* sv) {
+    if (!sv) return;
+    void* ptrs[] = {sv->lambda, sv->color, sv->order, sv->pred, sv->done, sv->bpri, sv->bmask, sv->blast, sv->meta};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete sv;
+}
+
+dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_bodies* bodies, float dt,
+                       cudaStream_t s) {
+    if (!sv || !contacts || !bodies) return DYPH_ERR_INVALID;
+    if (bodies->n > sv->max_bodies || contacts->capacity > sv->max_contacts) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaMemsetAsync(sv->meta, 0, kMetaWords * 4, s));
+    dyph_contacts cv = *contacts;
+    GlobalBodies B{*bodies};
+    int mode = static_cast<int>(sv->mode);
+    int n_iters = sv->n_iters;
+    float mu = sv->friction;
+    void* args[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &sv->order, &sv->bpri,
+                    &sv->bmask, &sv->meta};
+    DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(color_solve_kernel), dim3(sv->coop_blocks),
+                                              dim3(kColorThreads), args, 0, s));
+    // b-side list entries reuse `order`; per-body counts and offsets live in `blast`.
+    sequential_solve_kernel<<<1, kSeqThreads, 0, s>>>(cv, B, mode, n_iters, mu, dt, sv->lambda, sv->pred,
+                                                      sv->order, sv->done, sv->blast,
+                                                      sv->blast + sv->max_bodies + 1, sv->meta);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    return DYPH_OK;
+}
+
+}  // namespace dyph
+
+using namespace dyph;
+
+extern "C" dyph_status dyph_xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bodies, float friction,
+                                        dyph_xpbd** out) {
+    return xpbd_create(n_iters, max_contacts, max_bodies, friction, out);
+}
+extern "C" void dyph_xpbd_destroy(dyph_xpbd* sv) { xpbd_destroy(sv); }
+extern "C" dyph_status dyph_xpbd_set_mode(dyph_xpbd* sv, dyph_solver_mode mode) {
+    if (!sv || (mode != DYPH_SOLVER_REFERENCE && mode != DYPH_SOLVER_SEQUENTIAL && mode != DYPH_SOLVER_COLORED))
+        return DYPH_ERR_INVALID;
+    sv->mode = mode;
+    return DYPH_OK;
+}
+extern "C" dyph_status dyph_xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_bodies* bodies,
+                                       float dt, dyph_stream s) {
+    return xpbd_solve(sv, contacts, bodies, dt, reinterpret_cast<cudaStream_t>(s));
+}

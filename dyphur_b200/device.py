@@ -1,0 +1,357 @@
+"""Device-resident scenes and the frame-step handles, over the C ABI.
+
+PyTorch provides the device memory (CUDA tensors) and streams; every kernel
+that runs is the library's own (``libdyphur_b200.so``). There is no CPU path:
+constructing any of these objects without a B200 raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+from .capi import check
+
+STATE_FIELDS = ("pos_x", "pos_y", "pos_z", "rot_w", "rot_x", "rot_y", "rot_z",
+                "vel_x", "vel_y", "vel_z", "ang_x", "ang_y", "ang_z")
+INV_FIELDS = ("iI_xx", "iI_yy", "iI_zz", "iI_xy", "iI_xz", "iI_yz")
+
+
+def require_device() -> None:
+    if not torch.cuda.is_available():
+        raise RuntimeError("dyphur_b200 needs a CUDA device (sm_100); none is visible")
+    check(capi.lib().dyph_device_check(), "dyph_device_check")
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return int(t.data_ptr())
+
+
+def pack_bodies(scene):
+    """Host BodyStore::add over a SceneSet -> (state13, inv_mass, iI6, flags)."""
+    n = scene.n_bodies
+    st = np.empty((13, n), np.float32)
+    im = np.empty(n, np.float32)
+    ii = np.empty((6, n), np.float32)
+    fl = np.empty(n, np.uint32)
+    args = [np.ascontiguousarray(a) for a in (scene.pos.astype(np.float32), scene.rot.astype(np.float32),
+                                              scene.vel.astype(np.float32), scene.ang.astype(np.float32),
+                                              scene.mass.astype(np.float32), scene.inertia.astype(np.float32),
+                                              scene.flags.astype(np.uint32))]
+    capi.lib().dyph_pack_bodies(n, *[a.ctypes.data for a in args], st.ctypes.data, im.ctypes.data,
+                                ii.ctypes.data, fl.ctypes.data)
+    return st, im, ii, fl
+
+
+class DeviceBodies:
+    """BodyView SoA in CUDA memory (one tensor per field)."""
+
+    def __init__(self, scene, device="cuda"):
+        require_device()
+        st, im, ii, fl = pack_bodies(scene)
+        self.n = scene.n_bodies
+        # one allocation for the float fields keeps them 256-byte aligned and contiguous
+        pad = (self.n + 63) // 64 * 64
+        self.fbuf = torch.zeros((20, pad), dtype=torch.float32, device=device)
+        self.fbuf[:13, :self.n] = torch.from_numpy(st).to(device)
+        self.fbuf[13, :self.n] = torch.from_numpy(im).to(device)
+        self.fbuf[14:20, :self.n] = torch.from_numpy(ii).to(device)
+        self.shape = torch.from_numpy(scene.shape.astype(np.int32)).to(device)
+        self.flags = torch.from_numpy(fl.astype(np.int32)).to(device)
+        self.view = capi.Bodies()
+        for k, f in enumerate(STATE_FIELDS):
+            setattr(self.view, f, _ptr(self.fbuf[k]))
+        self.view.inv_mass = _ptr(self.fbuf[13])
+        for k, f in enumerate(INV_FIELDS):
+            setattr(self.view, f, _ptr(self.fbuf[14 + k]))
+        self.view.shape = _ptr(self.shape)
+        self.view.flags = _ptr(self.flags)
+        self.view.n = self.n
+
+    def state(self) -> np.ndarray:
+        return self.fbuf[:13, :self.n].cpu().numpy().copy()
+
+    def set_state(self, st: np.ndarray) -> None:
+        self.fbuf[:13, :self.n] = torch.from_numpy(np.ascontiguousarray(st, np.float32)).to(self.fbuf.device)
+
+    def inv(self):
+        return self.fbuf[13, :self.n].cpu().numpy(), self.fbuf[14:20, :self.n].cpu().numpy()
+
+
+class DeviceShapes:
+    def __init__(self, scene, device="cuda"):
+        self.n = int(scene.shape_type.shape[0])
+        self.type = torch.from_numpy(scene.shape_type.astype(np.int32)).to(device)
+        self.half = torch.from_numpy(np.ascontiguousarray(scene.shape_half.T, np.float32)).to(device)
+        self.ext = torch.zeros(max(self.n, 1), dtype=torch.int32, device=device)
+        self.view = capi.Shapes(_ptr(self.type), _ptr(self.half[0]), _ptr(self.half[1]), _ptr(self.half[2]),
+                                _ptr(self.ext), self.n)
+
+
+def _stream_ptr(stream) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def aabb(bounds) -> capi.AABB:
+    b = [float(x) for x in np.asarray(bounds).reshape(-1)[:6]]
+    return capi.AABB(*b)
+
+
+class Broadphase:
+    """Mirror of class Broadphase (core/include/core/broadphase.hpp:50-111)."""
+
+    def __init__(self, max_bodies: int, max_pairs: int):
+        require_device()
+        h = C.c_void_p()
+        check(capi.lib().dyph_broadphase_create(max_bodies, max_pairs, C.byref(h)), "dyph_broadphase_create")
+        self.h = h
+        self.max_pairs = max_pairs
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            capi.lib().dyph_broadphase_destroy(self.h)
+            self.h = None
+
+    def build_and_query(self, bodies: DeviceBodies, shapes: DeviceShapes, bounds, stream=None) -> None:
+        b = aabb(bounds)
+        check(capi.lib().dyph_broadphase_build_and_query(self.h, C.byref(bodies.view), C.byref(shapes.view),
+                                                         C.byref(b), _stream_ptr(stream)), "build_and_query")
+
+    def download_count(self, stream=None) -> int:
+        out = C.c_uint32()
+        check(capi.lib().dyph_broadphase_download_count(self.h, _stream_ptr(stream), C.byref(out)))
+        return int(out.value)
+
+    def pairs(self, stream=None) -> np.ndarray:
+        n = min(self.download_count(stream), self.max_pairs)
+        out = np.empty((n, 2), np.uint32)
+        if n:
+            torch.cuda.synchronize()
+            host = torch.empty((n, 2), dtype=torch.int32)
+            src = capi.lib().dyph_broadphase_pairs(self.h)
+            _d2h(host, src, n * 8)
+            out = host.numpy().view(np.uint32).copy()
+        return out
+
+    def bvh(self, n: int) -> dict:
+        v = capi.BvhView()
+        check(capi.lib().dyph_broadphase_bvh_view(self.h, n, C.byref(v)))
+        out = {}
+        specs = [("keys", v.sorted_keys, n, np.uint64, torch.int64), ("sorted_idx", v.sorted_idx, n, np.uint32, torch.int32),
+                 ("left", v.left, n - 1, np.int32, torch.int32), ("right", v.right, n - 1, np.int32, torch.int32),
+                 ("parent", v.parent, 2 * n - 1, np.int32, torch.int32)]
+        torch.cuda.synchronize()
+        for name, ptr, cnt, npdt, tdt in specs:
+            host = torch.empty(max(cnt, 0), dtype=tdt)
+            if cnt > 0:
+                _d2h(host, ptr, cnt * host.element_size())
+            out[name] = host.numpy().view(npdt).copy()
+        box = torch.empty((2 * n - 1, 8), dtype=torch.int16)
+        _d2h(box, v.aabb, (2 * n - 1) * 16)
+        out["aabb"] = box.numpy().view(np.uint16).copy()
+        return out
+
+
+def _d2h(host: torch.Tensor, dev_ptr, nbytes: int) -> None:
+    """Blocking device -> host copy of raw bytes (dyph_copy_to_host)."""
+    if nbytes <= 0:
+        return
+    check(capi.lib().dyph_copy_to_host(host.data_ptr(), int(dev_ptr), nbytes, None), "dyph_copy_to_host")
+
+
+def _h2d(dev_ptr, host: torch.Tensor, nbytes: int) -> None:
+    if nbytes <= 0:
+        return
+    check(capi.lib().dyph_copy_to_device(int(dev_ptr), host.data_ptr(), nbytes, None), "dyph_copy_to_device")
+
+
+def read_contacts(view: capi.Contacts, n: int):
+    """Download the first n rows of a ContactView: (ab [n,2] u32, p7 [n,7] f32)."""
+    torch.cuda.synchronize()
+    ab = np.empty((n, 2), np.uint32)
+    p7 = np.empty((n, 7), np.float32)
+    if n == 0:
+        return ab, p7
+    cols = [view.body_a, view.body_b, view.pos_x, view.pos_y, view.pos_z, view.norm_x, view.norm_y, view.norm_z,
+            view.depth]
+    for k, ptr in enumerate(cols):
+        host = torch.empty(n, dtype=torch.int32 if k < 2 else torch.float32)
+        _d2h(host, ptr, n * 4)
+        if k < 2:
+            ab[:, k] = host.numpy().view(np.uint32)
+        else:
+            p7[:, k - 2] = host.numpy()
+    return ab, p7
+
+
+class Narrowphase:
+    """Mirror of class Narrowphase (core/include/core/narrowphase.hpp:26-73)."""
+
+    def __init__(self, max_contacts: int):
+        require_device()
+        h = C.c_void_p()
+        check(capi.lib().dyph_narrowphase_create(max_contacts, C.byref(h)), "dyph_narrowphase_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            capi.lib().dyph_narrowphase_destroy(self.h)
+            self.h = None
+
+    def run(self, bp: Broadphase, bodies: DeviceBodies, shapes: DeviceShapes, stream=None) -> None:
+        L = capi.lib()
+        check(L.dyph_narrowphase_run(self.h, L.dyph_broadphase_pairs(bp.h), L.dyph_broadphase_count_ptr(bp.h),
+                                     C.byref(bodies.view), C.byref(shapes.view), _stream_ptr(stream)), "run")
+
+    def run_pairs(self, pairs_dev: torch.Tensor, n_pairs: int, bodies, shapes, stream=None) -> None:
+        check(capi.lib().dyph_narrowphase_run_host_count(self.h, _ptr(pairs_dev), n_pairs, C.byref(bodies.view),
+                                                        C.byref(shapes.view), _stream_ptr(stream)), "run")
+
+    def contacts_view(self) -> capi.Contacts:
+        v = capi.Contacts()
+        check(capi.lib().dyph_narrowphase_contacts(self.h, C.byref(v)))
+        return v
+
+    def download_count(self, stream=None):
+        a, b = C.c_uint32(), C.c_uint32()
+        check(capi.lib().dyph_narrowphase_download_count(self.h, _stream_ptr(stream), C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
+    def contacts(self, stream=None):
+        n, _ = self.download_count(stream)
+        return read_contacts(self.contacts_view(), n)
+
+
+class XpbdSolver:
+    """Mirror of class XpbdSolver (core/include/core/xpbd_solver.hpp:29-70)."""
+
+    def __init__(self, n_iters: int = 10, max_contacts: int = 16384, max_bodies: int = 1 << 16,
+                 friction: float = 0.5):
+        require_device()
+        h = C.c_void_p()
+        check(capi.lib().dyph_xpbd_create(n_iters, max_contacts, max_bodies, friction, C.byref(h)),
+              "dyph_xpbd_create")
+        self.h = h
+        self.max_contacts = max_contacts
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            capi.lib().dyph_xpbd_destroy(self.h)
+            self.h = None
+
+    def set_mode(self, mode: int) -> None:
+        check(capi.lib().dyph_xpbd_set_mode(self.h, mode))
+
+    def set_force_serial(self, v: bool) -> None:
+        self.set_mode(capi.SOLVER_SEQUENTIAL if v else capi.SOLVER_REFERENCE)
+
+    def solve(self, contacts: capi.Contacts, bodies: DeviceBodies, dt: float, stream=None) -> None:
+        check(capi.lib().dyph_xpbd_solve(self.h, C.byref(contacts), C.byref(bodies.view), float(dt),
+                                         _stream_ptr(stream)), "solve")
+
+    def colors(self, n: int, stream=None):
+        out = np.empty(max(n, 1), np.uint32)
+        nc = C.c_uint32()
+        check(capi.lib().dyph_xpbd_download_colors(self.h, _stream_ptr(stream), out.ctypes.data_as(capi._up), n,
+                                                   C.byref(nc)))
+        return out[:n], int(nc.value)
+
+
+def integrate(bodies: DeviceBodies, gravity=(0.0, -9.81, 0.0), dt=1.0 / 60.0, n_substeps=1, stream=None) -> None:
+    p = capi.IntegratorParams((C.c_float * 3)(*gravity), dt, n_substeps)
+    check(capi.lib().dyph_integrate(C.byref(bodies.view), C.byref(p), _stream_ptr(stream)), "integrate")
+
+
+def device_error(stream=None) -> int:
+    code = C.c_uint32()
+    check(capi.lib().dyph_download_device_error(_stream_ptr(stream), C.byref(code)))
+    return int(code.value)
+
+
+def state_hash(bodies: DeviceBodies, stream=None) -> int:
+    out = torch.zeros(1, dtype=torch.int64, device=bodies.fbuf.device)
+    check(capi.lib().dyph_fnv1a64_state(C.byref(bodies.view), _ptr(out), _stream_ptr(stream)))
+    return int(out.cpu().numpy().view(np.uint64)[0])
+
+
+class World:
+    """The whole frame step on one scene (dyph_world_*), graph-replayed."""
+
+    def __init__(self, scene, mode: int = capi.SOLVER_REFERENCE, max_pairs=None, max_contacts=None):
+        require_device()
+        self.scene = scene
+        self.bodies = DeviceBodies(scene)
+        self.shapes = DeviceShapes(scene)
+        d = capi.WorldDesc()
+        d.bodies = self.bodies.view
+        d.shapes = self.shapes.view
+        d.scene_bounds = aabb(scene.bounds[0])
+        d.integrator = capi.IntegratorParams((C.c_float * 3)(*scene.gravity), scene.dt, scene.n_substeps)
+        d.max_pairs = int(max_pairs or scene.max_pairs)
+        d.max_contacts = int(max_contacts or scene.max_contacts)
+        d.n_iters = scene.n_iters
+        d.friction = scene.friction
+        d.mode = mode
+        self.desc = d
+        h = C.c_void_p()
+        check(capi.lib().dyph_world_create(C.byref(d), None, C.byref(h)), "dyph_world_create")
+        self.h = h
+        bp, np_, sv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(capi.lib().dyph_world_broadphase(h, C.byref(bp)))
+        check(capi.lib().dyph_world_narrowphase(h, C.byref(np_)))
+        check(capi.lib().dyph_world_solver(h, C.byref(sv)))
+        self._bp, self._np, self._sv = bp, np_, sv
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().dyph_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, frames: int = 1, stream=None) -> None:
+        check(capi.lib().dyph_world_step(self.h, frames, _stream_ptr(stream)), "dyph_world_step")
+
+    def stats(self, stream=None) -> dict:
+        v = [C.c_uint32() for _ in range(5)]
+        check(capi.lib().dyph_world_download_stats(self.h, _stream_ptr(stream), *[C.byref(x) for x in v]))
+        keys = ("last_pairs", "last_contacts", "peak_pairs", "peak_contacts", "status")
+        return {k: int(x.value) for k, x in zip(keys, v)}
+
+    def state(self) -> np.ndarray:
+        torch.cuda.synchronize()
+        return self.bodies.state()
+
+    def hash(self) -> int:
+        return state_hash(self.bodies)
+
+    def pairs(self) -> np.ndarray:
+        L = capi.lib()
+        n = C.c_uint32()
+        check(L.dyph_broadphase_download_count(self._bp, None, C.byref(n)))
+        m = min(int(n.value), int(L.dyph_broadphase_max_pairs(self._bp)))
+        host = torch.empty((m, 2), dtype=torch.int32)
+        _d2h(host, L.dyph_broadphase_pairs(self._bp), m * 8)
+        return host.numpy().view(np.uint32).copy()
+
+    def contacts(self):
+        v = capi.Contacts()
+        check(capi.lib().dyph_narrowphase_contacts(self._np, C.byref(v)))
+        a, b = C.c_uint32(), C.c_uint32()
+        check(capi.lib().dyph_narrowphase_download_count(self._np, None, C.byref(a), C.byref(b)))
+        return read_contacts(v, int(a.value))
+
+    def bvh(self) -> dict:
+        bp = Broadphase.__new__(Broadphase)
+        bp.h = self._bp
+        try:
+            return bp.bvh(self.bodies.n)
+        finally:
+            bp.h = None

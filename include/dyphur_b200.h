@@ -118,7 +118,11 @@ typedef enum dyph_solver_mode {
     DYPH_SOLVER_REFERENCE = 0,
     /* XpbdSolver::set_force_serial(true) (core/include/core/xpbd_solver.hpp:48):
      * sorted contact order, run as a level schedule (bit-identical). */
-    DYPH_SOLVER_SEQUENTIAL = 1
+    DYPH_SOLVER_SEQUENTIAL = 1,
+    /* Jones–Plassmann colours at every contact count (no sequential threshold):
+     * the fast mode for batched small scenes; its drift against the
+     * sequential order is measured, not zero. */
+    DYPH_SOLVER_COLORED = 2
 } dyph_solver_mode;
 
 /* ── library ──────────────────────────────────────────────────────────────── */
@@ -129,6 +133,10 @@ dyph_status dyph_device_check(void);
 /* Sticky device-side error word of the library (DYPH_ERR_TIMEOUT etc.), read
  * and cleared. Blocks on the stream. */
 dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code);
+/* Blocking raw copies between host memory and device memory (the Buffer<T>
+ * upload / download of compute/include/compute/buffer.hpp:41-49). */
+dyph_status dyph_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, dyph_stream s);
+dyph_status dyph_copy_to_device(void* dev_dst, const void* host_src, size_t bytes, dyph_stream s);
 
 /* ── integrate — replaces integrate(Stream&, BodyView, const IntegratorParams&)
  *    (core/include/core/integrator.hpp:25, core/src/integrator.cpp:7-71) ──── */

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Integer / index outputs (Morton keys, BVH arrays, pair lists, contact pairs,
+colours) and every float of the body state are compared bit for bit: the
+kernels are built with --fmad=false and IEEE division / sqrt, so the
+reference's float path is reproduced exactly (tolerance 0 ULP).
+"""
+import numpy as np
+import pytest
+
+from dyphur_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    from dyphur_b200 import device
+    device.require_device()
+    return device
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+def stage_parity(dev, oracle_mod, scene, frame, mode=0):
+    """Advance the oracle to `frame`, then run each stage of the next frame on
+    both sides from the same input state and compare every output."""
+    o = oracle_mod.World(scene)
+    assert o.step(frame, mode) == 0
+    s0 = o.state()
+    bodies = dev.DeviceBodies(scene)
+    shapes = dev.DeviceShapes(scene)
+    im_o, ii_o = o.inv()
+    im_g, ii_g = bodies.inv()
+    assert np.array_equal(bits(im_o), bits(im_g)) and np.array_equal(bits(ii_o), bits(ii_g))
+    bodies.set_state(s0)
+    # integrate
+    o.stage(oracle_mod.STAGE_INTEGRATE)
+    dev.integrate(bodies, scene.gravity, scene.dt, scene.n_substeps)
+    assert np.array_equal(bits(o.state()), bits(bodies.state())), "integrate"
+    # broadphase
+    o.stage(oracle_mod.STAGE_BROADPHASE)
+    bp = dev.Broadphase(scene.n_bodies, scene.max_pairs)
+    bp.build_and_query(bodies, shapes, scene.bounds[0])
+    po, npo = o.pairs()
+    assert bp.download_count() == npo
+    assert np.array_equal(bp.pairs(), po), "pairs"
+    if scene.n_bodies >= 2:
+        bo, bg = o.bvh(), bp.bvh(scene.n_bodies)
+        for k in ("keys", "sorted_idx", "left", "right", "parent", "aabb"):
+            assert np.array_equal(bo[k], bg[k]), k
+    # narrowphase
+    o.stage(oracle_mod.STAGE_NARROWPHASE)
+    npz = dev.Narrowphase(scene.max_contacts)
+    npz.run(bp, bodies, shapes)
+    ao, co = o.contacts()
+    ag, cg = npz.contacts()
+    assert np.array_equal(ao, ag), "contact pairs"
+    assert np.array_equal(bits(co), bits(cg)), "contact geometry"
+    # solve
+    o.stage(oracle_mod.STAGE_SOLVE, mode)
+    sv = dev.XpbdSolver(scene.n_iters, scene.max_contacts, scene.n_bodies, scene.friction)
+    sv.set_mode(mode)
+    sv.solve(npz.contacts_view(), bodies, scene.dt)
+    assert np.array_equal(bits(o.state()), bits(bodies.state())), "solve"
+    if mode == 0 and len(ao) > 256:
+        cols, ncol = sv.colors(len(ao))
+        assert ncol > 0 and np.array_equal(cols, o.colors()), "JP colours"
+    assert dev.device_error() == 0
+
+
+@pytest.mark.parametrize("frame", [0, 22, 40, 90, 200])
+def test_stage_parity_blocks(dev, oracle_mod, frame):
+    stage_parity(dev, oracle_mod, scenes.stress_blocks(), frame)
+
+
+@pytest.mark.parametrize("frame", [30, 120])
+def test_stage_parity_blocks_sequential(dev, oracle_mod, frame):
+    stage_parity(dev, oracle_mod, scenes.stress_blocks(), frame, mode=1)
+
+
+@pytest.mark.parametrize("frame", [0, 2])
+def test_stage_parity_random_pile_65k(dev, oracle_mod, frame):
+    stage_parity(dev, oracle_mod, scenes.random_pile(65536), frame)
+
+
+def test_world_determinism_golden(dev):
+    """The reference's 8-box / 20-frame sim hash (core/tests/sim_determinism_test.cpp:224)."""
+    w = dev.World(scenes.determinism())
+    w.step(20)
+    assert w.hash() == 0xcbcd209c3665c818
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_world_blocks_300_frames(dev, oracle_mod, mode):
+    s = scenes.stress_blocks()
+    o = oracle_mod.World(s)
+    assert o.step(300, mode) == 0
+    w = dev.World(s, mode=mode)
+    w.step(300)
+    st = w.stats()
+    assert st["status"] == 0
+    assert np.array_equal(bits(w.state()), bits(o.state()))
+    assert w.hash() == o.hash()
+    assert np.array_equal(w.pairs(), o.pairs()[0])
+
+
+def test_world_run_to_run(dev):
+    s = scenes.stress_blocks()
+    hs = []
+    for _ in range(2):
+        w = dev.World(s)
+        w.step(120)
+        hs.append(w.hash())
+    assert hs[0] == hs[1]
+
+
+def test_world_random_pile_frames(dev, oracle_mod):
+    s = scenes.random_pile(65536)
+    o = oracle_mod.World(s)
+    w = dev.World(s)
+    for _ in range(3):
+        o.step(1)
+        w.step(1)
+        assert np.array_equal(bits(w.state()), bits(o.state()))
+    assert np.array_equal(w.pairs(), o.pairs()[0])
+    ag, cg = w.contacts()
+    ao, co = o.contacts()
+    assert np.array_equal(ag, ao) and np.array_equal(bits(cg), bits(co))
+
+
+def test_single_and_pair_scenes(dev, oracle_mod):
+    """Edge sizes: one body (no tree), two bodies (root only)."""
+    for n in (1, 2):
+        s = scenes.determinism((1, n, 1)) if n == 1 else scenes.determinism((1, 1, 1))
+        o = oracle_mod.World(s)
+        w = dev.World(s)
+        o.step(30)
+        w.step(30)
+        assert np.array_equal(bits(w.state()), bits(o.state()))
+
+
+def test_pair_overflow_keeps_sorted_prefix(dev, oracle_mod):
+    s = scenes.stress_blocks()
+    o = oracle_mod.World(s)
+    o.step(60)
+    full, n_true = o.pairs()
+    cap = n_true // 2
+    bodies, shapes = dev.DeviceBodies(s), dev.DeviceShapes(s)
+    bodies.set_state(o.state())
+    bp = dev.Broadphase(s.n_bodies, cap)
+    bp.build_and_query(bodies, shapes, s.bounds[0])
+    assert bp.download_count() == n_true
+    assert np.array_equal(bp.pairs(), full[:cap])
+
+
+@pytest.mark.parametrize("n", [1, 7, 4096, 4097, 100003, 1 << 20])
+def test_sort_by_key_u64(dev, n):
+    import ctypes as C
+    import torch
+    from dyphur_b200 import capi
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 2**63, n, dtype=np.int64)
+    keys[::7] = keys[0]  # duplicates: stability matters
+    vals = np.arange(n, dtype=np.int32)
+    kd = torch.from_numpy(keys).cuda()
+    vd = torch.from_numpy(vals).cuda()
+    ws_bytes = capi.lib().dyph_sort_workspace_bytes(n)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device="cuda")
+    capi.check(capi.lib().dyph_sort_by_key_u64_u32(kd.data_ptr(), vd.data_ptr(), n, ws.data_ptr(), ws_bytes,
+                                                  torch.cuda.current_stream().cuda_stream))
+    order = np.argsort(keys.view(np.uint64), kind="stable")
+    assert np.array_equal(kd.cpu().numpy(), keys[order])
+    assert np.array_equal(vd.cpu().numpy(), vals[order])
