@@ -80,14 +80,15 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
         const int dr = boundary_delta(codes, si, r, n);
         const bool is_left = dr > dl;  // merge across boundary r: we are the left child
         const int s = is_left ? r : l - 1;
-        // Publish our far end and box, then rendezvous at split s.
-        T.slot[s] = static_cast<uint32_t>(is_left ? l : r);
+        // Publish our far end (left child: slot 2s, right child: slot 2s+1) and
+        // box, then rendezvous at split s.
+        T.slot[2 * s + (is_left ? 0 : 1)] = static_cast<uint32_t>(is_left ? l : r);
         __threadfence();
         const uint32_t old = atomicAdd(&T.flags[s], 1u);
         if ((old & 1u) == 0u) return;  // first arrival: the sibling carries on
         __threadfence();
         // L2 loads (ld.global.cg): the sibling's writes were made on another SM.
-        const int other = static_cast<int>(__ldcg(&T.slot[s]));
+        const int other = static_cast<int>(__ldcg(&T.slot[2 * s + (is_left ? 1 : 0)]));
         const int L = is_left ? l : other;
         const int R = is_left ? other : r;
         const int lidx = (L == s) ? (n - 1 + L) : s;
@@ -143,7 +144,14 @@ __device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const B
     uint32_t count = 0;
     p.m = 0;
     int node = 0;
+    // A well-formed tree visits each node at most once; anything longer (or an
+    // index outside the tree) is reported instead of followed.
+    int budget = 2 * n;
     while (node >= 0) {
+        if (node >= 2 * n - 1 || --budget < 0) {
+            raise_error(DYPH_ERR_INVALID);
+            break;
+        }
         const BoxF nb = unpack_box(__ldg(&T.aabb[node]));
         int r;
         if (box_overlap(nb, q)) {
@@ -161,6 +169,10 @@ __device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const B
             }
         } else {
             r = (node >= n - 1) ? node - (n - 1) : __ldg(&T.range_hi[node]);
+        }
+        if (r < 0 || r > n - 1) {
+            raise_error(DYPH_ERR_INVALID);
+            break;
         }
         node = (r == n - 1) ? -1 : __ldg(&T.rsplit[r]);
     }
@@ -262,7 +274,7 @@ dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broa
               dev_alloc(&bp->bvh.right, ni) == cudaSuccess && dev_alloc(&bp->bvh.parent, nn) == cudaSuccess &&
               dev_alloc(&bp->bvh.root, 1) == cudaSuccess && dev_alloc(&bp->bvh.aabb, nn) == cudaSuccess &&
               dev_alloc(&bp->bvh.range_hi, ni) == cudaSuccess && dev_alloc(&bp->bvh.rsplit, ni) == cudaSuccess &&
-              dev_alloc(&bp->bvh.slot, ni) == cudaSuccess && dev_alloc(&bp->bvh.flags, ni) == cudaSuccess &&
+              dev_alloc(&bp->bvh.slot, 2 * ni) == cudaSuccess && dev_alloc(&bp->bvh.flags, ni) == cudaSuccess &&
               dev_alloc(&bp->pairs, max_pairs) == cudaSuccess && dev_alloc(&bp->counts, 4) == cudaSuccess &&
               dev_alloc(&bp->tstatus, (nb + kBpThreads - 1) / kBpThreads) == cudaSuccess;
     if (ok) {

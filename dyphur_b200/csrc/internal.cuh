@@ -21,7 +21,7 @@ struct BvhBuffers {
     uint4* aabb;            // [2n-1] NodeBox (6 x fp16 + 2 pad)
     int32_t* range_hi;      // [n-1] last leaf covered by internal node i
     int32_t* rsplit;        // [n-1] right child of the node whose split is s
-    uint32_t* slot;         // [n-1] build rendezvous: far end of the first child
+    uint32_t* slot;         // [2(n-1)] build rendezvous: far end of the left / right child
     uint32_t* flags;        // [n-1] build arrival counters (two per build)
 };
 

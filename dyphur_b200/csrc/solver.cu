@@ -299,7 +299,9 @@ __global__ void __launch_bounds__(kSeqThreads) sequential_solve_kernel(
                 while (cursor < mine && done[t + cursor * kSeqThreads] != 0u) ++cursor;
                 __syncthreads();
                 ++wave;
-                if (wave > kSpinLimit) {
+                // The smallest unsolved contact is always ready, so a correct
+                // schedule needs at most nc waves.
+                if (wave > nc + 2u) {
                     raise_error(DYPH_ERR_TIMEOUT);
                     return;
                 }

@@ -145,11 +145,14 @@ def test_single_and_pair_scenes(dev, oracle_mod):
 def test_pair_overflow_keeps_sorted_prefix(dev, oracle_mod):
     s = scenes.stress_blocks()
     o = oracle_mod.World(s)
-    o.step(60)
+    o.step(59)
+    o.stage(oracle_mod.STAGE_INTEGRATE)
+    st = o.state()
+    o.stage(oracle_mod.STAGE_BROADPHASE)
     full, n_true = o.pairs()
     cap = n_true // 2
     bodies, shapes = dev.DeviceBodies(s), dev.DeviceShapes(s)
-    bodies.set_state(o.state())
+    bodies.set_state(st)
     bp = dev.Broadphase(s.n_bodies, cap)
     bp.build_and_query(bodies, shapes, s.bounds[0])
     assert bp.download_count() == n_true
