@@ -80,6 +80,8 @@ _PROTOS = {
     "dyph_xpbd_set_mode": (_st, [_vp, C.c_int]),
     "dyph_xpbd_solve": (_st, [_vp, C.POINTER(Contacts), C.POINTER(Bodies), C.c_float, _vp]),
     "dyph_xpbd_download_colors": (_st, [_vp, _vp, _up, C.c_uint32, _up]),
+    "dyph_xpbd_download_stats": (_st, [_vp, _vp, _up, _up, _up]),
+    "dyph_xpbd_download_phase_ns": (_st, [_vp, _vp, _vp]),
     "dyph_fnv1a64_state": (_st, [C.POINTER(Bodies), _vp, _vp]),
     "dyph_world_create": (_st, [C.POINTER(WorldDesc), _vp, C.POINTER(_vp)]),
     "dyph_world_destroy": (None, [_vp]),
@@ -88,6 +90,13 @@ _PROTOS = {
     "dyph_world_broadphase": (_st, [_vp, C.POINTER(_vp)]),
     "dyph_world_narrowphase": (_st, [_vp, C.POINTER(_vp)]),
     "dyph_world_solver": (_st, [_vp, C.POINTER(_vp)]),
+    "dyph_world_capture_episode": (_st, [_vp, C.c_int32, C.c_int32, C.POINTER(_vp), C.POINTER(_vp)]),
+    "dyph_world_run_episode": (_st, [_vp, _vp]),
+    "dyph_world_download_history": (_st, [_vp, _vp, _vp, _vp, C.c_uint32, _up]),
+    "dyph_event_create": (_st, [C.POINTER(_vp)]),
+    "dyph_event_destroy": (None, [_vp]),
+    "dyph_event_record": (_st, [_vp, _vp]),
+    "dyph_event_elapsed_ms": (_st, [_vp, _vp, C.POINTER(C.c_float)]),
     "dyph_copy_to_host": (_st, [_vp, _vp, C.c_size_t, _vp]),
     "dyph_copy_to_device": (_st, [_vp, _vp, C.c_size_t, _vp]),
     "dyph_pack_bodies": (None, [C.c_uint32] + [_vp] * 11),

@@ -25,12 +25,14 @@ __global__ void __launch_bounds__(kBpThreads) morton_kernel(GlobalBodies B, uint
                                                             uint32_t* __restrict__ codes,
                                                             uint32_t* __restrict__ sorted_idx,
                                                             uint32_t* __restrict__ counts,
-                                                            uint32_t* __restrict__ tstatus, uint32_t n_tiles) {
+                                                            uint32_t* __restrict__ tstatus, uint32_t n_tiles,
+                                                            uint32_t* __restrict__ bucket_cnt) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < n; i += stride) {
         codes[i] = morton_code(B.px(i), B.py(i), B.pz(i), bounds);
         sorted_idx[i] = i;
+        bucket_cnt[i] = 0u;
     }
     for (uint32_t t = tid; t < n_tiles; t += stride) tstatus[t] = 0u;
     if (tid == 0) {
@@ -65,6 +67,10 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
                          B.qz(body), S.hx(sh), S.hy(sh), S.hz(sh));
     int node = n - 1 + k;
     T.aabb[node] = box;
+    // Static bodies (grounds, walls) are "large": pairs with them are found
+    // from the other body's side, so no single thread walks the whole tree.
+    uint32_t big = B.im(body) == 0.f ? 1u : 0u;
+    T.big[node] = big;
     if (k == 0) {
         T.parent[0] = -1;
         T.root[0] = 0;
@@ -103,11 +109,14 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
         }
         const uint4 sib = __ldcg(&T.aabb[is_left ? ridx : lidx]);
         box = is_left ? merge_box(box, sib) : merge_box(sib, box);
+        big |= __ldcg(&T.big[is_left ? ridx : lidx]);
+        T.big[pidx] = big;
         T.aabb[pidx] = box;
         T.left[pidx] = lidx;
         T.right[pidx] = ridx;
         T.parent[lidx] = pidx;
         T.parent[ridx] = pidx;
+        T.range_lo[pidx] = L;
         T.range_hi[pidx] = R;
         T.rsplit[s] = ridx;
         l = L;
@@ -136,13 +145,73 @@ __device__ __forceinline__ void partner_insert(Partners& p, uint32_t b) {
     p.v[pos] = b;
 }
 
-// Stackless pre-order traversal with escape links: on a hit at an internal
-// node go to its left child, otherwise jump to the right child of the split
-// at the node's range end. Collects leaves whose body index exceeds `lo`.
-// Returns the number of such leaves; keeps the kMaxPartners smallest.
-__device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const BoxF& q, uint32_t lo, Partners& p) {
-    uint32_t count = 0;
-    p.m = 0;
+// Traversal record of every node (32 bytes): box + left child / body, then
+// lo, hi and the escape node — the right child of the internal node whose
+// split is hi (the next node in pre-order once this subtree is skipped), or -1
+// when hi is the last leaf.
+__global__ void __launch_bounds__(kBpThreads) finalize_nodes_kernel(uint32_t n_u, BvhBuffers T) {
+    const int n = static_cast<int>(n_u);
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= 2 * n - 1) return;
+    const uint4 box = T.aabb[j];
+    int lo, hi, w;
+    if (j >= n - 1) {
+        lo = hi = j - (n - 1);
+        w = static_cast<int>(T.sorted_idx[lo]);
+    } else {
+        lo = T.range_lo[j];
+        hi = T.range_hi[j];
+        w = T.left[j];
+    }
+    const int esc = (hi >= n - 1) ? -1 : T.rsplit[hi];
+    T.trav[2 * j] = make_uint4(box.x, box.y, box.z, static_cast<uint32_t>(w));
+    T.trav[2 * j + 1] = make_uint4(static_cast<uint32_t>(lo), static_cast<uint32_t>(hi), static_cast<uint32_t>(esc),
+                                   T.big[j]);
+}
+
+// Pair search of leaf k (pass 1). Every overlapping pair must be found exactly
+// once: a pair of two small leaves from the larger leaf index, a pair with a
+// large (static) leaf from the small side, a pair of two large leaves from the
+// larger index. So a small query visits leaves i < k plus large leaves i > k,
+// and a large query visits only large leaves i < k.
+template <typename F>
+__device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const BoxF& q, int k, bool me_big, F&& visit) {
+    int node = 0;
+    int budget = 2 * n;
+    while (node >= 0) {
+        if (node >= 2 * n - 1 || --budget < 0) {
+            raise_error(DYPH_ERR_INVALID);
+            return;
+        }
+        const uint4 r0 = __ldg(&T.trav[2 * node]);
+        const uint4 r1 = __ldg(&T.trav[2 * node + 1]);
+        const bool before = static_cast<int>(r1.x) < k;
+        const bool has_big = r1.w != 0u;
+        const bool wanted = me_big ? (has_big && before) : (before || has_big);
+        if (!wanted) {
+            if (me_big && !before) return;  // pre-order lo never decreases
+            node = static_cast<int>(r1.z);
+            continue;
+        }
+        if (box_overlap(unpack_box(r0), q)) {
+            if (node >= n - 1) {
+                visit(r0.w);
+            } else {
+                node = static_cast<int>(r0.w);
+                continue;
+            }
+        }
+        node = static_cast<int>(r1.z);
+    }
+}
+
+// Stackless pre-order traversal over the traversal records: on a hit at an
+// internal node go to its left child, otherwise take the escape link. Visits
+// only nodes whose leaf range starts below `leaf_end` (pre-order lo values
+// never decrease, so the walk stops at the first node that starts at or past
+// it). `visit(body)` is called for every overlapping leaf.
+template <typename F>
+__device__ __forceinline__ void walk(const BvhBuffers& T, int n, const BoxF& q, int leaf_end, F&& visit) {
     int node = 0;
     // A well-formed tree visits each node at most once; anything longer (or an
     // index outside the tree) is reported instead of followed.
@@ -150,38 +219,64 @@ __device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const B
     while (node >= 0) {
         if (node >= 2 * n - 1 || --budget < 0) {
             raise_error(DYPH_ERR_INVALID);
-            break;
+            return;
         }
-        const BoxF nb = unpack_box(__ldg(&T.aabb[node]));
-        int r;
+        const uint4 r0 = __ldg(&T.trav[2 * node]);
+        const uint4 r1 = __ldg(&T.trav[2 * node + 1]);
+        if (static_cast<int>(r1.x) >= leaf_end) return;
+        const BoxF nb = unpack_box(r0);
         if (box_overlap(nb, q)) {
             if (node >= n - 1) {
-                const int leaf = node - (n - 1);
-                const uint32_t b = __ldg(&T.sorted_idx[leaf]);
-                if (b > lo) {
-                    ++count;
-                    partner_insert(p, b);
-                }
-                r = leaf;
+                visit(r0.w);
             } else {
-                node = __ldg(&T.left[node]);
+                node = static_cast<int>(r0.w);
                 continue;
             }
-        } else {
-            r = (node >= n - 1) ? node - (n - 1) : __ldg(&T.range_hi[node]);
         }
-        if (r < 0 || r > n - 1) {
-            raise_error(DYPH_ERR_INVALID);
-            break;
-        }
-        node = (r == n - 1) ? -1 : __ldg(&T.rsplit[r]);
+        node = static_cast<int>(r1.z);
     }
+}
+
+// All overlapping partners b > lo of a query box, smallest kMaxPartners kept.
+__device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const BoxF& q, uint32_t a, uint32_t lo,
+                                             Partners& p) {
+    uint32_t count = 0;
+    p.m = 0;
+    walk(T, n, q, n, [&](uint32_t b) {
+        if (b > lo && b != a) {
+            ++count;
+            partner_insert(p, b);
+        }
+    });
     return count;
 }
 
-__global__ void __launch_bounds__(kBpThreads) traverse_kernel(uint32_t n_u, BvhBuffers T, uint2* __restrict__ pairs,
-                                                              uint32_t max_pairs, uint32_t* __restrict__ counts,
-                                                              uint32_t* __restrict__ tstatus) {
+// Pass 1, one thread per leaf in Morton order (neighbouring threads walk the
+// same part of the tree): leaf k tests only leaves i < k, so every
+// overlapping pair is found once; the pair goes to the bucket of its smaller
+// body index.
+__global__ void __launch_bounds__(kBpThreads) pair_find_kernel(uint32_t n_u, BvhBuffers T) {
+    const int n = static_cast<int>(n_u);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint4 r0 = __ldg(&T.trav[2 * (n - 1 + k)]);
+    const uint4 r1 = __ldg(&T.trav[2 * (n - 1 + k) + 1]);
+    const BoxF q = unpack_box(r0);
+    const uint32_t me = r0.w;
+    walk_pairs(T, n, q, k, r1.w != 0u, [&](uint32_t other) {
+        const uint32_t a = me < other ? me : other;
+        const uint32_t b = me < other ? other : me;
+        const uint32_t slot = atomicAdd(&T.bucket_cnt[a], 1u);
+        if (slot < static_cast<uint32_t>(kBucket)) T.bucket[static_cast<size_t>(a) * kBucket + slot] = b;
+    });
+}
+
+// Pass 2, one thread per body in body order: sort the bucket, place it with a
+// block scan + decoupled look-back, write it. Buckets that overflowed are
+// rebuilt by a full traversal from the body's own leaf.
+__global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, BvhBuffers T, uint2* __restrict__ pairs,
+                                                                uint32_t max_pairs, uint32_t* __restrict__ counts,
+                                                                uint32_t* __restrict__ tstatus) {
     __shared__ uint32_t s_tile, s_excl;
     __shared__ uint32_t s_scan[kBpThreads / 32];
     const int n = static_cast<int>(n_u);
@@ -190,14 +285,20 @@ __global__ void __launch_bounds__(kBpThreads) traverse_kernel(uint32_t n_u, BvhB
     const uint32_t tile = s_tile;
     const uint32_t a = tile * kBpThreads + threadIdx.x;
     Partners P;
+    P.m = 0;
     uint32_t cnt = 0;
     BoxF q{};
+    bool full = false;
     if (a < n_u) {
-        const uint32_t leaf = __ldg(&T.inv_sorted[a]);
-        q = unpack_box(__ldg(&T.aabb[n - 1 + static_cast<int>(leaf)]));
-        cnt = traverse(T, n, q, a, P);
-    } else {
-        P.m = 0;
+        cnt = T.bucket_cnt[a];
+        if (cnt <= static_cast<uint32_t>(kBucket)) {
+            for (uint32_t i = 0; i < cnt; ++i) partner_insert(P, T.bucket[static_cast<size_t>(a) * kBucket + i]);
+        } else {
+            full = true;
+            const uint32_t leaf = __ldg(&T.inv_sorted[a]);
+            q = unpack_box(__ldg(&T.trav[2 * (n - 1 + static_cast<int>(leaf))]));
+            traverse(T, n, q, a, a, P);
+        }
     }
     uint32_t total;
     const uint32_t excl_block = block_exclusive_scan<kBpThreads>(cnt, s_scan, total);
@@ -223,9 +324,9 @@ __global__ void __launch_bounds__(kBpThreads) traverse_kernel(uint32_t n_u, BvhB
             if (pos < max_pairs) pairs[pos] = make_uint2(a, P.v[i]);
         }
         written += static_cast<uint32_t>(P.m);
-        if (written >= cnt || P.m == 0) break;
+        if (!full || written >= cnt || P.m == 0) break;
         const uint32_t last = P.v[P.m - 1];
-        traverse(T, n, q, last, P);
+        traverse(T, n, q, a, last, P);
     }
 }
 
@@ -246,17 +347,21 @@ dyph_status broadphase_build(dyph_broadphase* bp, const dyph_bodies* bodies, con
     GlobalShapes S{*shapes};
     const uint32_t mblocks = std::max(1u, std::min((n + kBpThreads - 1) / kBpThreads, 2048u));
     morton_kernel<<<mblocks, kBpThreads, 0, s>>>(B, n, *bounds, bp->codes, bp->bvh.sorted_idx, bp->counts,
-                                                 bp->tstatus, n_tiles);
+                                                 bp->tstatus, n_tiles, bp->bvh.bucket_cnt);
     DYPH_CUDA_TRY(cudaGetLastError());
     bp->last_n = n;
     if (n < 2) return DYPH_OK;
     dyph_status st = sort_u32_u32(bp->codes, bp->bvh.sorted_idx, n, 30, bp->sort_ws, bp->sort_ws_bytes, s);
     if (st != DYPH_OK) return st;
-    build_kernel<<<(n + kBpThreads - 1) / kBpThreads, kBpThreads, 0, s>>>(B, S, n, bp->codes, bp->bvh.sorted_idx,
-                                                                         bp->bvh);
+    const uint32_t leaf_blocks = (n + kBpThreads - 1) / kBpThreads;
+    build_kernel<<<leaf_blocks, kBpThreads, 0, s>>>(B, S, n, bp->codes, bp->bvh.sorted_idx, bp->bvh);
     DYPH_CUDA_TRY(cudaGetLastError());
-    traverse_kernel<<<n_tiles, kBpThreads, 0, s>>>(n, bp->bvh, reinterpret_cast<uint2*>(bp->pairs), bp->max_pairs,
-                                                   bp->counts, bp->tstatus);
+    finalize_nodes_kernel<<<(2 * n - 1 + kBpThreads - 1) / kBpThreads, kBpThreads, 0, s>>>(n, bp->bvh);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    pair_find_kernel<<<leaf_blocks, kBpThreads, 0, s>>>(n, bp->bvh);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    pair_write_kernel<<<n_tiles, kBpThreads, 0, s>>>(n, bp->bvh, reinterpret_cast<uint2*>(bp->pairs), bp->max_pairs,
+                                                     bp->counts, bp->tstatus);
     DYPH_CUDA_TRY(cudaGetLastError());
     return DYPH_OK;
 }
@@ -276,7 +381,10 @@ dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broa
               dev_alloc(&bp->bvh.range_hi, ni) == cudaSuccess && dev_alloc(&bp->bvh.rsplit, ni) == cudaSuccess &&
               dev_alloc(&bp->bvh.slot, 2 * ni) == cudaSuccess && dev_alloc(&bp->bvh.flags, ni) == cudaSuccess &&
               dev_alloc(&bp->pairs, max_pairs) == cudaSuccess && dev_alloc(&bp->counts, 4) == cudaSuccess &&
-              dev_alloc(&bp->tstatus, (nb + kBpThreads - 1) / kBpThreads) == cudaSuccess;
+              dev_alloc(&bp->tstatus, (nb + kBpThreads - 1) / kBpThreads) == cudaSuccess &&
+              dev_alloc(&bp->bvh.range_lo, ni) == cudaSuccess && dev_alloc(&bp->bvh.trav, 2 * nn) == cudaSuccess &&
+              dev_alloc(&bp->bvh.bucket_cnt, nb) == cudaSuccess && dev_alloc(&bp->bvh.big, nn) == cudaSuccess &&
+              dev_alloc(&bp->bvh.bucket, nb * kBucket) == cudaSuccess;
     if (ok) {
         bp->sort_ws_bytes = sort_workspace_bytes(nb, 4);
         ok = cudaMalloc(&bp->sort_ws, bp->sort_ws_bytes) == cudaSuccess;
@@ -297,7 +405,8 @@ void broadphase_destroy(dyph_broadphase* bp) {
     if (!bp) return;
     void* ptrs[] = {bp->codes, bp->bvh.sorted_idx, bp->bvh.sorted_keys, bp->bvh.inv_sorted, bp->bvh.left,
                     bp->bvh.right, bp->bvh.parent, bp->bvh.root, bp->bvh.aabb, bp->bvh.range_hi, bp->bvh.rsplit,
-                    bp->bvh.slot, bp->bvh.flags, bp->pairs, bp->counts, bp->tstatus, bp->sort_ws};
+                    bp->bvh.slot, bp->bvh.flags, bp->pairs, bp->counts, bp->tstatus, bp->sort_ws,
+                    bp->bvh.range_lo, bp->bvh.trav, bp->bvh.bucket_cnt, bp->bvh.bucket, bp->bvh.big};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete bp;

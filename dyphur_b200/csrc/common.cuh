@@ -146,7 +146,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t n_blocks) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(16);
             }
         }
         __threadfence();

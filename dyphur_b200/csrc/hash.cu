@@ -48,6 +48,31 @@ extern "C" dyph_status dyph_fnv1a64_state(const dyph_bodies* bodies, uint64_t* d
     return dyph::fnv_state(bodies, nullptr, 1u, d_hash, reinterpret_cast<cudaStream_t>(s));
 }
 
+extern "C" dyph_status dyph_xpbd_download_stats(dyph_xpbd* sv, dyph_stream s, uint32_t* path, uint32_t* n_colors,
+                                                uint32_t* rounds) {
+    if (!sv) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    uint32_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    DYPH_CUDA_TRY(cudaMemcpyAsync(meta, sv->meta, sizeof(meta), cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    if (path) *path = meta[0];
+    if (n_colors) *n_colors = meta[0] == 2u ? meta[3] + 1u : 0u;
+    if (rounds) *rounds = meta[7];
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_xpbd_download_phase_ns(dyph_xpbd* sv, dyph_stream s, uint64_t* out4) {
+    if (!sv || !out4) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    uint32_t t[10];
+    DYPH_CUDA_TRY(cudaMemcpyAsync(t, sv->meta + 144, sizeof(t), cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    uint64_t ts[5];
+    for (int i = 0; i < 5; ++i) ts[i] = static_cast<uint64_t>(t[2 * i]) | (static_cast<uint64_t>(t[2 * i + 1]) << 32);
+    for (int i = 0; i < 4; ++i) out4[i] = (ts[i + 1] >= ts[i]) ? ts[i + 1] - ts[i] : 0u;
+    return DYPH_OK;
+}
+
 extern "C" dyph_status dyph_xpbd_download_colors(dyph_xpbd* sv, dyph_stream s, uint32_t* host_colors, uint32_t cap,
                                                  uint32_t* n_colors) {
     if (!sv) return DYPH_ERR_INVALID;

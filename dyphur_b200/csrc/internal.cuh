@@ -23,7 +23,18 @@ struct BvhBuffers {
     int32_t* rsplit;        // [n-1] right child of the node whose split is s
     uint32_t* slot;         // [2(n-1)] build rendezvous: far end of the left / right child
     uint32_t* flags;        // [n-1] build arrival counters (two per build)
+    int32_t* range_lo;      // [n-1] first leaf covered by internal node i
+    // Traversal record per node, 32 bytes = one sector: [2j] = fp16 box (12 B) +
+    // left child (internal) or body (leaf); [2j+1] = lo, hi, escape node, 0.
+    uint4* trav;            // [2(2n-1)]
+    uint32_t* big;          // [2n-1] 1 when the subtree holds a static body's leaf
+    uint32_t* bucket_cnt;   // [n] candidate partners b > a found for body a
+    uint32_t* bucket;       // [n * kBucket] first kBucket partners of body a (unordered)
 };
+
+// Partners kept per body by the Morton-order pass; bodies with more take a
+// second, body-order traversal.
+constexpr int kBucket = 32;
 
 }  // namespace dyph
 
@@ -57,7 +68,7 @@ struct dyph_xpbd {
     uint32_t* order = nullptr;      // [max_contacts] contacts grouped by colour / level
     uint32_t* pred = nullptr;       // [2 max_contacts] predecessor contact on body a / b
     uint32_t* done = nullptr;       // [max_contacts] wave in which a contact was solved
-    uint64_t* bpri = nullptr;       // [2 max_bodies] JP priorities (double-buffered)
+    uint64_t* bpri = nullptr;       // [3 max_bodies] JP priorities (read / post / clear buffers)
     uint64_t* bmask = nullptr;      // [max_bodies] JP used-colour masks
     uint32_t* blast = nullptr;      // [max_bodies] last contact seen per body (sequential path)
     uint32_t* meta = nullptr;       // solver control words (see solver.cu)

@@ -23,7 +23,6 @@
 namespace dyph {
 namespace {
 
-constexpr int kColorThreads = 256;
 constexpr int kSeqThreads = 1024;
 constexpr int kSeqWindow = 4;
 constexpr uint32_t kUncolored = 0xFFFFFFFFu;
@@ -38,6 +37,10 @@ constexpr int kMetaOverflow = 2;
 constexpr int kMetaMaxColor = 3;
 constexpr int kMetaBarrier = 4;   // [4] count, [5] generation
 constexpr int kMetaDeferred = 6;
+constexpr int kMetaRounds = 7;    // JP rounds of the last coloured solve (diagnostic)
+constexpr int kMetaListLen = 8;   // [8, 11) work-list lengths of the JP rounds
+constexpr int kMetaTailRemaining = 11;
+constexpr int kMetaTime = 144;    // [144, 154) phase timestamps (ns) of the coloured solve
 constexpr int kMetaColorCount = 16;   // [16, 80)
 constexpr int kMetaColorCursor = 80;  // [80, 144)
 constexpr int kMetaWords = 160;
@@ -71,127 +74,13 @@ __device__ __forceinline__ void renorm_body(const GlobalBodies& B, uint32_t i, i
     B.qw(i) = qw; B.qx(i) = qx; B.qy(i) = qy; B.qz(i) = qz;
 }
 
-// ── coloured path (cooperative launch) ──────────────────────────────────────
-__global__ void __launch_bounds__(kColorThreads) color_solve_kernel(dyph_contacts cv, GlobalBodies B, int mode,
-                                                                    int n_iters, float mu, float dt,
-                                                                    float* __restrict__ lambda,
-                                                                    uint32_t* __restrict__ color,
-                                                                    uint32_t* __restrict__ order,
-                                                                    uint64_t* __restrict__ bpri,
-                                                                    uint64_t* __restrict__ bmask,
-                                                                    uint32_t* __restrict__ meta) {
-    __shared__ uint32_t s_off[65];
-    const uint32_t nc = contact_count(cv);
-    if (nc == 0 || wants_sequential(mode, nc)) return;
-    const uint32_t nb = B.v.n;
-    const uint32_t nblk = gridDim.x;
-    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t gstride = gridDim.x * blockDim.x;
-    uint32_t* bar = meta + kMetaBarrier;
+}  // namespace
+}  // namespace dyph
 
-    for (uint32_t k = gtid; k < nc; k += gstride) {
-        lambda[k] = 0.f;
-        color[k] = kUncolored;
-    }
-    for (uint32_t i = gtid; i < nb; i += gstride) {
-        bmask[i] = 0ull;
-        bpri[i] = 0ull;
-    }
-    if (gtid == 0) meta[kMetaRemaining] = nc;
-    if (!grid_barrier(bar, nblk)) return;
+#include "solver_color.cuh"
 
-    // Jones–Plassmann rounds (xpbd_solver.cpp:645-688).
-    uint32_t r = 0;
-    for (; r < kMaxRounds; ++r) {
-        uint64_t* pri = bpri + static_cast<size_t>(r & 1u) * nb;
-        uint64_t* pri_next = bpri + static_cast<size_t>((r + 1u) & 1u) * nb;
-        for (uint32_t k = gtid; k < nc; k += gstride) {
-            if (color[k] != kUncolored) continue;
-            const uint32_t a = cv.body_a[k], b = cv.body_b[k];
-            const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
-            if (B.im(a) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[a]), pk);
-            if (B.im(b) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[b]), pk);
-        }
-        if (!grid_barrier(bar, nblk)) return;
-        for (uint32_t k = gtid; k < nc; k += gstride) {
-            if (color[k] != kUncolored) continue;
-            const uint32_t a = cv.body_a[k], b = cv.body_b[k];
-            const bool da = B.im(a) != 0.f, db = B.im(b) != 0.f;
-            const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
-            if ((da && pri[a] != pk) || (db && pri[b] != pk)) continue;
-            const uint64_t used = (da ? bmask[a] : 0ull) | (db ? bmask[b] : 0ull);
-            const uint64_t freebits = ~used;
-            if (freebits == 0ull) {
-                meta[kMetaOverflow] = 1u;
-                continue;
-            }
-            const uint32_t col = static_cast<uint32_t>(__ffsll(static_cast<long long>(freebits)) - 1);
-            color[k] = col;
-            const uint64_t bit = 1ull << col;
-            if (da) atomicOr(reinterpret_cast<unsigned long long*>(&bmask[a]), bit);
-            if (db) atomicOr(reinterpret_cast<unsigned long long*>(&bmask[b]), bit);
-            atomicMax(&meta[kMetaMaxColor], col);
-            atomicSub(&meta[kMetaRemaining], 1u);
-        }
-        for (uint32_t i = gtid; i < nb; i += gstride) pri_next[i] = 0ull;
-        if (!grid_barrier(bar, nblk)) return;
-        const uint32_t rem = ld_acquire(&meta[kMetaRemaining]);
-        const uint32_t ovf = ld_acquire(&meta[kMetaOverflow]);
-        if (rem == 0u || ovf != 0u) break;
-    }
-    {
-        const uint32_t rem = ld_acquire(&meta[kMetaRemaining]);
-        const uint32_t ovf = ld_acquire(&meta[kMetaOverflow]);
-        if (rem != 0u || ovf != 0u) {  // >64 colours or not converged: serial (xpbd_solver.cpp:690-693)
-            if (gtid == 0) meta[kMetaDecision] = 1u;
-            return;
-        }
-    }
-    const uint32_t n_colors = ld_acquire(&meta[kMetaMaxColor]) + 1u;
-    // Group contacts by colour (order inside a colour is irrelevant: disjoint dynamic bodies).
-    for (uint32_t k = gtid; k < nc; k += gstride) atomicAdd(&meta[kMetaColorCount + color[k]], 1u);
-    if (!grid_barrier(bar, nblk)) return;
-    if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (uint32_t c = 0; c < n_colors; ++c) {
-            s_off[c] = acc;
-            acc += ld_acquire(&meta[kMetaColorCount + c]);
-        }
-        s_off[n_colors] = acc;
-    }
-    __syncthreads();
-    for (uint32_t k = gtid; k < nc; k += gstride) {
-        const uint32_t c = color[k];
-        order[s_off[c] + atomicAdd(&meta[kMetaColorCursor + c], 1u)] = k;
-    }
-    if (!grid_barrier(bar, nblk)) return;
-    // Gauss–Seidel across colours, parallel within a colour (xpbd_solver.cpp:718-732).
-    bool deferred_any = false;
-    for (int iter = 0; iter < n_iters; ++iter) {
-        if (iter == 0 || deferred_any) {
-            for (uint32_t ci = 0; ci < n_colors; ++ci) {
-                for (uint32_t idx = s_off[ci] + gtid; idx < s_off[ci + 1]; idx += gstride) {
-                    const uint32_t k = order[idx];
-                    const Contact ct = load_contact(cv, k);
-                    float lc = lambda[k];
-                    const int res = solve_contact(B, ct, mu, lc, dt);
-                    lambda[k] = lc;
-                    if (res == kSolveDeferred) meta[kMetaDeferred] = 1u;
-                }
-                if (!grid_barrier(bar, nblk)) return;
-            }
-            deferred_any = ld_acquire(&meta[kMetaDeferred]) != 0u;
-        }
-        if (!deferred_any) {
-            // Remaining iterations only renormalise: apply them all now.
-            for (uint32_t i = gtid; i < nb; i += gstride) renorm_body(B, i, n_iters - iter);
-            break;
-        }
-        for (uint32_t i = gtid; i < nb; i += gstride) renorm_body(B, i, 1);
-        if (!grid_barrier(bar, nblk)) return;
-    }
-    if (gtid == 0) meta[kMetaDecision] = 2u;
-}
+namespace dyph {
+namespace {
 
 // ── sequential path (one block) ─────────────────────────────────────────────
 // Predecessors: contacts are sorted by (a, b), so the contacts touching body x
@@ -325,7 +214,7 @@ int coop_block_count() {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, color_solve_kernel, kColorThreads, 0);
-        blocks = sms * std::max(1, std::min(per_sm, 2));
+        blocks = sms * std::max(1, std::min(per_sm, 1));
     }
     return blocks;
 }
@@ -334,7 +223,9 @@ int coop_block_count() {
 
 dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bodies, float friction,
                         dyph_xpbd** out) {
-    if (!out || n_iters < 0 || max_contacts == 0 || max_bodies == 0) return DYPH_ERR_INVALID;
+    // Contact indices must fit the 24-bit field of the colouring priorities.
+    if (!out || n_iters < 0 || max_contacts == 0 || max_contacts >= (1u << 24) || max_bodies == 0)
+        return DYPH_ERR_INVALID;
     auto* sv = new (std::nothrow) dyph_xpbd();
     if (!sv) return DYPH_ERR_NOMEM;
     sv->n_iters = n_iters;
@@ -344,7 +235,7 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
     const size_t mc = max_contacts, mb = max_bodies;
     bool ok = cudaMalloc(&sv->lambda, mc * 4) == cudaSuccess && cudaMalloc(&sv->color, mc * 4) == cudaSuccess &&
               cudaMalloc(&sv->order, mc * 4) == cudaSuccess && cudaMalloc(&sv->pred, 2 * mc * 4) == cudaSuccess &&
-              cudaMalloc(&sv->done, mc * 4) == cudaSuccess && cudaMalloc(&sv->bpri, 2 * mb * 8) == cudaSuccess &&
+              cudaMalloc(&sv->done, mc * 4) == cudaSuccess && cudaMalloc(&sv->bpri, 3 * mb * 8) == cudaSuccess &&
               cudaMalloc(&sv->bmask, mb * 8) == cudaSuccess && cudaMalloc(&sv->blast, 2 * (mb + 1) * 4) == cudaSuccess &&
               cudaMalloc(&sv->meta, kMetaWords * 4) == cudaSuccess;
     if (!ok) {
@@ -374,8 +265,8 @@ dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_
     int mode = static_cast<int>(sv->mode);
     int n_iters = sv->n_iters;
     float mu = sv->friction;
-    void* args[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &sv->order, &sv->bpri,
-                    &sv->bmask, &sv->meta};
+    void* args[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &sv->order, &sv->pred,
+                    &sv->bpri, &sv->bmask, &sv->meta};
     DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(color_solve_kernel), dim3(sv->coop_blocks),
                                               dim3(kColorThreads), args, 0, s));
     // b-side list entries reuse `order`; per-body counts and offsets live in `blast`.

@@ -21,10 +21,15 @@ struct dyph_world {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t episode = nullptr;  // n_frames frames in one graph (dyph_world_capture_episode)
+    int32_t episode_frames = 0;
 };
 
 namespace dyph {
 namespace {
+
+constexpr uint32_t kHistory = 4096;
+constexpr size_t kStatsWords = 8 + 2 * kHistory;
 
 __global__ void frame_stats_kernel(const uint32_t* __restrict__ bp_counts, const uint32_t* __restrict__ np_counts,
                                    uint32_t max_pairs, uint32_t max_contacts, uint32_t* __restrict__ stats) {
@@ -33,20 +38,40 @@ __global__ void frame_stats_kernel(const uint32_t* __restrict__ bp_counts, const
     stats[1] = c;
     stats[2] = max(stats[2], p);
     stats[3] = max(stats[3], c);
+    // per-frame history ring: [8 + 2 k] pairs, [9 + 2 k] contacts of frame k mod kHistory
+    const uint32_t f = stats[5]++;
+    stats[8 + 2 * (f % kHistory)] = p;
+    stats[9 + 2 * (f % kHistory)] = c;
     if (p > max_pairs) atomicCAS(&stats[4], 0u, static_cast<uint32_t>(DYPH_ERR_PAIR_OVERFLOW));
     if (c > max_contacts) atomicCAS(&stats[4], 0u, static_cast<uint32_t>(DYPH_ERR_CONTACT_OVERFLOW));
 }
 
-dyph_status enqueue_frame(dyph_world* w, cudaStream_t s) {
+// Records an event inside a stream capture as a real timestamp node.
+dyph_status probe_record(void* ev, cudaStream_t s) {
+    if (!ev) return DYPH_OK;
+    DYPH_CUDA_TRY(cudaEventRecordWithFlags(static_cast<cudaEvent_t>(ev), s, cudaEventRecordExternal));
+    return DYPH_OK;
+}
+
+// One frame; when probe_stage matches a stage (0 integrate, 1 broadphase,
+// 2 narrowphase, 3 solver) the events are recorded around it.
+dyph_status enqueue_frame(dyph_world* w, cudaStream_t s, int probe_stage = -1, void* ev0 = nullptr,
+                          void* ev1 = nullptr) {
     const dyph_world_desc& d = w->desc;
-    dyph_status st = integrate_launch(&d.bodies, &d.integrator, s);
-    if (st != DYPH_OK) return st;
-    st = broadphase_build(w->bp, &d.bodies, &d.shapes, &d.scene_bounds, s);
-    if (st != DYPH_OK) return st;
-    st = narrowphase_run(w->np, w->bp->pairs, w->bp->counts, w->bp->max_pairs, &d.bodies, &d.shapes, s);
-    if (st != DYPH_OK) return st;
-    st = xpbd_solve(w->sv, &w->np->view, &d.bodies, d.integrator.dt, s);
-    if (st != DYPH_OK) return st;
+    dyph_status st;
+    for (int stage = 0; stage < 4; ++stage) {
+        if (stage == probe_stage && (st = probe_record(ev0, s)) != DYPH_OK) return st;
+        switch (stage) {
+            case 0: st = integrate_launch(&d.bodies, &d.integrator, s); break;
+            case 1: st = broadphase_build(w->bp, &d.bodies, &d.shapes, &d.scene_bounds, s); break;
+            case 2:
+                st = narrowphase_run(w->np, w->bp->pairs, w->bp->counts, w->bp->max_pairs, &d.bodies, &d.shapes, s);
+                break;
+            default: st = xpbd_solve(w->sv, &w->np->view, &d.bodies, d.integrator.dt, s); break;
+        }
+        if (st != DYPH_OK) return st;
+        if (stage == probe_stage && (st = probe_record(ev1, s)) != DYPH_OK) return st;
+    }
     frame_stats_kernel<<<1, 1, 0, s>>>(w->bp->counts, w->np->counts, w->bp->max_pairs, w->np->max_contacts,
                                        w->stats);
     DYPH_CUDA_TRY(cudaGetLastError());
@@ -61,6 +86,7 @@ using namespace dyph;
 extern "C" void dyph_world_destroy(dyph_world* w) {
     if (!w) return;
     if (w->graph) cudaGraphExecDestroy(w->graph);
+    if (w->episode) cudaGraphExecDestroy(w->episode);
     if (w->ev_in) cudaEventDestroy(w->ev_in);
     if (w->ev_out) cudaEventDestroy(w->ev_out);
     if (w->stream) cudaStreamDestroy(w->stream);
@@ -84,8 +110,8 @@ extern "C" dyph_status dyph_world_create(const dyph_world_desc* desc, dyph_strea
     if (st == DYPH_OK) st = xpbd_create(desc->n_iters, desc->max_contacts, desc->bodies.n, desc->friction, &w->sv);
     if (st == DYPH_OK) {
         w->sv->mode = desc->mode;
-        if (cudaMalloc(&w->stats, 8 * sizeof(uint32_t)) != cudaSuccess ||
-            cudaMemset(w->stats, 0, 8 * sizeof(uint32_t)) != cudaSuccess ||
+        if (cudaMalloc(&w->stats, kStatsWords * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMemset(w->stats, 0, kStatsWords * sizeof(uint32_t)) != cudaSuccess ||
             cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&w->ev_in, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&w->ev_out, cudaEventDisableTiming) != cudaSuccess)
@@ -128,6 +154,72 @@ extern "C" dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_str
     return DYPH_OK;
 }
 
+extern "C" dyph_status dyph_world_capture_episode(dyph_world* w, int32_t n_frames, int32_t probe_stage,
+                                                  void* const* ev_start, void* const* ev_end) {
+    if (!w || n_frames <= 0 || probe_stage < -1 || probe_stage > 3) return DYPH_ERR_INVALID;
+    if (probe_stage >= 0 && (!ev_start || !ev_end)) return DYPH_ERR_INVALID;
+    if (w->episode) {
+        cudaGraphExecDestroy(w->episode);
+        w->episode = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    DYPH_CUDA_TRY(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+    dyph_status st = DYPH_OK;
+    for (int32_t f = 0; f < n_frames && st == DYPH_OK; ++f)
+        st = enqueue_frame(w, w->stream, probe_stage, probe_stage >= 0 ? ev_start[f] : nullptr,
+                           probe_stage >= 0 ? ev_end[f] : nullptr);
+    cudaError_t ce = cudaStreamEndCapture(w->stream, &g);
+    if (st != DYPH_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (ce != cudaSuccess) return DYPH_ERR_CUDA;
+    ce = cudaGraphInstantiate(&w->episode, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+        w->episode = nullptr;
+        return DYPH_ERR_CUDA;
+    }
+    w->episode_frames = n_frames;
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_run_episode(dyph_world* w, dyph_stream s) {
+    if (!w || !w->episode) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaEventRecord(w->ev_in, cs));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(w->stream, w->ev_in, 0));
+    DYPH_CUDA_TRY(cudaGraphLaunch(w->episode, w->stream));
+    DYPH_CUDA_TRY(cudaEventRecord(w->ev_out, w->stream));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->ev_out, 0));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_event_create(void** out) {
+    if (!out) return DYPH_ERR_INVALID;
+    cudaEvent_t e = nullptr;
+    DYPH_CUDA_TRY(cudaEventCreate(&e));
+    *out = e;
+    return DYPH_OK;
+}
+
+extern "C" void dyph_event_destroy(void* ev) {
+    if (ev) cudaEventDestroy(static_cast<cudaEvent_t>(ev));
+}
+
+extern "C" dyph_status dyph_event_record(void* ev, dyph_stream s) {
+    if (!ev) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaEventRecord(static_cast<cudaEvent_t>(ev), reinterpret_cast<cudaStream_t>(s)));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_event_elapsed_ms(void* start, void* end, float* ms) {
+    if (!start || !end || !ms) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaEventSynchronize(static_cast<cudaEvent_t>(end)));
+    DYPH_CUDA_TRY(cudaEventElapsedTime(ms, static_cast<cudaEvent_t>(start), static_cast<cudaEvent_t>(end)));
+    return DYPH_OK;
+}
+
 extern "C" dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* last_pairs,
                                                  uint32_t* last_contacts, uint32_t* peak_pairs,
                                                  uint32_t* peak_contacts, uint32_t* status) {
@@ -141,6 +233,26 @@ extern "C" dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, u
     if (peak_pairs) *peak_pairs = h[2];
     if (peak_contacts) *peak_contacts = h[3];
     if (status) *status = h[4];
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_download_history(dyph_world* w, dyph_stream s, uint32_t* pairs,
+                                                   uint32_t* contacts, uint32_t cap, uint32_t* frames_total) {
+    if (!w) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    static thread_local uint32_t h[kStatsWords];
+    DYPH_CUDA_TRY(cudaMemcpyAsync(h, w->stats, sizeof(h), cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    const uint32_t total = h[5];
+    if (frames_total) *frames_total = total;
+    // most recent min(cap, total, kHistory) frames, oldest first
+    uint32_t m = total < kHistory ? total : kHistory;
+    if (m > cap) m = cap;
+    for (uint32_t i = 0; i < m; ++i) {
+        const uint32_t f = total - m + i;
+        if (pairs) pairs[i] = h[8 + 2 * (f % kHistory)];
+        if (contacts) contacts[i] = h[9 + 2 * (f % kHistory)];
+    }
     return DYPH_OK;
 }
 

@@ -319,6 +319,52 @@ class World:
     def step(self, frames: int = 1, stream=None) -> None:
         check(capi.lib().dyph_world_step(self.h, frames, _stream_ptr(stream)), "dyph_world_step")
 
+    def capture_episode(self, n_frames: int, probe_stage: int = -1) -> None:
+        """Record n_frames frames as one graph; probe_stage 0..3 times that stage per frame."""
+        L = capi.lib()
+        self._free_probe()
+        if probe_stage >= 0:
+            evs = []
+            for _ in range(2 * n_frames):
+                e = C.c_void_p()
+                check(L.dyph_event_create(C.byref(e)))
+                evs.append(e.value)
+            self._probe = ((C.c_void_p * n_frames)(*evs[:n_frames]), (C.c_void_p * n_frames)(*evs[n_frames:]))
+            check(L.dyph_world_capture_episode(self.h, n_frames, probe_stage, self._probe[0], self._probe[1]))
+        else:
+            check(L.dyph_world_capture_episode(self.h, n_frames, -1, None, None))
+        self.episode_frames = n_frames
+
+    def history(self, cap: int = 4096):
+        """(pairs, contacts) true counts of the most recent frames, oldest first."""
+        p = np.zeros(cap, np.uint32)
+        c = np.zeros(cap, np.uint32)
+        tot = C.c_uint32()
+        check(capi.lib().dyph_world_download_history(self.h, None, p.ctypes.data, c.ctypes.data, cap,
+                                                     C.byref(tot)))
+        m = min(cap, int(tot.value), 4096)
+        return p[:m], c[:m]
+
+    def run_episode(self, stream=None) -> None:
+        check(capi.lib().dyph_world_run_episode(self.h, _stream_ptr(stream)), "dyph_world_run_episode")
+
+    def probe_ms(self) -> np.ndarray:
+        """Per-frame duration (ms) of the probed stage in the last episode run."""
+        out = np.zeros(self.episode_frames, np.float64)
+        ms = C.c_float()
+        for f in range(self.episode_frames):
+            check(capi.lib().dyph_event_elapsed_ms(self._probe[0][f], self._probe[1][f], C.byref(ms)))
+            out[f] = ms.value
+        return out
+
+    def _free_probe(self):
+        p = getattr(self, "_probe", None)
+        if p:
+            for arr in p:
+                for e in arr:
+                    capi.lib().dyph_event_destroy(e)
+        self._probe = None
+
     def stats(self, stream=None) -> dict:
         v = [C.c_uint32() for _ in range(5)]
         check(capi.lib().dyph_world_download_stats(self.h, _stream_ptr(stream), *[C.byref(x) for x in v]))

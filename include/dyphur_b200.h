@@ -204,6 +204,16 @@ dyph_status dyph_xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const 
 dyph_status dyph_xpbd_download_colors(dyph_xpbd* sv, dyph_stream s, uint32_t* host_colors, uint32_t cap,
                                       uint32_t* n_colors);
 
+/* Blocking: which path the last solve took (0 none / sequential, 1 coloured
+ * attempt fell back to sequential, 2 coloured), its colour count and the
+ * number of Jones–Plassmann rounds it needed. */
+dyph_status dyph_xpbd_download_stats(dyph_xpbd* sv, dyph_stream s, uint32_t* path, uint32_t* n_colors,
+                                     uint32_t* rounds);
+
+/* Blocking: durations (ns, device clock) of the last coloured solve's phases:
+ * set-up, colouring, grouping by colour, sweeps + renormalisation. */
+dyph_status dyph_xpbd_download_phase_ns(dyph_xpbd* sv, dyph_stream s, uint64_t* out4);
+
 /* ── state hash — replaces the host FNV-1a-64 loop
  *    (examples/stress_test_blocks/main.cpp:34-41, 301-311) ───────────────── */
 dyph_status dyph_fnv1a64_state(const dyph_bodies* bodies, uint64_t* d_hash, dyph_stream s);
@@ -234,6 +244,25 @@ dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_stream s);
 dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* last_pairs,
                                       uint32_t* last_contacts, uint32_t* peak_pairs, uint32_t* peak_contacts,
                                       uint32_t* status);
+/* Capture n_frames consecutive frames as one graph (an "episode"); with
+ * probe_stage 0..3 (integrate, broadphase, narrowphase, solver) the caller's
+ * events ev_start[f] / ev_end[f] (from dyph_event_create) are recorded around
+ * that stage of frame f — the per-stage timing of the reference's --profile
+ * mode (examples/stress_test_blocks/main.cpp:199-254) without host fences.
+ * probe_stage -1 records nothing. */
+dyph_status dyph_world_capture_episode(dyph_world* w, int32_t n_frames, int32_t probe_stage,
+                                       void* const* ev_start, void* const* ev_end);
+dyph_status dyph_world_run_episode(dyph_world* w, dyph_stream s);
+/* Timing events (cudaEvent_t behind void*). */
+dyph_status dyph_event_create(void** out);
+void dyph_event_destroy(void* ev);
+dyph_status dyph_event_record(void* ev, dyph_stream s);
+/* Blocks until `end` completes. */
+dyph_status dyph_event_elapsed_ms(void* start, void* end, float* ms);
+/* Blocking: true pair / contact counts of the most recent min(cap, 4096)
+ * frames (oldest first) and the number of frames stepped so far. */
+dyph_status dyph_world_download_history(dyph_world* w, dyph_stream s, uint32_t* pairs, uint32_t* contacts,
+                                        uint32_t cap, uint32_t* frames_total);
 dyph_status dyph_world_broadphase(dyph_world* w, dyph_broadphase** out);
 dyph_status dyph_world_narrowphase(dyph_world* w, dyph_narrowphase** out);
 dyph_status dyph_world_solver(dyph_world* w, dyph_xpbd** out);
