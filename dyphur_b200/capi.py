@@ -55,6 +55,7 @@ _PROTOS = {
     "dyph_status_string": (C.c_char_p, [C.c_int]),
     "dyph_device_check": (_st, []),
     "dyph_download_device_error": (_st, [_vp, _up]),
+    "dyph_download_device_error_site": (_st, [_vp, _up, _up]),
     "dyph_integrate": (_st, [C.POINTER(Bodies), C.POINTER(IntegratorParams), _vp]),
     "dyph_sort_workspace_bytes": (C.c_size_t, [C.c_size_t]),
     "dyph_sort_by_key_u64_u32": (_st, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, _vp]),

@@ -180,7 +180,7 @@ __device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const Box
     int budget = 2 * n;
     while (node >= 0) {
         if (node >= 2 * n - 1 || --budget < 0) {
-            raise_error(DYPH_ERR_INVALID);
+            raise_error(DYPH_ERR_INVALID, 6u);
             return;
         }
         const uint4 r0 = __ldg(&T.trav[2 * node]);
@@ -218,7 +218,7 @@ __device__ __forceinline__ void walk(const BvhBuffers& T, int n, const BoxF& q, 
     int budget = 2 * n;
     while (node >= 0) {
         if (node >= 2 * n - 1 || --budget < 0) {
-            raise_error(DYPH_ERR_INVALID);
+            raise_error(DYPH_ERR_INVALID, 7u);
             return;
         }
         const uint4 r0 = __ldg(&T.trav[2 * node]);

@@ -27,7 +27,13 @@ constexpr uint32_t kSpinLimit = 1u << 24;
 // Defined here: the library is compiled as one translation unit (dyphur_b200.cu).
 __device__ uint32_t g_device_error = 0u;
 
-__device__ __forceinline__ void raise_error(uint32_t code) { atomicCAS(&g_device_error, 0u, code); }
+// Where the first error was raised (1 look-back, 2 sort look-back, 3 grid
+// barrier, 5 sequential schedule, 6 / 7 tree walk, 8 narrowphase pair index).
+__device__ uint32_t g_device_error_site = 0u;
+
+__device__ __forceinline__ void raise_error(uint32_t code, uint32_t site = 0u) {
+    if (atomicCAS(&g_device_error, 0u, code) == 0u) g_device_error_site = site;
+}
 
 __device__ __forceinline__ float rsqrt_ieee(float x) { return __fdiv_rn(1.0f, __fsqrt_rn(x)); }
 
@@ -106,7 +112,7 @@ __device__ __forceinline__ uint32_t lookback_warp(uint32_t* status, uint32_t til
         unsigned need = (first_prefix >= 31u) ? 0xffffffffu : ((1u << (first_prefix + 1u)) - 1u);
         if (not_ready & need) {
             if (++spins > kSpinLimit) {
-                raise_error(DYPH_ERR_TIMEOUT);
+                raise_error(DYPH_ERR_TIMEOUT, 1u);
                 return 0u;
             }
             __nanosleep(32);
@@ -126,30 +132,42 @@ __device__ __forceinline__ uint32_t lookback_warp(uint32_t* status, uint32_t til
 // ── bounded grid barrier for cooperative launches ───────────────────────────
 // bar[0] = arrival count, bar[1] = generation. Returns false (and raises
 // DYPH_ERR_TIMEOUT) if the wait gave up; the caller must then leave the kernel.
+// The block's writes are ordered before thread 0's arrival by __syncthreads;
+// the arrival is an acq_rel atomic (release of the block's writes, acquire of
+// the earlier arrivals'), and the release store of the generation word with
+// the acquire spin on it carries the rest, so no separate fences are needed.
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t n_blocks) {
     __shared__ int ok_flag;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        uint32_t gen = ld_acquire(&bar[1]);
-        __threadfence();
-        uint32_t arrived = atomicAdd(&bar[0], 1u);
+        const uint32_t gen = ld_acquire(&bar[1]);
+        const uint32_t arrived = atom_add_acq_rel(&bar[0], 1u);
         if (arrived == n_blocks - 1) {
             bar[0] = 0u;
-            __threadfence();
             st_release(&bar[1], gen + 1u);
         } else {
             uint32_t spins = 0;
             while (ld_acquire(&bar[1]) == gen) {
-                if (++spins > kSpinLimit || ld_acquire(&g_device_error) == DYPH_ERR_TIMEOUT) {
-                    raise_error(DYPH_ERR_TIMEOUT);
+                if (++spins > kSpinLimit) {
+                    raise_error(DYPH_ERR_TIMEOUT, 3u);
                     ok = 0;
                     break;
                 }
-                __nanosleep(16);
+                if ((spins & 1023u) == 0u && ld_acquire(&g_device_error) == DYPH_ERR_TIMEOUT) {
+                    ok = 0;
+                    break;
+                }
+                // back-off keeps hundreds of pollers from starving the arrivals
+                __nanosleep(32);
             }
         }
-        __threadfence();
         ok_flag = ok;
     }
     __syncthreads();

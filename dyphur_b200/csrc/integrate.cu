@@ -93,12 +93,21 @@ extern "C" dyph_status dyph_copy_to_device(void* dev_dst, const void* host_src, 
     return DYPH_OK;
 }
 
-extern "C" dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code) {
+extern "C" dyph_status dyph_download_device_error_site(dyph_stream s, uint32_t* out_code, uint32_t* out_site) {
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
-    uint32_t h = 0, zero = 0;
-    DYPH_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h, dyph::g_device_error, sizeof(h), 0, cudaMemcpyDeviceToHost, cs));
+    uint32_t h[2] = {0, 0};
+    const uint32_t zero = 0;
+    DYPH_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h[0], dyph::g_device_error, sizeof(uint32_t), 0, cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h[1], dyph::g_device_error_site, sizeof(uint32_t), 0,
+                                            cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaMemcpyToSymbolAsync(dyph::g_device_error_site, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, cs));
     DYPH_CUDA_TRY(cudaMemcpyToSymbolAsync(dyph::g_device_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, cs));
     DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
-    if (out_code) *out_code = h;
+    if (out_code) *out_code = h[0];
+    if (out_site) *out_site = h[1];
     return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code) {
+    return dyph_download_device_error_site(s, out_code, nullptr);
 }

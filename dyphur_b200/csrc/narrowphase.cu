@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kNpThreads) narrowphase_kernel(const uint2* __
         if (i < np_) {
             const uint2 p = __ldg(&pairs[i]);
             if (p.x < B.v.n && p.y < B.v.n) has = process_pair(B, S, p.x, p.y, c);
-            else raise_error(DYPH_ERR_INVALID);
+            else raise_error(DYPH_ERR_INVALID, 8u);
         }
         uint32_t total;
         const uint32_t excl = block_exclusive_scan<kNpThreads>(has ? 1u : 0u, s_scan, total);

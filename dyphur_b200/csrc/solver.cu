@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kSeqThreads) sequential_solve_kernel(
                 // The smallest unsolved contact is always ready, so a correct
                 // schedule needs at most nc waves.
                 if (wave > nc + 2u) {
-                    raise_error(DYPH_ERR_TIMEOUT);
+                    raise_error(DYPH_ERR_TIMEOUT, 5u);
                     return;
                 }
             }

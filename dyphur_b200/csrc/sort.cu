@@ -72,7 +72,7 @@ __device__ __forceinline__ uint32_t lookback_column(uint32_t* status, uint32_t t
         uint32_t flag = s & ~kLbMask;
         if (flag == 0u) {
             if (++spins > kSpinLimit) {
-                raise_error(DYPH_ERR_TIMEOUT);
+                raise_error(DYPH_ERR_TIMEOUT, 2u);
                 return 0u;
             }
             __nanosleep(32);

@@ -271,6 +271,13 @@ def device_error(stream=None) -> int:
     return int(code.value)
 
 
+def device_error_site(stream=None) -> tuple:
+    """(code, site) of the first device-side error since the last read; both cleared."""
+    code, site = C.c_uint32(), C.c_uint32()
+    check(capi.lib().dyph_download_device_error_site(_stream_ptr(stream), C.byref(code), C.byref(site)))
+    return int(code.value), int(site.value)
+
+
 def state_hash(bodies: DeviceBodies, stream=None) -> int:
     out = torch.zeros(1, dtype=torch.int64, device=bodies.fbuf.device)
     check(capi.lib().dyph_fnv1a64_state(C.byref(bodies.view), _ptr(out), _stream_ptr(stream)))

@@ -133,6 +133,10 @@ dyph_status dyph_device_check(void);
 /* Sticky device-side error word of the library (DYPH_ERR_TIMEOUT etc.), read
  * and cleared. Blocks on the stream. */
 dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code);
+/* The same, plus where the first error was raised: 1 tile look-back, 2 sort
+ * look-back, 3 grid barrier, 5 sequential solve schedule, 6 / 7 tree walk,
+ * 8 narrowphase pair index. Both words are cleared. */
+dyph_status dyph_download_device_error_site(dyph_stream s, uint32_t* out_code, uint32_t* out_site);
 /* Blocking raw copies between host memory and device memory (the Buffer<T>
  * upload / download of compute/include/compute/buffer.hpp:41-49). */
 dyph_status dyph_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, dyph_stream s);
