@@ -6,7 +6,8 @@ import ctypes as C
 from ._lib import load_library
 
 OK, ERR_INVALID, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_CONTACT_OVERFLOW, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_NOMEM, \
-    ERR_NOT_FINITE = range(9)
+    ERR_NOT_FINITE, ERR_TOO_LARGE = range(10)
+SORT_NOALLOC_MAX_KEYS = 262144
 SOLVER_REFERENCE, SOLVER_SEQUENTIAL, SOLVER_COLORED = 0, 1, 2
 
 _fp = C.POINTER(C.c_float)
@@ -59,6 +60,7 @@ _PROTOS = {
     "dyph_integrate": (_st, [C.POINTER(Bodies), C.POINTER(IntegratorParams), _vp]),
     "dyph_sort_workspace_bytes": (C.c_size_t, [C.c_size_t]),
     "dyph_sort_by_key_u64_u32": (_st, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, _vp]),
+    "dyph_sort_by_key_u64_u32_noalloc": (_st, [_vp, _vp, C.c_size_t, _vp]),
     "dyph_sort_u64": (_st, [_vp, C.c_size_t, _vp, C.c_size_t, _vp]),
     "dyph_sort_by_key_u32_u32": (_st, [_vp, _vp, C.c_size_t, C.c_int, _vp, C.c_size_t, _vp]),
     "dyph_broadphase_create": (_st, [C.c_uint32, C.c_uint32, C.POINTER(_vp)]),

@@ -58,6 +58,7 @@ extern "C" const char* dyph_status_string(int status) {
         case DYPH_ERR_NO_DEVICE: return "no sm_100 CUDA device";
         case DYPH_ERR_NOMEM: return "device allocation failed";
         case DYPH_ERR_NOT_FINITE: return "non-finite body state";
+        case DYPH_ERR_TOO_LARGE: return "size exceeds the fixed scratch of a no-allocation entry point";
         default: return "unknown status";
     }
 }

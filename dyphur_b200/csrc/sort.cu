@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "sort.cuh"
@@ -335,5 +336,60 @@ extern "C" dyph_status dyph_sort_u64(uint64_t* keys, size_t n, void* ws, size_t 
 extern "C" dyph_status dyph_sort_by_key_u32_u32(uint32_t* keys, uint32_t* values, size_t n, int key_bits,
                                                 void* ws, size_t ws_bytes, dyph_stream s) {
     return dyph::radix_sort<uint32_t, true>(keys, values, n, key_bits, ws, ws_bytes,
+                                            reinterpret_cast<cudaStream_t>(s));
+}
+
+// ── sort with library-owned scratch ─────────────────────────────────────────
+// The scratch is a file-scope device array sized for DYPH_SORT_NOALLOC_MAX_KEYS
+// 64-bit keys with 32-bit values: histograms, pass counters and look-back
+// status (cleared on the stream by every call), then the alternate key and
+// value buffers. Nothing here calls cudaMalloc or cudaFree.
+namespace dyph {
+namespace {
+
+constexpr size_t kNoAllocMaxKeys = DYPH_SORT_NOALLOC_MAX_KEYS;
+constexpr size_t round256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+constexpr size_t kNoAllocTiles = (kNoAllocMaxKeys + kTile - 1) / kTile;
+constexpr size_t kNoAllocScratchBytes = round256(kMaxPasses * 256 * 4) + round256(kMaxPasses * 4) +
+                                        round256(kMaxPasses * kNoAllocTiles * 256 * 4) +
+                                        round256(kNoAllocMaxKeys * 8) + round256(kNoAllocMaxKeys * 4);
+
+static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+void* g_sort_scratch_ptr[kNoAllocMaxDevices] = {};
+std::mutex g_sort_scratch_mu;
+
+// Per-device set-up, done by the first call with that device current: the
+// array's device address and the small-sort kernel's shared-memory attribute.
+dyph_status noalloc_scratch(void** out) {
+    int dev = 0;
+    DYPH_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return DYPH_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_sort_scratch_mu);
+    if (!g_sort_scratch_ptr[dev]) {
+        void* p = nullptr;
+        DYPH_CUDA_TRY(cudaGetSymbolAddress(&p, g_sort_scratch));
+        DYPH_CUDA_TRY(cudaFuncSetAttribute(small_sort_kernel<uint64_t, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(small_smem_bytes<uint64_t, true>())));
+        g_sort_scratch_ptr[dev] = p;
+    }
+    *out = g_sort_scratch_ptr[dev];
+    return DYPH_OK;
+}
+
+}  // namespace
+}  // namespace dyph
+
+extern "C" dyph_status dyph_sort_by_key_u64_u32_noalloc(uint64_t* keys, uint32_t* values, size_t n, dyph_stream s) {
+    if (n > dyph::kNoAllocMaxKeys) return DYPH_ERR_TOO_LARGE;
+    if (n <= 1) return DYPH_OK;
+    if (!keys || !values) return DYPH_ERR_INVALID;
+    void* scratch = nullptr;
+    const dyph_status st = dyph::noalloc_scratch(&scratch);
+    if (st != DYPH_OK) return st;
+    if (dyph::ws_bytes<uint64_t>(n, 8) > dyph::kNoAllocScratchBytes) return DYPH_ERR_TOO_LARGE;
+    return dyph::radix_sort<uint64_t, true>(keys, values, n, 64, scratch, dyph::kNoAllocScratchBytes,
                                             reinterpret_cast<cudaStream_t>(s));
 }

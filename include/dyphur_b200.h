@@ -37,7 +37,8 @@ typedef enum dyph_status {
     DYPH_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
     DYPH_ERR_NO_DEVICE = 6,        /* no CUDA device / not an sm_100 device */
     DYPH_ERR_NOMEM = 7,            /* device allocation failed */
-    DYPH_ERR_NOT_FINITE = 8        /* NaN / Inf found in body state */
+    DYPH_ERR_NOT_FINITE = 8,       /* NaN / Inf found in body state */
+    DYPH_ERR_TOO_LARGE = 9         /* size above a fixed-scratch entry point's maximum */
 } dyph_status;
 
 /* Mirrors BodyView (core/include/core/body.hpp:30-46). */
@@ -155,6 +156,29 @@ dyph_status dyph_sort_by_key_u64_u32(uint64_t* keys, uint32_t* values, size_t n,
 dyph_status dyph_sort_u64(uint64_t* keys, size_t n, void* workspace, size_t workspace_bytes, dyph_stream s);
 dyph_status dyph_sort_by_key_u32_u32(uint32_t* keys, uint32_t* values, size_t n, int key_bits, void* workspace,
                                      size_t workspace_bytes, dyph_stream s);
+
+/* Sort by key without any device allocation and without a caller workspace.
+ * No counterpart in the reference: its sort_by_key (compute/include/compute/
+ * sort.hpp:29-80) is an in-place bitonic sort that needs no scratch. This
+ * radix sort needs scratch, which dyph_sort_by_key_u64_u32 takes from the
+ * caller and this entry point keeps inside the library.
+ *
+ * For callers that must not allocate device memory while they run — a host
+ * engine whose frame callback owns the device memory budget, or a process at
+ * its memory limit, where cudaMalloc / cudaFree would fail or synchronise the
+ * device in the middle of a frame — and that cannot hand in a workspace.
+ * Scratch is a fixed library-owned device array of about 4.2 MB, sized for
+ * DYPH_SORT_NOALLOC_MAX_KEYS keys; larger n returns DYPH_ERR_TOO_LARGE and
+ * touches nothing. The first call on each device (with that device current)
+ * looks the array up and sets the sort kernels' attributes; make that first
+ * call before any stream capture. The scratch counters are cleared on the
+ * stream at the start of every call.
+ *
+ * There is one scratch array per device: calls that overlap on a device (two
+ * streams, two host threads, or two graph launches in flight together) race
+ * on it and give wrong results. Serialise them, e.g. on one stream. */
+#define DYPH_SORT_NOALLOC_MAX_KEYS 262144u
+dyph_status dyph_sort_by_key_u64_u32_noalloc(uint64_t* keys, uint32_t* values, size_t n, dyph_stream s);
 
 /* ── broadphase — replaces class Broadphase
  *    (core/include/core/broadphase.hpp:50-111, core/src/broadphase.cpp:82-377).
