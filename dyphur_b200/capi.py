@@ -8,7 +8,7 @@ from ._lib import load_library
 OK, ERR_INVALID, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_CONTACT_OVERFLOW, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_NOMEM, \
     ERR_NOT_FINITE, ERR_TOO_LARGE = range(10)
 SORT_NOALLOC_MAX_KEYS = 262144
-SOLVER_REFERENCE, SOLVER_SEQUENTIAL, SOLVER_COLORED = 0, 1, 2
+SOLVER_REFERENCE, SOLVER_SEQUENTIAL, SOLVER_COLORED, SOLVER_REFERENCE_ROUNDS = 0, 1, 2, 3
 
 _fp = C.POINTER(C.c_float)
 _up = C.POINTER(C.c_uint32)

@@ -310,3 +310,96 @@ __device__ __forceinline__ int solve_contact(const Bodies& B, const Contact& ct,
 }
 
 }  // namespace dyph
+
+namespace dyph {
+
+// The two bodies of one contact held in registers (index 0 = body a, 1 = body
+// b), so solve_contact's read-modify-writes stay on chip; only the 13 state
+// floats of a dynamic body are written back.
+struct LocalPair {
+    float p[2][3], q[2][4], v[2][3], w[2][3], m[2], I[2][6];
+    __device__ __forceinline__ float& px(uint32_t i) { return p[i][0]; }
+    __device__ __forceinline__ float& py(uint32_t i) { return p[i][1]; }
+    __device__ __forceinline__ float& pz(uint32_t i) { return p[i][2]; }
+    __device__ __forceinline__ float& qw(uint32_t i) { return q[i][0]; }
+    __device__ __forceinline__ float& qx(uint32_t i) { return q[i][1]; }
+    __device__ __forceinline__ float& qy(uint32_t i) { return q[i][2]; }
+    __device__ __forceinline__ float& qz(uint32_t i) { return q[i][3]; }
+    __device__ __forceinline__ float& vx(uint32_t i) { return v[i][0]; }
+    __device__ __forceinline__ float& vy(uint32_t i) { return v[i][1]; }
+    __device__ __forceinline__ float& vz(uint32_t i) { return v[i][2]; }
+    __device__ __forceinline__ float& wx(uint32_t i) { return w[i][0]; }
+    __device__ __forceinline__ float& wy(uint32_t i) { return w[i][1]; }
+    __device__ __forceinline__ float& wz(uint32_t i) { return w[i][2]; }
+    __device__ __forceinline__ float im(uint32_t i) const { return m[i]; }
+    __device__ __forceinline__ float ixx(uint32_t i) const { return I[i][0]; }
+    __device__ __forceinline__ float iyy(uint32_t i) const { return I[i][1]; }
+    __device__ __forceinline__ float izz(uint32_t i) const { return I[i][2]; }
+    __device__ __forceinline__ float ixy(uint32_t i) const { return I[i][3]; }
+    __device__ __forceinline__ float ixz(uint32_t i) const { return I[i][4]; }
+    __device__ __forceinline__ float iyz(uint32_t i) const { return I[i][5]; }
+};
+
+// LocalPair's accessors are non-const; solve_contact takes `const Bodies&`,
+// so it is driven through this thin reference wrapper.
+struct LocalPairRef {
+    LocalPair* s;
+    __device__ __forceinline__ float& px(uint32_t i) const { return s->p[i][0]; }
+    __device__ __forceinline__ float& py(uint32_t i) const { return s->p[i][1]; }
+    __device__ __forceinline__ float& pz(uint32_t i) const { return s->p[i][2]; }
+    __device__ __forceinline__ float& qw(uint32_t i) const { return s->q[i][0]; }
+    __device__ __forceinline__ float& qx(uint32_t i) const { return s->q[i][1]; }
+    __device__ __forceinline__ float& qy(uint32_t i) const { return s->q[i][2]; }
+    __device__ __forceinline__ float& qz(uint32_t i) const { return s->q[i][3]; }
+    __device__ __forceinline__ float& vx(uint32_t i) const { return s->v[i][0]; }
+    __device__ __forceinline__ float& vy(uint32_t i) const { return s->v[i][1]; }
+    __device__ __forceinline__ float& vz(uint32_t i) const { return s->v[i][2]; }
+    __device__ __forceinline__ float& wx(uint32_t i) const { return s->w[i][0]; }
+    __device__ __forceinline__ float& wy(uint32_t i) const { return s->w[i][1]; }
+    __device__ __forceinline__ float& wz(uint32_t i) const { return s->w[i][2]; }
+    __device__ __forceinline__ float im(uint32_t i) const { return s->m[i]; }
+    __device__ __forceinline__ float ixx(uint32_t i) const { return s->I[i][0]; }
+    __device__ __forceinline__ float iyy(uint32_t i) const { return s->I[i][1]; }
+    __device__ __forceinline__ float izz(uint32_t i) const { return s->I[i][2]; }
+    __device__ __forceinline__ float ixy(uint32_t i) const { return s->I[i][3]; }
+    __device__ __forceinline__ float ixz(uint32_t i) const { return s->I[i][4]; }
+    __device__ __forceinline__ float iyz(uint32_t i) const { return s->I[i][5]; }
+};
+
+__device__ __forceinline__ void load_local(const GlobalBodies& B, uint32_t bi, LocalPair& L, int j) {
+    L.p[j][0] = B.px(bi); L.p[j][1] = B.py(bi); L.p[j][2] = B.pz(bi);
+    L.q[j][0] = B.qw(bi); L.q[j][1] = B.qx(bi); L.q[j][2] = B.qy(bi); L.q[j][3] = B.qz(bi);
+    L.v[j][0] = B.vx(bi); L.v[j][1] = B.vy(bi); L.v[j][2] = B.vz(bi);
+    L.w[j][0] = B.wx(bi); L.w[j][1] = B.wy(bi); L.w[j][2] = B.wz(bi);
+    L.m[j] = B.im(bi);
+    L.I[j][0] = B.ixx(bi); L.I[j][1] = B.iyy(bi); L.I[j][2] = B.izz(bi);
+    L.I[j][3] = B.ixy(bi); L.I[j][4] = B.ixz(bi); L.I[j][5] = B.iyz(bi);
+}
+
+__device__ __forceinline__ void store_local(const GlobalBodies& B, uint32_t bi, const LocalPair& L, int j) {
+    B.px(bi) = L.p[j][0]; B.py(bi) = L.p[j][1]; B.pz(bi) = L.p[j][2];
+    B.qw(bi) = L.q[j][0]; B.qx(bi) = L.q[j][1]; B.qy(bi) = L.q[j][2]; B.qz(bi) = L.q[j][3];
+    B.vx(bi) = L.v[j][0]; B.vy(bi) = L.v[j][1]; B.vz(bi) = L.v[j][2];
+    B.wx(bi) = L.w[j][0]; B.wy(bi) = L.w[j][1]; B.wz(bi) = L.w[j][2];
+}
+
+// solve_contact on register copies of the two bodies: the same arithmetic in
+// the same order, so the results are bit-identical to the global-memory form.
+__device__ __forceinline__ int solve_contact_reg(const GlobalBodies& B, const Contact& ct, float mu, float& lc,
+                                                 float dt) {
+    if (ct.depth <= 0.f || ct.depth - lc <= 1e-6f) return kSolveSkipped;
+    LocalPair L;
+    load_local(B, ct.a, L, 0);
+    load_local(B, ct.b, L, 1);
+    Contact lct = ct;
+    lct.a = 0u;
+    lct.b = 1u;
+    const int res = solve_contact(LocalPairRef{&L}, lct, mu, lc, dt);
+    if (res == kSolveDone) {
+        if (L.m[0] != 0.f) store_local(B, ct.a, L, 0);
+        if (L.m[1] != 0.f) store_local(B, ct.b, L, 1);
+    }
+    return res;
+}
+
+}  // namespace dyph

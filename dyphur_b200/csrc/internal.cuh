@@ -72,7 +72,11 @@ struct dyph_xpbd {
     uint64_t* bmask = nullptr;      // [max_bodies] JP used-colour masks
     uint32_t* blast = nullptr;      // [max_bodies] last contact seen per body (sequential path)
     uint32_t* meta = nullptr;       // solver control words (see solver.cu)
-    int coop_blocks = 0;            // co-resident blocks of the coloured kernel
+    uint32_t* body_list = nullptr;  // [64 max_bodies] dataflow path: contact entries of each body
+    uint32_t* link = nullptr;       // [2 max_contacts] dataflow path: list predecessor of each entry
+    uint64_t* cmask = nullptr;      // [2 max_contacts] dataflow path: published colour masks
+    int coop_blocks = 0;            // co-resident blocks of the round-synchronous coloured kernel
+    int flow_blocks = 0;            // co-resident blocks of the dataflow kernel
 };
 
 namespace dyph {

@@ -40,6 +40,7 @@ constexpr int kMetaDeferred = 6;
 constexpr int kMetaRounds = 7;    // JP rounds of the last coloured solve (diagnostic)
 constexpr int kMetaListLen = 8;   // [8, 11) work-list lengths of the JP rounds
 constexpr int kMetaTailRemaining = 11;
+constexpr int kMetaFlowPath = 12;  // 1 when the last coloured solve ran the dataflow kernel
 constexpr int kMetaTime = 144;    // [144, 154) phase timestamps (ns) of the coloured solve
 constexpr int kMetaColorCount = 16;   // [16, 80)
 constexpr int kMetaColorCursor = 80;  // [80, 144)
@@ -65,7 +66,8 @@ __device__ __forceinline__ uint32_t contact_count(const dyph_contacts& cv) {
 }
 
 __device__ __forceinline__ bool wants_sequential(int mode, uint32_t nc) {
-    return mode == DYPH_SOLVER_SEQUENTIAL || (mode == DYPH_SOLVER_REFERENCE && nc <= kSerialThreshold);
+    return mode == DYPH_SOLVER_SEQUENTIAL ||
+           ((mode == DYPH_SOLVER_REFERENCE || mode == DYPH_SOLVER_REFERENCE_ROUNDS) && nc <= kSerialThreshold);
 }
 
 __device__ __forceinline__ void renorm_body(const GlobalBodies& B, uint32_t i, int times) {
@@ -78,6 +80,7 @@ __device__ __forceinline__ void renorm_body(const GlobalBodies& B, uint32_t i, i
 }  // namespace dyph
 
 #include "solver_color.cuh"
+#include "solver_flow.cuh"
 
 namespace dyph {
 namespace {
@@ -219,6 +222,20 @@ int coop_block_count() {
     return blocks;
 }
 
+// Co-resident blocks of the dataflow kernel: as many as fit, at most 4 per SM
+// (more threads -> fewer contacts per thread; more blocks -> dearer barriers).
+int flow_block_count() {
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flow_solve_kernel, kFlowThreads, 0);
+        blocks = sms * std::max(1, std::min(per_sm, 4));
+    }
+    return blocks;
+}
+
 }  // namespace
 
 dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bodies, float friction,
@@ -237,19 +254,23 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
               cudaMalloc(&sv->order, mc * 4) == cudaSuccess && cudaMalloc(&sv->pred, 2 * mc * 4) == cudaSuccess &&
               cudaMalloc(&sv->done, mc * 4) == cudaSuccess && cudaMalloc(&sv->bpri, 3 * mb * 8) == cudaSuccess &&
               cudaMalloc(&sv->bmask, mb * 8) == cudaSuccess && cudaMalloc(&sv->blast, 2 * (mb + 1) * 4) == cudaSuccess &&
-              cudaMalloc(&sv->meta, kMetaWords * 4) == cudaSuccess;
+              cudaMalloc(&sv->meta, kMetaWords * 4) == cudaSuccess &&
+              cudaMalloc(&sv->body_list, mb * kBodySlots * 4) == cudaSuccess &&
+              cudaMalloc(&sv->link, 2 * mc * 4) == cudaSuccess && cudaMalloc(&sv->cmask, 2 * mc * 8) == cudaSuccess;
     if (!ok) {
         xpbd_destroy(sv);
         return DYPH_ERR_NOMEM;
     }
     sv->coop_blocks = coop_block_count();
+    sv->flow_blocks = flow_block_count();
     *out = sv;
     return DYPH_OK;
 }
 
 void xpbd_destroy(dyph_xpbd* sv) {
     if (!sv) return;
-    void* ptrs[] = {sv->lambda, sv->color, sv->order, sv->pred, sv->done, sv->bpri, sv->bmask, sv->blast, sv->meta};
+    void* ptrs[] = {sv->lambda, sv->color, sv->order, sv->pred, sv->done, sv->bpri, sv->bmask, sv->blast, sv->meta,
+                    sv->body_list, sv->link, sv->cmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sv;
@@ -265,6 +286,13 @@ dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_
     int mode = static_cast<int>(sv->mode);
     int n_iters = sv->n_iters;
     float mu = sv->friction;
+    // Per-body contact counts live in `blast`, JP rounds in `order`: the
+    // kernels that also use them run only after this one declined the frame.
+    FlowBufs F{sv->blast, sv->body_list, sv->link, reinterpret_cast<unsigned long long*>(sv->cmask), sv->order,
+               sv->done};
+    void* fargs[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &F, &sv->meta};
+    DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(flow_solve_kernel), dim3(sv->flow_blocks),
+                                              dim3(kFlowThreads), fargs, 0, s));
     void* args[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &sv->order, &sv->pred,
                     &sv->bpri, &sv->bmask, &sv->meta};
     DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(color_solve_kernel), dim3(sv->coop_blocks),
@@ -287,7 +315,8 @@ extern "C" dyph_status dyph_xpbd_create(int32_t n_iters, uint32_t max_contacts, 
 }
 extern "C" void dyph_xpbd_destroy(dyph_xpbd* sv) { xpbd_destroy(sv); }
 extern "C" dyph_status dyph_xpbd_set_mode(dyph_xpbd* sv, dyph_solver_mode mode) {
-    if (!sv || (mode != DYPH_SOLVER_REFERENCE && mode != DYPH_SOLVER_SEQUENTIAL && mode != DYPH_SOLVER_COLORED))
+    if (!sv || (mode != DYPH_SOLVER_REFERENCE && mode != DYPH_SOLVER_SEQUENTIAL && mode != DYPH_SOLVER_COLORED &&
+                mode != DYPH_SOLVER_REFERENCE_ROUNDS))
         return DYPH_ERR_INVALID;
     sv->mode = mode;
     return DYPH_OK;

@@ -101,6 +101,8 @@ __global__ void __launch_bounds__(kColorThreads) color_solve_kernel(dyph_contact
     __shared__ uint32_t s_wbase[kColorThreads / 32];
     const uint32_t nc = contact_count(cv);
     if (nc == 0 || wants_sequential(mode, nc)) return;
+    // Runs when asked for, or when the dataflow kernel had too many contacts per thread.
+    if (mode != DYPH_SOLVER_REFERENCE_ROUNDS && ld_acquire(&meta[kMetaDecision]) != 3u) return;
     const uint32_t nb = B.v.n;
     const uint32_t nblk = gridDim.x;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,0 +1,322 @@
+// Dataflow XPBD path (included by solver.cu): the reference's Jones–Plassmann
+// colouring and colour-ordered Gauss–Seidel sweep, scheduled per contact
+// instead of per round / per colour.
+//
+// Facts it rests on (xpbd_solver.cpp:645-732):
+//   * priorities hash(k) << 32 | k are distinct and fixed across rounds, and a
+//     contact wins a round exactly when every uncoloured contact sharing one of
+//     its dynamic bodies has a lower priority. So every higher-priority
+//     neighbour is coloured before it and no lower-priority one is: its colour
+//     is the lowest colour unused by its higher-priority neighbours (greedy
+//     colouring in priority order), and its round is the longest chain of
+//     higher-priority neighbours ending at it.
+//   * the sweep solves the contacts of one body in ascending colour order, and
+//     contacts that share no dynamic body commute exactly.
+// So each dynamic body gets its contact list sorted by priority (colouring) and
+// then by colour (sweep), and a contact waits only for its predecessor on the
+// lists of its two bodies. Published cells are write-once (0 = not yet), so
+// the colouring polls them with relaxed loads; the sweep hands body state on
+// with release / acquire. Every thread works through its own contacts in
+// priority (then colour) order, all threads are co-resident (cooperative
+// launch) and a warp never blocks on one lane, so the highest-priority
+// (lowest-colour) unfinished contact can always run: no deadlock.
+#pragma once
+
+namespace dyph {
+namespace {
+
+constexpr int kFlowThreads = 256;
+constexpr int kFlowItems = 16;     // contacts per thread; more -> the round-synchronous kernel
+constexpr int kBodySlots = 64;     // list slots per body: a body with more contacts needs > 64 colours
+constexpr uint32_t kNoLink = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const unsigned long long* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+struct FlowBufs {
+    uint32_t* body_cnt;          // [nb] contacts on each dynamic body
+    uint32_t* body_list;         // [nb * kBodySlots] entries (contact << 1 | side)
+    uint32_t* link;              // [2 nc] predecessor entry of each entry on its body's list
+    unsigned long long* cmask;   // [2 nc] colours used on the entry's body up to and including it
+    uint32_t* cround;            // [nc] JP round + 1 of each contact
+    uint32_t* done;              // [nc] last sweep iteration (1-based) that finished the contact
+};
+
+// Sort a thread's items (at most kFlowItems) by key, ascending.
+__device__ __forceinline__ void sort_items(uint32_t* item, uint32_t* key, int n) {
+    for (int i = 1; i < n; ++i) {
+        const uint32_t v = item[i], kv = key[i];
+        int j = i;
+        while (j > 0 && key[j - 1] > kv) {
+            item[j] = item[j - 1];
+            key[j] = key[j - 1];
+            --j;
+        }
+        item[j] = v;
+        key[j] = kv;
+    }
+}
+
+// Link every dynamic body's list in ascending key order, key = ~hash (i.e.
+// descending priority) or the colour.
+template <bool BY_COLOR>
+__device__ __forceinline__ void link_lists(const FlowBufs& F, uint32_t nb, const uint32_t* color, uint32_t gtid,
+                                           uint32_t gstride) {
+    uint32_t ent[kBodySlots], key[kBodySlots];
+    for (uint32_t x = gtid; x < nb; x += gstride) {
+        const uint32_t m = F.body_cnt[x];
+        if (m == 0u || m > static_cast<uint32_t>(kBodySlots)) continue;
+        const uint32_t* L = F.body_list + static_cast<size_t>(x) * kBodySlots;
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t e = L[i];
+            ent[i] = e;
+            key[i] = BY_COLOR ? color[e >> 1] : ~hash_u32(e >> 1);
+        }
+        sort_items(ent, key, static_cast<int>(m));
+        F.link[ent[0]] = kNoLink;
+        for (uint32_t i = 1; i < m; ++i) F.link[ent[i]] = ent[i - 1];
+    }
+}
+
+__device__ __forceinline__ uint32_t block_max(uint32_t v, uint32_t* smem) {
+    for (int d = 16; d > 0; d >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, d));
+    if ((threadIdx.x & 31) == 0) smem[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t r = 0;
+    for (int w = 0; w < kFlowThreads / 32; ++w) r = max(r, smem[w]);
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts cv, GlobalBodies B, int mode,
+                                                                  int n_iters, float mu, float dt,
+                                                                  float* __restrict__ lambda,
+                                                                  uint32_t* __restrict__ color, FlowBufs F,
+                                                                  uint32_t* __restrict__ meta) {
+    __shared__ uint32_t s_red[kFlowThreads / 32];
+    const uint32_t nc = contact_count(cv);
+    if (nc == 0 || wants_sequential(mode, nc) || mode == DYPH_SOLVER_REFERENCE_ROUNDS) return;
+    const uint32_t gstride = gridDim.x * blockDim.x;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (nc > static_cast<uint32_t>(kFlowItems) * gstride) {  // too many contacts per thread
+        if (gtid == 0) meta[kMetaDecision] = 3u;
+        return;
+    }
+    const uint32_t nb = B.v.n;
+    const uint32_t nblk = gridDim.x;
+    uint32_t* bar = meta + kMetaBarrier;
+    stamp(meta, gtid, 0);
+
+    // ── set-up: clear, then put every contact on its dynamic bodies' lists ──
+    for (uint32_t x = gtid; x < nb; x += gstride) F.body_cnt[x] = 0u;
+    for (uint32_t k = gtid; k < nc; k += gstride) {
+        F.cmask[2 * k] = 0ull;
+        F.cmask[2 * k + 1] = 0ull;
+        F.cround[k] = 0u;
+        F.done[k] = 0u;
+        lambda[k] = 0.f;
+        color[k] = kUncolored;
+    }
+    if (!grid_barrier(bar, nblk)) return;
+    for (uint32_t k = gtid; k < nc; k += gstride) {
+        const uint32_t a = cv.body_a[k], b = cv.body_b[k];
+        if (B.im(a) != 0.f) {
+            const uint32_t s = atomicAdd(&F.body_cnt[a], 1u);
+            if (s < static_cast<uint32_t>(kBodySlots)) F.body_list[static_cast<size_t>(a) * kBodySlots + s] = 2u * k;
+            else meta[kMetaOverflow] = 1u;  // > 64 contacts on a body: > 64 colours
+        }
+        if (B.im(b) != 0.f) {
+            const uint32_t s = atomicAdd(&F.body_cnt[b], 1u);
+            if (s < static_cast<uint32_t>(kBodySlots)) F.body_list[static_cast<size_t>(b) * kBodySlots + s] = 2u * k + 1u;
+            else meta[kMetaOverflow] = 1u;
+        }
+    }
+    if (!grid_barrier(bar, nblk)) return;
+    if (ld_acquire(&meta[kMetaOverflow]) != 0u) {  // serial fallback (xpbd_solver.cpp:690-693)
+        if (gtid == 0) meta[kMetaDecision] = 1u;
+        return;
+    }
+    link_lists<false>(F, nb, color, gtid, gstride);
+    if (!grid_barrier(bar, nblk)) return;
+    stamp(meta, gtid, 1);
+
+    // ── colouring: greedy in priority order, each contact after its list predecessors ──
+    // Lanes of a warp take contacts far apart (position lane * warps + warp),
+    // so they rarely wait on one another. The warp polls in lock step: every
+    // pass each lane checks its current contact once and finishes it if its
+    // predecessors are published, so no lane ever blocks its warp.
+    const uint32_t n_warps = gstride / 32u;
+    const uint32_t pos = (threadIdx.x & 31u) * n_warps + (gtid >> 5);
+    uint32_t item[kFlowItems], key[kFlowItems];
+    int n_items = 0;
+    for (uint32_t k = pos; k < nc; k += gstride) {
+        item[n_items] = k;
+        key[n_items] = ~hash_u32(k);
+        ++n_items;
+    }
+    sort_items(item, key, n_items);
+    uint32_t my_max_color = 0, my_rounds = 0;
+    {
+        int cur = 0;
+        bool have = false;
+        uint32_t k = 0, la = kNoLink, lb = kNoLink, ra = 0, rb = 0;
+        bool da = false, db = false;
+        uint64_t ma = 0, mb = 0;
+        uint32_t idle = 0;
+        while (__any_sync(0xffffffffu, cur < n_items)) {
+            bool progressed = false;
+            if (cur < n_items) {
+                if (!have) {
+                    k = item[cur];
+                    const uint32_t a = cv.body_a[k], b = cv.body_b[k];
+                    da = B.im(a) != 0.f;
+                    db = B.im(b) != 0.f;
+                    la = da ? F.link[2 * k] : kNoLink;
+                    lb = db ? F.link[2 * k + 1] : kNoLink;
+                    ma = mb = 0;
+                    ra = rb = 0;
+                    have = true;
+                }
+                if (la != kNoLink) {
+                    if (ma == 0) ma = ld_relaxed_u64(&F.cmask[la]);
+                    if (ra == 0) ra = ld_relaxed_u32(&F.cround[la >> 1]);
+                }
+                if (lb != kNoLink) {
+                    if (mb == 0) mb = ld_relaxed_u64(&F.cmask[lb]);
+                    if (rb == 0) rb = ld_relaxed_u32(&F.cround[lb >> 1]);
+                }
+                if ((la == kNoLink || (ma != 0 && ra != 0)) && (lb == kNoLink || (mb != 0 && rb != 0))) {
+                    const uint64_t used = ma | mb;
+                    uint64_t bit;
+                    if (~used == 0ull) {
+                        bit = ~0ull;  // > 64 colours at a body: publish anyway so the lists drain
+                        meta[kMetaOverflow] = 1u;
+                    } else {
+                        const uint32_t col = static_cast<uint32_t>(__ffsll(static_cast<long long>(~used)) - 1);
+                        bit = 1ull << col;
+                        color[k] = col;
+                        my_max_color = max(my_max_color, col);
+                    }
+                    const uint32_t round = max(ra, rb);  // predecessors store round + 1
+                    my_rounds = max(my_rounds, round + 1u);
+                    st_relaxed_u32(&F.cround[k], round + 1u);
+                    if (da) st_relaxed_u64(&F.cmask[2 * k], ma | bit);
+                    if (db) st_relaxed_u64(&F.cmask[2 * k + 1], mb | bit);
+                    ++cur;
+                    have = false;
+                    progressed = true;
+                }
+            }
+            if (__any_sync(0xffffffffu, progressed)) {
+                idle = 0;
+            } else {
+                if (++idle > kSpinLimit) {
+                    raise_error(DYPH_ERR_TIMEOUT, 9u);
+                    break;
+                }
+                if ((idle & 1023u) == 0u && ld_relaxed_u32(&g_device_error) == DYPH_ERR_TIMEOUT) break;
+                __nanosleep(32);
+            }
+        }
+    }
+    {
+        const uint32_t bm = block_max(my_max_color, s_red);
+        const uint32_t br = block_max(my_rounds, s_red);
+        if (threadIdx.x == 0) {
+            atomicMax(&meta[kMetaMaxColor], bm);
+            atomicMax(&meta[kMetaRounds], br);
+        }
+    }
+    if (!grid_barrier(bar, nblk)) return;
+    // JP stops after MAX_ROUNDS rounds (xpbd_solver.cpp:645): a contact whose
+    // round index reaches it is left uncoloured -> serial fallback.
+    if (ld_acquire(&meta[kMetaOverflow]) != 0u || ld_acquire(&meta[kMetaRounds]) > kMaxRounds ||
+        ld_relaxed_u32(&g_device_error) != 0u) {
+        if (gtid == 0) meta[kMetaDecision] = 1u;
+        return;
+    }
+    stamp(meta, gtid, 2);
+    link_lists<true>(F, nb, color, gtid, gstride);
+    for (int i = 0; i < n_items; ++i) key[i] = color[item[i]];
+    sort_items(item, key, n_items);
+    if (!grid_barrier(bar, nblk)) return;
+    stamp(meta, gtid, 3);
+
+    // ── sweeps: each contact after the lower-colour contacts of its two bodies ──
+    bool deferred_any = false;
+    for (int iter = 0; iter < n_iters; ++iter) {
+        if (iter == 0 || deferred_any) {
+            const uint32_t pass = static_cast<uint32_t>(iter) + 1u;
+            int cur = 0;
+            bool have = false, ready_a = false, ready_b = false;
+            uint32_t k = 0, la = kNoLink, lb = kNoLink;
+            uint32_t idle = 0;
+            while (__any_sync(0xffffffffu, cur < n_items)) {
+                bool progressed = false;
+                if (cur < n_items) {
+                    if (!have) {
+                        k = item[cur];
+                        la = B.im(cv.body_a[k]) != 0.f ? F.link[2 * k] : kNoLink;
+                        lb = B.im(cv.body_b[k]) != 0.f ? F.link[2 * k + 1] : kNoLink;
+                        ready_a = la == kNoLink;
+                        ready_b = lb == kNoLink;
+                        have = true;
+                    }
+                    if (!ready_a) ready_a = ld_acquire(&F.done[la >> 1]) >= pass;
+                    if (!ready_b) ready_b = ld_acquire(&F.done[lb >> 1]) >= pass;
+                    if (ready_a && ready_b) {
+                        const Contact ct = load_contact(cv, k);
+                        float lc = lambda[k];
+                        if (solve_contact_reg(B, ct, mu, lc, dt) == kSolveDeferred) meta[kMetaDeferred] = 1u;
+                        lambda[k] = lc;
+                        st_release(&F.done[k], pass);
+                        ++cur;
+                        have = false;
+                        progressed = true;
+                    }
+                }
+                if (__any_sync(0xffffffffu, progressed)) {
+                    idle = 0;
+                } else {
+                    if (++idle > kSpinLimit) {
+                        raise_error(DYPH_ERR_TIMEOUT, 10u);
+                        break;
+                    }
+                    if ((idle & 1023u) == 0u && ld_relaxed_u32(&g_device_error) == DYPH_ERR_TIMEOUT) break;
+                    __nanosleep(32);
+                }
+            }
+            if (!grid_barrier(bar, nblk)) return;
+            deferred_any = ld_acquire(&meta[kMetaDeferred]) != 0u;
+        }
+        if (!deferred_any) {
+            // Remaining iterations only renormalise: apply them all now.
+            for (uint32_t i = gtid; i < nb; i += gstride) renorm_body(B, i, n_iters - iter);
+            break;
+        }
+        for (uint32_t i = gtid; i < nb; i += gstride) renorm_body(B, i, 1);
+        if (!grid_barrier(bar, nblk)) return;
+    }
+    stamp(meta, gtid, 4);
+    if (gtid == 0) {
+        meta[kMetaFlowPath] = 1u;
+        meta[kMetaDecision] = 2u;
+    }
+}
+
+}  // namespace
+}  // namespace dyph

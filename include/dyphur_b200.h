@@ -123,7 +123,13 @@ typedef enum dyph_solver_mode {
     /* Jones–Plassmann colours at every contact count (no sequential threshold):
      * the fast mode for batched small scenes; its drift against the
      * sequential order is measured, not zero. */
-    DYPH_SOLVER_COLORED = 2
+    DYPH_SOLVER_COLORED = 2,
+    /* As DYPH_SOLVER_REFERENCE, with the colouring and sweeps run round by
+     * round and colour by colour behind grid barriers (the reference's own
+     * schedule) instead of the per-contact dataflow schedule. Same results;
+     * the coloured modes use this schedule by themselves when a frame has more
+     * than 16 contacts per resident thread. */
+    DYPH_SOLVER_REFERENCE_ROUNDS = 3
 } dyph_solver_mode;
 
 /* ── library ──────────────────────────────────────────────────────────────── */

@@ -885,7 +885,7 @@ static void solve(world* w, int mode) { /* XpbdSolver::solve, :603-733 */
     uint32_t nc = w->nc;
     w->colored_last = 0;
     if (nc == 0) return;
-    if (mode == DYO_SOLVER_SERIAL || nc <= 256u) { run_serial(w, nc); return; }
+    if (mode == DYO_SOLVER_SERIAL || (mode == DYO_SOLVER_REFERENCE && nc <= 256u)) { run_serial(w, nc); return; }
     uint32_t n_colors = jp_color(w, nc);
     if (n_colors == 0) { run_serial(w, nc); return; }
     w->colored_last = 1;

@@ -20,7 +20,7 @@ ORACLE_SO = os.path.join(HERE, "_build", "libdyphur_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libdyphur_ref.so")
 
 STAGE_INTEGRATE, STAGE_BROADPHASE, STAGE_NARROWPHASE, STAGE_SOLVE = 1, 2, 3, 4
-SOLVER_REFERENCE, SOLVER_SERIAL = 0, 1
+SOLVER_REFERENCE, SOLVER_SERIAL, SOLVER_COLORED = 0, 1, 2
 
 
 class _Scene(ctypes.Structure):

@@ -48,6 +48,8 @@ typedef struct dyo_scene {
 /* Solver modes. */
 #define DYO_SOLVER_REFERENCE 0  /* serial when n_con <= 256, else Jones–Plassmann colouring */
 #define DYO_SOLVER_SERIAL 1     /* XpbdSolver::set_force_serial(true) */
+#define DYO_SOLVER_COLORED 2    /* colouring at every contact count: the library's coloured mode, no reference
+                                 * counterpart (the restatement only drops the n_con <= 256 test) */
 
 /* Stages for *_run_stage. */
 #define DYO_STAGE_INTEGRATE 1

@@ -100,6 +100,8 @@ struct RefWorld {
     }
 
     int stage(int st, int mode) {
+        // The reference has no always-coloured mode (DYO_SOLVER_COLORED).
+        if (mode != DYO_SOLVER_REFERENCE && mode != DYO_SOLVER_SERIAL) return -2;
         BodyView bv = bs.view();
         ShapeView sv = ss.view();
         switch (st) {

@@ -93,11 +93,13 @@ def test_world_determinism_golden(dev):
     assert w.hash() == 0xcbcd209c3665c818
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 3])
 def test_world_blocks_300_frames(dev, oracle_mod, mode):
+    """Modes 0 (reference: dataflow colouring above 256 contacts), 1 (sequential)
+    and 3 (round-synchronous colouring, checked against the reference mode)."""
     s = scenes.stress_blocks()
     o = oracle_mod.World(s)
-    assert o.step(300, mode) == 0
+    assert o.step(300, 0 if mode == 3 else mode) == 0
     w = dev.World(s, mode=mode)
     w.step(300)
     st = w.stats()
@@ -177,3 +179,42 @@ def test_sort_by_key_u64(dev, n):
     order = np.argsort(keys.view(np.uint64), kind="stable")
     assert np.array_equal(kd.cpu().numpy(), keys[order])
     assert np.array_equal(vd.cpu().numpy(), vals[order])
+
+
+def with_static_box(s, pos=(0.0, -0.6, 0.0)):
+    """The scene plus a second static box overlapping the ground: their contact
+    has w_total == 0, so it is deferred in every iteration and every solver
+    iteration sweeps again."""
+    import dataclasses
+    n = s.n_bodies
+    cat = lambda a, row: np.concatenate([a, np.asarray(row, a.dtype).reshape((1,) + a.shape[1:])])
+    return dataclasses.replace(
+        s, pos=cat(s.pos, pos), rot=cat(s.rot, (1, 0, 0, 0)), vel=cat(s.vel, (0, 0, 0)),
+        ang=cat(s.ang, (0, 0, 0)), mass=cat(s.mass, 0.0), inertia=cat(s.inertia, np.eye(3).ravel()),
+        shape=cat(s.shape, s.shape[n - 1]), flags=cat(s.flags, s.flags[n - 1]),
+        targets=cat(s.targets, (0, 0, 0)), body_offset=np.array([0, n + 1], s.body_offset.dtype))
+
+
+@pytest.mark.parametrize("mode", [0, 3])
+def test_static_static_contact_sweeps_every_iteration(dev, oracle_mod, mode):
+    s = with_static_box(scenes.stress_blocks())
+    assert s.n_bodies == 1026
+    o = oracle_mod.World(s)
+    w = dev.World(s, mode=mode)
+    for frames in (40, 80):
+        assert o.step(frames, 0) == 0
+        w.step(frames)
+        assert np.array_equal(bits(w.state()), bits(o.state()))
+    assert w.stats()["status"] == 0 and dev.device_error() == 0
+
+
+@pytest.mark.parametrize("scene", ["determinism", "blocks"])
+def test_colored_mode_below_threshold(dev, oracle_mod, scene):
+    """Mode 2 colours at every contact count, including frames with <= 256
+    contacts that the reference mode solves sequentially."""
+    s = scenes.determinism((3, 3, 3)) if scene == "determinism" else scenes.stress_blocks()
+    o = oracle_mod.World(s)
+    w = dev.World(s, mode=2)
+    assert o.step(90, oracle_mod.SOLVER_COLORED) == 0
+    w.step(90)
+    assert np.array_equal(bits(w.state()), bits(o.state()))
