@@ -271,35 +271,27 @@ __global__ void __launch_bounds__(kBpThreads) pair_find_kernel(uint32_t n_u, Bvh
     });
 }
 
-// Pass 2, one thread per body in body order: sort the bucket, place it with a
-// block scan + decoupled look-back, write it. Buckets that overflowed are
-// rebuilt by a full traversal from the body's own leaf.
+// Pass 2, one thread per body in body order: place each body's pairs with a
+// block scan + decoupled look-back (the counts are final after pass 1, so
+// every tile publishes its aggregate at once), then write them sorted by b.
+// Buckets of up to kMaxPartners are sorted by their own thread; larger ones
+// go to a block queue and each warp ranks one bucket at a time; buckets that
+// overflowed are rebuilt by a full traversal from the body's own leaf.
 __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, BvhBuffers T, uint2* __restrict__ pairs,
                                                                 uint32_t max_pairs, uint32_t* __restrict__ counts,
                                                                 uint32_t* __restrict__ tstatus) {
-    __shared__ uint32_t s_tile, s_excl;
+    __shared__ uint32_t s_tile, s_excl, s_nbig;
     __shared__ uint32_t s_scan[kBpThreads / 32];
+    __shared__ uint32_t s_big[kBpThreads], s_big_off[kBpThreads], s_big_cnt[kBpThreads];
     const int n = static_cast<int>(n_u);
-    if (threadIdx.x == 0) s_tile = atomicAdd(&counts[2], 1u);
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(&counts[2], 1u);
+        s_nbig = 0u;
+    }
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint32_t a = tile * kBpThreads + threadIdx.x;
-    Partners P;
-    P.m = 0;
-    uint32_t cnt = 0;
-    BoxF q{};
-    bool full = false;
-    if (a < n_u) {
-        cnt = T.bucket_cnt[a];
-        if (cnt <= static_cast<uint32_t>(kBucket)) {
-            for (uint32_t i = 0; i < cnt; ++i) partner_insert(P, T.bucket[static_cast<size_t>(a) * kBucket + i]);
-        } else {
-            full = true;
-            const uint32_t leaf = __ldg(&T.inv_sorted[a]);
-            q = unpack_box(__ldg(&T.trav[2 * (n - 1 + static_cast<int>(leaf))]));
-            traverse(T, n, q, a, a, P);
-        }
-    }
+    const uint32_t cnt = a < n_u ? T.bucket_cnt[a] : 0u;
     uint32_t total;
     const uint32_t excl_block = block_exclusive_scan<kBpThreads>(cnt, s_scan, total);
     if (threadIdx.x < 32) {
@@ -315,18 +307,66 @@ __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, Bv
         }
     }
     __syncthreads();
-    if (a >= n_u || cnt == 0) return;
-    uint32_t off = s_excl + excl_block;
-    uint32_t written = 0;
-    while (true) {
+    const uint32_t off = s_excl + excl_block;
+    if (cnt > static_cast<uint32_t>(kMaxPartners) && cnt <= static_cast<uint32_t>(kBucket)) {
+        const uint32_t qi = atomicAdd(&s_nbig, 1u);
+        s_big[qi] = a;
+        s_big_off[qi] = off;
+        s_big_cnt[qi] = cnt;
+    }
+    if (cnt != 0u && cnt <= static_cast<uint32_t>(kMaxPartners)) {
+        Partners P;
+        P.m = 0;
+        for (uint32_t i = 0; i < cnt; ++i) partner_insert(P, T.bucket[static_cast<size_t>(a) * kBucket + i]);
         for (int i = 0; i < P.m; ++i) {
-            const uint32_t pos = off + written + static_cast<uint32_t>(i);
+            const uint32_t pos = off + static_cast<uint32_t>(i);
             if (pos < max_pairs) pairs[pos] = make_uint2(a, P.v[i]);
         }
-        written += static_cast<uint32_t>(P.m);
-        if (!full || written >= cnt || P.m == 0) break;
-        const uint32_t last = P.v[P.m - 1];
-        traverse(T, n, q, a, last, P);
+    } else if (cnt > static_cast<uint32_t>(kBucket)) {
+        Partners P;
+        const uint32_t leaf = __ldg(&T.inv_sorted[a]);
+        const BoxF q = unpack_box(__ldg(&T.trav[2 * (n - 1 + static_cast<int>(leaf))]));
+        traverse(T, n, q, a, a, P);
+        uint32_t written = 0;
+        while (true) {
+            for (int i = 0; i < P.m; ++i) {
+                const uint32_t pos = off + written + static_cast<uint32_t>(i);
+                if (pos < max_pairs) pairs[pos] = make_uint2(a, P.v[i]);
+            }
+            written += static_cast<uint32_t>(P.m);
+            if (written >= cnt || P.m == 0) break;
+            traverse(T, n, q, a, P.v[P.m - 1], P);
+        }
+    }
+    __syncthreads();
+    // Warp-ranked buckets: lane l holds elements l, l+32, ...; each element's
+    // place is the number of smaller partners (the partners are distinct).
+    const uint32_t lane = threadIdx.x & 31u;
+    constexpr int kPer = kBucket / 32;
+    for (uint32_t q = threadIdx.x >> 5; q < s_nbig; q += kBpThreads / 32) {
+        const uint32_t ab = s_big[q], base = s_big_off[q], mb = s_big_cnt[q];
+        uint32_t v[kPer], rank[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const uint32_t i = lane + 32u * j;
+            v[j] = i < mb ? T.bucket[static_cast<size_t>(ab) * kBucket + i] : 0xFFFFFFFFu;
+            rank[j] = 0u;
+        }
+#pragma unroll
+        for (int jj = 0; jj < kPer; ++jj) {
+            for (uint32_t l = 0; l < 32u; ++l) {
+                if (32u * jj + l >= mb) break;  // warp-uniform
+                const uint32_t w = __shfl_sync(0xffffffffu, v[jj], l);
+#pragma unroll
+                for (int j = 0; j < kPer; ++j) rank[j] += (w < v[j]) ? 1u : 0u;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const uint32_t i = lane + 32u * j;
+            const uint32_t pos = base + rank[j];
+            if (i < mb && pos < max_pairs) pairs[pos] = make_uint2(ab, v[j]);
+        }
     }
 }
 

@@ -32,9 +32,9 @@ struct BvhBuffers {
     uint32_t* bucket;       // [n * kBucket] first kBucket partners of body a (unordered)
 };
 
-// Partners kept per body by the Morton-order pass; bodies with more take a
-// second, body-order traversal.
-constexpr int kBucket = 32;
+// Partners kept per body by the Morton-order pass (a multiple of 32); bodies
+// with more take a second, body-order traversal.
+constexpr int kBucket = 128;
 
 }  // namespace dyph
 
@@ -72,7 +72,8 @@ struct dyph_xpbd {
     uint64_t* bmask = nullptr;      // [max_bodies] JP used-colour masks
     uint32_t* blast = nullptr;      // [max_bodies] last contact seen per body (sequential path)
     uint32_t* meta = nullptr;       // solver control words (see solver.cu)
-    uint32_t* body_list = nullptr;  // [64 max_bodies] dataflow path: contact entries of each body
+    uint64_t* body_list = nullptr;  // [64 max_bodies] dataflow path: (key, entry) lists of each body
+    uint32_t* slot = nullptr;       // [2 max_contacts] dataflow path: list slot of each entry
     uint32_t* link = nullptr;       // [2 max_contacts] dataflow path: list predecessor of each entry
     uint64_t* cmask = nullptr;      // [2 max_contacts] dataflow path: published colour masks
     int coop_blocks = 0;            // co-resident blocks of the round-synchronous coloured kernel

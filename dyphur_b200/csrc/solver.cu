@@ -255,7 +255,8 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
               cudaMalloc(&sv->done, mc * 4) == cudaSuccess && cudaMalloc(&sv->bpri, 3 * mb * 8) == cudaSuccess &&
               cudaMalloc(&sv->bmask, mb * 8) == cudaSuccess && cudaMalloc(&sv->blast, 2 * (mb + 1) * 4) == cudaSuccess &&
               cudaMalloc(&sv->meta, kMetaWords * 4) == cudaSuccess &&
-              cudaMalloc(&sv->body_list, mb * kBodySlots * 4) == cudaSuccess &&
+              cudaMalloc(&sv->body_list, mb * kBodySlots * 8) == cudaSuccess &&
+              cudaMalloc(&sv->slot, 2 * mc * 4) == cudaSuccess &&
               cudaMalloc(&sv->link, 2 * mc * 4) == cudaSuccess && cudaMalloc(&sv->cmask, 2 * mc * 8) == cudaSuccess;
     if (!ok) {
         xpbd_destroy(sv);
@@ -270,7 +271,7 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
 void xpbd_destroy(dyph_xpbd* sv) {
     if (!sv) return;
     void* ptrs[] = {sv->lambda, sv->color, sv->order, sv->pred, sv->done, sv->bpri, sv->bmask, sv->blast, sv->meta,
-                    sv->body_list, sv->link, sv->cmask};
+                    sv->body_list, sv->slot, sv->link, sv->cmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sv;
@@ -288,8 +289,8 @@ dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_
     float mu = sv->friction;
     // Per-body contact counts live in `blast`, JP rounds in `order`: the
     // kernels that also use them run only after this one declined the frame.
-    FlowBufs F{sv->blast, sv->body_list, sv->link, reinterpret_cast<unsigned long long*>(sv->cmask), sv->order,
-               sv->done};
+    FlowBufs F{sv->blast, reinterpret_cast<unsigned long long*>(sv->body_list), sv->slot, sv->link,
+               reinterpret_cast<unsigned long long*>(sv->cmask), sv->order, sv->done};
     void* fargs[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &F, &sv->meta};
     DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(flow_solve_kernel), dim3(sv->flow_blocks),
                                               dim3(kFlowThreads), fargs, 0, s));

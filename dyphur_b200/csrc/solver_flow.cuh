@@ -46,10 +46,16 @@ __device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// With a relaxed load that saw a release store before it, this fence makes the
+// writer's earlier stores visible to the loads after it (acquire pattern).
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 struct FlowBufs {
     uint32_t* body_cnt;          // [nb] contacts on each dynamic body
-    uint32_t* body_list;         // [nb * kBodySlots] entries (contact << 1 | side)
+    // [nb * kBodySlots] (key << 32 | entry), entry = contact << 1 | side; the
+    // key half is 0 until the colouring writes the contact's colour there.
+    unsigned long long* body_list;
+    uint32_t* slot;              // [2 nc] list slot of each entry
     uint32_t* link;              // [2 nc] predecessor entry of each entry on its body's list
     unsigned long long* cmask;   // [2 nc] colours used on the entry's body up to and including it
     uint32_t* cround;            // [nc] JP round + 1 of each contact
@@ -71,24 +77,32 @@ __device__ __forceinline__ void sort_items(uint32_t* item, uint32_t* key, int n)
     }
 }
 
-// Link every dynamic body's list in ascending key order, key = ~hash (i.e.
-// descending priority) or the colour.
+// Link every entry to its predecessor on its body's list in ascending key
+// order, key = ~hash (descending priority) or the colour. One thread per
+// contact scans its bodies' lists (at most kBodySlots entries each).
 template <bool BY_COLOR>
-__device__ __forceinline__ void link_lists(const FlowBufs& F, uint32_t nb, const uint32_t* color, uint32_t gtid,
-                                           uint32_t gstride) {
-    uint32_t ent[kBodySlots], key[kBodySlots];
-    for (uint32_t x = gtid; x < nb; x += gstride) {
-        const uint32_t m = F.body_cnt[x];
-        if (m == 0u || m > static_cast<uint32_t>(kBodySlots)) continue;
-        const uint32_t* L = F.body_list + static_cast<size_t>(x) * kBodySlots;
-        for (uint32_t i = 0; i < m; ++i) {
-            const uint32_t e = L[i];
-            ent[i] = e;
-            key[i] = BY_COLOR ? color[e >> 1] : ~hash_u32(e >> 1);
+__device__ __forceinline__ void link_lists(const FlowBufs& F, const dyph_contacts& cv, const GlobalBodies& B,
+                                           uint32_t nc, const uint32_t* color, uint32_t gtid, uint32_t gstride) {
+    for (uint32_t k = gtid; k < nc; k += gstride) {
+        const uint32_t mykey = BY_COLOR ? color[k] : ~hash_u32(k);
+        for (uint32_t side = 0; side < 2u; ++side) {
+            const uint32_t x = side ? cv.body_b[k] : cv.body_a[k];
+            if (B.im(x) == 0.f) continue;
+            const uint32_t e = 2u * k + side;
+            const uint32_t m = min(F.body_cnt[x], static_cast<uint32_t>(kBodySlots));
+            const unsigned long long* L = F.body_list + static_cast<size_t>(x) * kBodySlots;
+            uint32_t best = kNoLink, best_key = 0;
+            for (uint32_t i = 0; i < m; ++i) {
+                const uint64_t v = L[i];
+                const uint32_t e2 = static_cast<uint32_t>(v);
+                const uint32_t key2 = BY_COLOR ? static_cast<uint32_t>(v >> 32) : ~hash_u32(e2 >> 1);
+                if (e2 != e && key2 < mykey && (best == kNoLink || key2 > best_key)) {
+                    best = e2;
+                    best_key = key2;
+                }
+            }
+            F.link[e] = best;
         }
-        sort_items(ent, key, static_cast<int>(m));
-        F.link[ent[0]] = kNoLink;
-        for (uint32_t i = 1; i < m; ++i) F.link[ent[i]] = ent[i - 1];
     }
 }
 
@@ -136,13 +150,21 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
         const uint32_t a = cv.body_a[k], b = cv.body_b[k];
         if (B.im(a) != 0.f) {
             const uint32_t s = atomicAdd(&F.body_cnt[a], 1u);
-            if (s < static_cast<uint32_t>(kBodySlots)) F.body_list[static_cast<size_t>(a) * kBodySlots + s] = 2u * k;
-            else meta[kMetaOverflow] = 1u;  // > 64 contacts on a body: > 64 colours
+            if (s < static_cast<uint32_t>(kBodySlots)) {
+                F.body_list[static_cast<size_t>(a) * kBodySlots + s] = 2u * k;
+                F.slot[2 * k] = s;
+            } else {
+                meta[kMetaOverflow] = 1u;  // > 64 contacts on a body: > 64 colours
+            }
         }
         if (B.im(b) != 0.f) {
             const uint32_t s = atomicAdd(&F.body_cnt[b], 1u);
-            if (s < static_cast<uint32_t>(kBodySlots)) F.body_list[static_cast<size_t>(b) * kBodySlots + s] = 2u * k + 1u;
-            else meta[kMetaOverflow] = 1u;
+            if (s < static_cast<uint32_t>(kBodySlots)) {
+                F.body_list[static_cast<size_t>(b) * kBodySlots + s] = 2u * k + 1u;
+                F.slot[2 * k + 1] = s;
+            } else {
+                meta[kMetaOverflow] = 1u;
+            }
         }
     }
     if (!grid_barrier(bar, nblk)) return;
@@ -150,7 +172,7 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
         if (gtid == 0) meta[kMetaDecision] = 1u;
         return;
     }
-    link_lists<false>(F, nb, color, gtid, gstride);
+    link_lists<false>(F, cv, B, nc, color, gtid, gstride);
     if (!grid_barrier(bar, nblk)) return;
     stamp(meta, gtid, 1);
 
@@ -173,7 +195,7 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
     {
         int cur = 0;
         bool have = false;
-        uint32_t k = 0, la = kNoLink, lb = kNoLink, ra = 0, rb = 0;
+        uint32_t k = 0, a = 0, b = 0, la = kNoLink, lb = kNoLink, ra = 0, rb = 0;
         bool da = false, db = false;
         uint64_t ma = 0, mb = 0;
         uint32_t idle = 0;
@@ -182,7 +204,8 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
             if (cur < n_items) {
                 if (!have) {
                     k = item[cur];
-                    const uint32_t a = cv.body_a[k], b = cv.body_b[k];
+                    a = cv.body_a[k];
+                    b = cv.body_b[k];
                     da = B.im(a) != 0.f;
                     db = B.im(b) != 0.f;
                     la = da ? F.link[2 * k] : kNoLink;
@@ -210,6 +233,13 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
                         bit = 1ull << col;
                         color[k] = col;
                         my_max_color = max(my_max_color, col);
+                        // the colour is the key of the sweep's list order
+                        if (da)
+                            reinterpret_cast<uint32_t*>(F.body_list + static_cast<size_t>(a) * kBodySlots +
+                                                        F.slot[2 * k])[1] = col;
+                        if (db)
+                            reinterpret_cast<uint32_t*>(F.body_list + static_cast<size_t>(b) * kBodySlots +
+                                                        F.slot[2 * k + 1])[1] = col;
                     }
                     const uint32_t round = max(ra, rb);  // predecessors store round + 1
                     my_rounds = max(my_rounds, round + 1u);
@@ -250,7 +280,7 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
         return;
     }
     stamp(meta, gtid, 2);
-    link_lists<true>(F, nb, color, gtid, gstride);
+    link_lists<true>(F, cv, B, nc, color, gtid, gstride);
     for (int i = 0; i < n_items; ++i) key[i] = color[item[i]];
     sort_items(item, key, n_items);
     if (!grid_barrier(bar, nblk)) return;
@@ -264,22 +294,24 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
             int cur = 0;
             bool have = false, ready_a = false, ready_b = false;
             uint32_t k = 0, la = kNoLink, lb = kNoLink;
+            Contact ct{};
             uint32_t idle = 0;
             while (__any_sync(0xffffffffu, cur < n_items)) {
                 bool progressed = false;
                 if (cur < n_items) {
                     if (!have) {
                         k = item[cur];
-                        la = B.im(cv.body_a[k]) != 0.f ? F.link[2 * k] : kNoLink;
-                        lb = B.im(cv.body_b[k]) != 0.f ? F.link[2 * k + 1] : kNoLink;
+                        ct = load_contact(cv, k);
+                        la = B.im(ct.a) != 0.f ? F.link[2 * k] : kNoLink;
+                        lb = B.im(ct.b) != 0.f ? F.link[2 * k + 1] : kNoLink;
                         ready_a = la == kNoLink;
                         ready_b = lb == kNoLink;
                         have = true;
                     }
-                    if (!ready_a) ready_a = ld_acquire(&F.done[la >> 1]) >= pass;
-                    if (!ready_b) ready_b = ld_acquire(&F.done[lb >> 1]) >= pass;
+                    if (!ready_a) ready_a = ld_relaxed_u32(&F.done[la >> 1]) >= pass;
+                    if (!ready_b) ready_b = ld_relaxed_u32(&F.done[lb >> 1]) >= pass;
                     if (ready_a && ready_b) {
-                        const Contact ct = load_contact(cv, k);
+                        if (la != kNoLink || lb != kNoLink) fence_acq_rel_gpu();
                         float lc = lambda[k];
                         if (solve_contact_reg(B, ct, mu, lc, dt) == kSolveDeferred) meta[kMetaDeferred] = 1u;
                         lambda[k] = lc;
