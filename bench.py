@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--frames", type=int, default=600)
+    ap.add_argument("--start-frame", type=int, default=0,
+                    help="step the pile this many frames (untimed) before recording the episode")
     ap.add_argument("--bodies", type=int, default=65536)
     ap.add_argument("--probe-stage", default="solver", choices=STAGES)
     ap.add_argument("--mode", default="reference", choices=["reference", "sequential", "colored"])
@@ -144,8 +146,11 @@ def stage_bytes(stage: str, n: int, pairs: np.ndarray, contacts: np.ndarray) -> 
 
 
 def kernels_per_frame(n: int) -> int:
-    sort = 1 if n <= 4096 else 5  # small in-smem sort, or histogram + 4 onesweep passes
-    return 1 + 1 + sort + 1 + 1 + 1 + 2 + 1  # integrate, morton, sort, build, traverse, narrowphase, solver x2, stats
+    """Library kernels one frame launches (matches the ncu launch list in profiles/)."""
+    sort = 1 if n <= 4096 else 5  # one-block sort, or histogram + 4 onesweep passes
+    # integrate, morton, sort, build, finalize, pair find, pair write, narrowphase,
+    # solver (dataflow, round-synchronous, sequential: two of them return at once), stats
+    return 1 + 1 + sort + 1 + 1 + 1 + 1 + 1 + 3 + 1
 
 
 def peaks() -> tuple[float, str]:
@@ -156,11 +161,15 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def committed_traffic(stage: str):
+def committed_traffic(stage: str, mean_algorithmic_bytes: float):
+    """DRAM bytes per launch of the stage, from the committed ncu capture
+    (profiles/traffic.json), scaled from the captured launch's units to the
+    episode's mean launch by the ratio of algorithmic bytes."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(stage)
+            rec = json.load(f).get(stage)
+        return float(rec["dram_bytes"]) * mean_algorithmic_bytes / float(rec["algorithmic_bytes"])
     except Exception:
         return None
 
@@ -183,6 +192,8 @@ def run_b200(args) -> None:
     scene = scenes.random_pile(args.bodies, seed=2 + rank)  # replicas: one scene per rank
     n = scene.n_bodies
     w = device.World(scene, mode=mode)
+    if args.start_frame > 0:
+        w.step(args.start_frame)
     stage_idx = STAGES.index(args.probe_stage)
     w.capture_episode(args.frames, stage_idx)
     fb = w.bodies.fbuf
@@ -252,12 +263,13 @@ def run_b200(args) -> None:
         bytes_f = stage_bytes(args.probe_stage, n, pairs, contacts)
         achieved = float(bytes_f.sum() / (probe.sum() / 1e3) / 1e9) if probe.sum() > 0 else None
         peak, peak_kind = peaks()
-        traffic = committed_traffic(args.probe_stage)
+        traffic = committed_traffic(args.probe_stage, float(bytes_f.mean())) if len(bytes_f) else None
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "bodies": n, "frames_per_step": args.frames,
+                       "start_frame": args.start_frame,
                        "solver_mode": args.mode, "parallelism": f"replicas{world}",
                        "l2": "working set ~10 MB stays L2-resident within a frame; no flush (each step "
                              "re-simulates from the initial state)",

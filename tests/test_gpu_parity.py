@@ -268,3 +268,14 @@ def test_crowd_scene_bucket_paths(dev, oracle_mod):
     assert per_a[0] > 128 and 32 < per_a[1:9].min() and per_a[1:9].max() <= 128
     assert per_a[9:].max() <= 32
     stage_parity(dev, oracle_mod, s, 0)
+
+
+def test_golden_fixtures(dev):
+    """Final-state hashes and counts the reference build wrote (tests/golden)."""
+    from test_oracle_pins import _golden_cases, _golden_scene
+    for name, g in _golden_cases().items():
+        w = dev.World(_golden_scene(name), mode=g["mode"])
+        w.step(g["frames"])
+        assert f"{w.hash():#018x}" == g["hash"], name
+        st = w.stats()
+        assert st["last_pairs"] == g["pairs"] and st["last_contacts"] == g["contacts"], name

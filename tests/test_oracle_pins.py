@@ -224,3 +224,28 @@ def test_oracle_matches_reference_build_pile(oracle_mod):
         r.step(1)
         assert np.array_equal(o.state().view(np.uint32), r.state().view(np.uint32))
         assert np.array_equal(o.pairs()[0], r.pairs()[0])
+
+
+def _golden_cases():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")) as f:
+        return json.load(f)["cases"]
+
+
+def _golden_scene(name):
+    from dyphur_b200 import scenes
+    if name.startswith("determinism"):
+        return scenes.determinism()
+    if name.startswith("blocks"):
+        return scenes.stress_blocks()
+    return scenes.random_pile(4096, seed=7)
+
+
+def test_restatement_matches_reference_golden_fixtures(oracle_mod):
+    """The C restatement against the fixtures the reference build wrote."""
+    for name, g in _golden_cases().items():
+        w = oracle_mod.World(_golden_scene(name))
+        assert w.step(g["frames"], g["mode"]) == 0
+        assert f"{w.hash():#018x}" == g["hash"], name
+        assert w.pairs()[1] == g["pairs"] and len(w.contacts()[0]) == g["contacts"], name
