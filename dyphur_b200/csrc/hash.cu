@@ -55,7 +55,8 @@ extern "C" dyph_status dyph_xpbd_download_stats(dyph_xpbd* sv, dyph_stream s, ui
     uint32_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     DYPH_CUDA_TRY(cudaMemcpyAsync(meta, sv->meta, sizeof(meta), cudaMemcpyDeviceToHost, cs));
     DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
-    if (path) *path = meta[0];
+    // decision word: 2 coloured; 4 fallback / 5 sequential order run by the dataflow kernel
+    if (path) *path = meta[0] == 4u ? 1u : (meta[0] == 5u ? 0u : meta[0]);
     if (n_colors) *n_colors = meta[0] == 2u ? meta[3] + 1u : 0u;
     if (rounds) *rounds = meta[7];
     return DYPH_OK;

@@ -76,6 +76,13 @@ struct dyph_xpbd {
     uint32_t* slot = nullptr;       // [2 max_contacts] dataflow path: list slot of each entry
     uint32_t* link = nullptr;       // [2 max_contacts] dataflow path: list predecessor of each entry
     uint64_t* cmask = nullptr;      // [2 max_contacts] dataflow path: published colour masks
+    uint64_t* hand = nullptr;       // [2 max_contacts][16] dataflow path: tagged body-state records
+    uint32_t* tail = nullptr;       // [max_bodies] dataflow path: last entry of each body's list
+    uint32_t* sweep_tag = nullptr;  // [1] dataflow path: last sweep-pass number (kept across solves)
+    uint32_t* csr_off = nullptr;    // [max_bodies + 1] dataflow sequential order: list offsets
+    uint32_t* csr_cur = nullptr;    // [max_bodies] dataflow sequential order: fill cursors
+    uint32_t* csr = nullptr;        // [2 max_contacts] dataflow sequential order: list entries
+    uint32_t* partial = nullptr;    // [4096] dataflow sequential order: per-block sums
     int coop_blocks = 0;            // co-resident blocks of the round-synchronous coloured kernel
     int flow_blocks = 0;            // co-resident blocks of the dataflow kernel
 };

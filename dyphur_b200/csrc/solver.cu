@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(kSeqThreads) sequential_solve_kernel(
     __shared__ int s_deferred;
     const uint32_t nc = contact_count(cv);
     if (nc == 0) return;
-    if (!wants_sequential(mode, nc) && ld_acquire(&meta[kMetaDecision]) != 1u) return;
+    // Small sequential-order frames, or a fallback the other kernels handed on.
+    if (!(wants_sequential(mode, nc) && nc <= kSeqOneBlock) && ld_acquire(&meta[kMetaDecision]) != 1u) return;
     const uint32_t nb = B.v.n;
     const uint32_t t = threadIdx.x;
     uint32_t* pred_a = pred;
@@ -231,7 +232,7 @@ int flow_block_count() {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flow_solve_kernel, kFlowThreads, 0);
-        blocks = sms * std::max(1, std::min(per_sm, 4));
+        blocks = std::min(sms * std::max(1, std::min(per_sm, 4)), kFlowMaxBlocks);
     }
     return blocks;
 }
@@ -257,7 +258,14 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
               cudaMalloc(&sv->meta, kMetaWords * 4) == cudaSuccess &&
               cudaMalloc(&sv->body_list, mb * kBodySlots * 8) == cudaSuccess &&
               cudaMalloc(&sv->slot, 2 * mc * 4) == cudaSuccess &&
-              cudaMalloc(&sv->link, 2 * mc * 4) == cudaSuccess && cudaMalloc(&sv->cmask, 2 * mc * 8) == cudaSuccess;
+              cudaMalloc(&sv->link, 2 * mc * 4) == cudaSuccess && cudaMalloc(&sv->cmask, 2 * mc * 8) == cudaSuccess &&
+              cudaMalloc(&sv->hand, 2 * mc * kHandWords * 8) == cudaSuccess &&
+              cudaMemset(sv->hand, 0, 2 * mc * kHandWords * 8) == cudaSuccess &&
+              cudaMalloc(&sv->tail, mb * 4) == cudaSuccess && cudaMalloc(&sv->sweep_tag, 4) == cudaSuccess &&
+              cudaMalloc(&sv->csr_off, (mb + 1) * 4) == cudaSuccess && cudaMalloc(&sv->csr_cur, mb * 4) == cudaSuccess &&
+              cudaMalloc(&sv->csr, 2 * mc * 4) == cudaSuccess &&
+              cudaMalloc(&sv->partial, kFlowMaxBlocks * 4) == cudaSuccess &&
+              cudaMemset(sv->sweep_tag, 0, 4) == cudaSuccess;
     if (!ok) {
         xpbd_destroy(sv);
         return DYPH_ERR_NOMEM;
@@ -271,7 +279,8 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
 void xpbd_destroy(dyph_xpbd* sv) {
     if (!sv) return;
     void* ptrs[] = {sv->lambda, sv->color, sv->order, sv->pred, sv->done, sv->bpri, sv->bmask, sv->blast, sv->meta,
-                    sv->body_list, sv->slot, sv->link, sv->cmask};
+                    sv->body_list, sv->slot, sv->link, sv->cmask, sv->hand, sv->tail, sv->sweep_tag,
+                    sv->csr_off, sv->csr_cur, sv->csr, sv->partial};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sv;
@@ -290,7 +299,9 @@ dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_
     // Per-body contact counts live in `blast`, JP rounds in `order`: the
     // kernels that also use them run only after this one declined the frame.
     FlowBufs F{sv->blast, reinterpret_cast<unsigned long long*>(sv->body_list), sv->slot, sv->link,
-               reinterpret_cast<unsigned long long*>(sv->cmask), sv->order, sv->done};
+               reinterpret_cast<unsigned long long*>(sv->cmask), sv->order,
+               reinterpret_cast<unsigned long long*>(sv->hand), 2u * sv->max_contacts, sv->tail, sv->sweep_tag,
+               sv->csr_off, sv->csr_cur, sv->csr, sv->partial};
     void* fargs[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &F, &sv->meta};
     DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(flow_solve_kernel), dim3(sv->flow_blocks),
                                               dim3(kFlowThreads), fargs, 0, s));

@@ -86,8 +86,10 @@ def test_stage_parity_blocks_sequential(dev, oracle_mod, frame):
 
 
 @pytest.mark.parametrize("frame", [0, 2])
-def test_stage_parity_random_pile_65k(dev, oracle_mod, frame):
-    stage_parity(dev, oracle_mod, scenes.random_pile(65536), frame)
+@pytest.mark.parametrize("mode", [0, 1])
+def test_stage_parity_random_pile_65k(dev, oracle_mod, frame, mode):
+    """Mode 1 here runs the sequential order on the dataflow kernel (> 2048 contacts)."""
+    stage_parity(dev, oracle_mod, scenes.random_pile(65536), frame, mode=mode)
 
 
 def test_world_determinism_golden(dev):
