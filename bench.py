@@ -148,9 +148,9 @@ def stage_bytes(stage: str, n: int, pairs: np.ndarray, contacts: np.ndarray) -> 
 def kernels_per_frame(n: int) -> int:
     """Library kernels one frame launches (matches the ncu launch list in profiles/)."""
     sort = 1 if n <= 4096 else 5  # one-block sort, or histogram + 4 onesweep passes
-    # integrate, morton, sort, build, finalize, pair find, pair write, narrowphase,
+    # integrate, morton, sort, build, finalize, pair find (two passes), pair write, narrowphase,
     # solver (dataflow, round-synchronous, sequential: two of them return at once), stats
-    return 1 + 1 + sort + 1 + 1 + 1 + 1 + 1 + 3 + 1
+    return 1 + 1 + sort + 1 + 1 + 2 + 1 + 1 + 3 + 1
 
 
 def peaks() -> tuple[float, str]:

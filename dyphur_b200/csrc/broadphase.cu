@@ -20,6 +20,9 @@ namespace {
 
 constexpr int kBpThreads = 256;
 constexpr int kMaxPartners = 32;  // per-thread sorted partner window (larger lists take extra passes)
+constexpr int kFrontier = 128;     // pass 1a hands subtrees of at most this many leaves to pass 1b
+constexpr int kFrontierItems = 16; // subtrees one query may hand on (more are walked in place)
+constexpr int kQueuePerBody = 16;  // pass 1b queue capacity per body (overflow is walked in place)
 
 __global__ void __launch_bounds__(kBpThreads) morton_kernel(GlobalBodies B, uint32_t n, dyph_aabb bounds,
                                                             uint32_t* __restrict__ codes,
@@ -39,6 +42,7 @@ __global__ void __launch_bounds__(kBpThreads) morton_kernel(GlobalBodies B, uint
         counts[0] = 0u;
         counts[1] = 0u;
         counts[2] = 0u;
+        counts[3] = 0u;  // pass 1b queue length
     }
 }
 
@@ -89,10 +93,10 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
         // Publish our far end (left child: slot 2s, right child: slot 2s+1) and
         // box, then rendezvous at split s.
         T.slot[2 * s + (is_left ? 0 : 1)] = static_cast<uint32_t>(is_left ? l : r);
-        __threadfence();
-        const uint32_t old = atomicAdd(&T.flags[s], 1u);
+        // One acq_rel atomic: releases this child's slot / box / big writes and,
+        // for the second arrival, acquires the sibling's.
+        const uint32_t old = atom_add_acq_rel(&T.flags[s], 1u);
         if ((old & 1u) == 0u) return;  // first arrival: the sibling carries on
-        __threadfence();
         // L2 loads (ld.global.cg): the sibling's writes were made on another SM.
         const int other = static_cast<int>(__ldcg(&T.slot[2 * s + (is_left ? 1 : 0)]));
         const int L = is_left ? l : other;
@@ -174,9 +178,15 @@ __global__ void __launch_bounds__(kBpThreads) finalize_nodes_kernel(uint32_t n_u
 // large (static) leaf from the small side, a pair of two large leaves from the
 // larger index. So a small query visits leaves i < k plus large leaves i > k,
 // and a large query visits only large leaves i < k.
-template <typename F>
-__device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const BoxF& q, int k, bool me_big, F&& visit) {
-    int node = 0;
+//
+// The walk covers the subtree at `start` (pre-order: it ends at the first node
+// whose leaf range starts past `end_leaf`). `frontier(node)` is offered every
+// wanted, overlapping internal node covering at most kFrontier leaves; when it
+// returns true the walk hands that subtree on instead of descending into it.
+template <typename F, typename G>
+__device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const BoxF& q, int k, bool me_big, int start,
+                                           int end_leaf, F&& visit, G&& frontier) {
+    int node = start;
     int budget = 2 * n;
     while (node >= 0) {
         if (node >= 2 * n - 1 || --budget < 0) {
@@ -185,6 +195,7 @@ __device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const Box
         }
         const uint4 r0 = __ldg(&T.trav[2 * node]);
         const uint4 r1 = __ldg(&T.trav[2 * node + 1]);
+        if (static_cast<int>(r1.x) > end_leaf) return;
         const bool before = static_cast<int>(r1.x) < k;
         const bool has_big = r1.w != 0u;
         const bool wanted = me_big ? (has_big && before) : (before || has_big);
@@ -196,7 +207,7 @@ __device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const Box
         if (box_overlap(unpack_box(r0), q)) {
             if (node >= n - 1) {
                 visit(r0.w);
-            } else {
+            } else if (!(static_cast<int>(r1.y - r1.x) < kFrontier && frontier(node))) {
                 node = static_cast<int>(r0.w);
                 continue;
             }
@@ -251,24 +262,89 @@ __device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const B
     return count;
 }
 
-// Pass 1, one thread per leaf in Morton order (neighbouring threads walk the
-// same part of the tree): leaf k tests only leaves i < k, so every
-// overlapping pair is found once; the pair goes to the bucket of its smaller
-// body index.
-__global__ void __launch_bounds__(kBpThreads) pair_find_kernel(uint32_t n_u, BvhBuffers T) {
+__device__ __forceinline__ void bucket_pair(const BvhBuffers& T, uint32_t me, uint32_t other) {
+    const uint32_t a = me < other ? me : other;
+    const uint32_t b = me < other ? other : me;
+    const uint32_t slot = atomicAdd(&T.bucket_cnt[a], 1u);
+    if (slot < static_cast<uint32_t>(kBucket)) T.bucket[static_cast<size_t>(a) * kBucket + slot] = b;
+}
+
+// Pass 1a, one thread per leaf in Morton order (neighbouring threads walk the
+// same part of the tree): walk the tree above subtrees of at most kFrontier
+// leaves and queue (leaf, subtree) items for pass 1b, so each query's work is
+// spread over several threads. Leaf k tests only leaves i < k (plus static
+// leaves from the small side), so every overlapping pair is found once; the
+// pair goes to the bucket of its smaller body index.
+__global__ void __launch_bounds__(kBpThreads) pair_find_kernel(uint32_t n_u, BvhBuffers T, uint2* __restrict__ queue,
+                                                               uint32_t queue_cap, uint32_t* __restrict__ queue_len) {
     const int n = static_cast<int>(n_u);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const uint4 r0 = __ldg(&T.trav[2 * (n - 1 + k)]);
-    const uint4 r1 = __ldg(&T.trav[2 * (n - 1 + k) + 1]);
-    const BoxF q = unpack_box(r0);
-    const uint32_t me = r0.w;
-    walk_pairs(T, n, q, k, r1.w != 0u, [&](uint32_t other) {
-        const uint32_t a = me < other ? me : other;
-        const uint32_t b = me < other ? other : me;
-        const uint32_t slot = atomicAdd(&T.bucket_cnt[a], 1u);
-        if (slot < static_cast<uint32_t>(kBucket)) T.bucket[static_cast<size_t>(a) * kBucket + slot] = b;
-    });
+    uint32_t items[kFrontierItems];
+    uint32_t m = 0;
+    if (k < n) {
+        const uint4 r0 = __ldg(&T.trav[2 * (n - 1 + k)]);
+        const uint4 r1 = __ldg(&T.trav[2 * (n - 1 + k) + 1]);
+        const BoxF q = unpack_box(r0);
+        const uint32_t me = r0.w;
+        const bool me_big = r1.w != 0u;
+        walk_pairs(
+            T, n, q, k, me_big, 0, n, [&](uint32_t other) { bucket_pair(T, me, other); },
+            [&](int node) {
+                if (m < static_cast<uint32_t>(kFrontierItems)) {
+                    items[m++] = static_cast<uint32_t>(node);
+                    return true;
+                }
+                return false;  // local list full: descend here instead
+            });
+    }
+    // Warp-aggregated append of the items.
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t incl = m;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= static_cast<uint32_t>(d)) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total) base = atomicAdd(queue_len, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    if (m == 0) return;
+    const uint32_t first = base + incl - m;
+    const BoxF q = unpack_box(__ldg(&T.trav[2 * (n - 1 + k)]));
+    const uint32_t me = __ldg(&T.trav[2 * (n - 1 + k)]).w;
+    const bool me_big = __ldg(&T.trav[2 * (n - 1 + k) + 1]).w != 0u;
+    for (uint32_t i = 0; i < m; ++i) {
+        if (first + i < queue_cap) {
+            queue[first + i] = make_uint2(static_cast<uint32_t>(k), items[i]);
+        } else {  // queue full: walk the subtree here
+            const int f = static_cast<int>(items[i]);
+            const int end_leaf = static_cast<int>(__ldg(&T.trav[2 * f + 1]).y);
+            walk_pairs(
+                T, n, q, k, me_big, f, end_leaf, [&](uint32_t other) { bucket_pair(T, me, other); },
+                [](int) { return false; });
+        }
+    }
+}
+
+// Pass 1b, one thread per queued (leaf, subtree) item.
+__global__ void __launch_bounds__(kBpThreads) pair_subtree_kernel(uint32_t n_u, BvhBuffers T,
+                                                                  const uint2* __restrict__ queue, uint32_t queue_cap,
+                                                                  const uint32_t* __restrict__ queue_len) {
+    const int n = static_cast<int>(n_u);
+    const uint32_t len = min(*queue_len, queue_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+        const uint2 it = queue[i];
+        const int k = static_cast<int>(it.x), f = static_cast<int>(it.y);
+        const uint4 r0 = __ldg(&T.trav[2 * (n - 1 + k)]);
+        const bool me_big = __ldg(&T.trav[2 * (n - 1 + k) + 1]).w != 0u;
+        const BoxF q = unpack_box(r0);
+        const uint32_t me = r0.w;
+        const int end_leaf = static_cast<int>(__ldg(&T.trav[2 * f + 1]).y);
+        walk_pairs(
+            T, n, q, k, me_big, f, end_leaf, [&](uint32_t other) { bucket_pair(T, me, other); },
+            [](int) { return false; });
+    }
 }
 
 // Pass 2, one thread per body in body order: place each body's pairs with a
@@ -370,6 +446,17 @@ __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, Bv
     }
 }
 
+int subtree_blocks() {
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        blocks = sms * 8;
+    }
+    return blocks;
+}
+
 template <typename T>
 cudaError_t dev_alloc(T** p, size_t count) {
     return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
@@ -398,7 +485,10 @@ dyph_status broadphase_build(dyph_broadphase* bp, const dyph_bodies* bodies, con
     DYPH_CUDA_TRY(cudaGetLastError());
     finalize_nodes_kernel<<<(2 * n - 1 + kBpThreads - 1) / kBpThreads, kBpThreads, 0, s>>>(n, bp->bvh);
     DYPH_CUDA_TRY(cudaGetLastError());
-    pair_find_kernel<<<leaf_blocks, kBpThreads, 0, s>>>(n, bp->bvh);
+    const uint32_t queue_cap = bp->max_bodies * static_cast<uint32_t>(kQueuePerBody);
+    pair_find_kernel<<<leaf_blocks, kBpThreads, 0, s>>>(n, bp->bvh, bp->queue, queue_cap, bp->counts + 3);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    pair_subtree_kernel<<<subtree_blocks(), kBpThreads, 0, s>>>(n, bp->bvh, bp->queue, queue_cap, bp->counts + 3);
     DYPH_CUDA_TRY(cudaGetLastError());
     pair_write_kernel<<<n_tiles, kBpThreads, 0, s>>>(n, bp->bvh, reinterpret_cast<uint2*>(bp->pairs), bp->max_pairs,
                                                      bp->counts, bp->tstatus);
@@ -424,7 +514,8 @@ dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broa
               dev_alloc(&bp->tstatus, (nb + kBpThreads - 1) / kBpThreads) == cudaSuccess &&
               dev_alloc(&bp->bvh.range_lo, ni) == cudaSuccess && dev_alloc(&bp->bvh.trav, 2 * nn) == cudaSuccess &&
               dev_alloc(&bp->bvh.bucket_cnt, nb) == cudaSuccess && dev_alloc(&bp->bvh.big, nn) == cudaSuccess &&
-              dev_alloc(&bp->bvh.bucket, nb * kBucket) == cudaSuccess;
+              dev_alloc(&bp->bvh.bucket, nb * kBucket) == cudaSuccess &&
+              dev_alloc(&bp->queue, nb * kQueuePerBody) == cudaSuccess;
     if (ok) {
         bp->sort_ws_bytes = sort_workspace_bytes(nb, 4);
         ok = cudaMalloc(&bp->sort_ws, bp->sort_ws_bytes) == cudaSuccess;
@@ -446,7 +537,7 @@ void broadphase_destroy(dyph_broadphase* bp) {
     void* ptrs[] = {bp->codes, bp->bvh.sorted_idx, bp->bvh.sorted_keys, bp->bvh.inv_sorted, bp->bvh.left,
                     bp->bvh.right, bp->bvh.parent, bp->bvh.root, bp->bvh.aabb, bp->bvh.range_hi, bp->bvh.rsplit,
                     bp->bvh.slot, bp->bvh.flags, bp->pairs, bp->counts, bp->tstatus, bp->sort_ws,
-                    bp->bvh.range_lo, bp->bvh.trav, bp->bvh.bucket_cnt, bp->bvh.bucket, bp->bvh.big};
+                    bp->bvh.range_lo, bp->bvh.trav, bp->bvh.bucket_cnt, bp->bvh.bucket, bp->bvh.big, bp->queue};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete bp;

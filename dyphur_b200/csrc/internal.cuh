@@ -43,7 +43,8 @@ struct dyph_broadphase {
     uint32_t* codes = nullptr;   // Morton codes, sorted in place
     dyph::BvhBuffers bvh{};
     dyph_pair* pairs = nullptr;  // [max_pairs]
-    uint32_t* counts = nullptr;  // [0] stored pairs, [1] true pairs, [2] traversal tile counter
+    uint32_t* counts = nullptr;  // [0] stored pairs, [1] true pairs, [2] tile counter, [3] subtree queue length
+    uint2* queue = nullptr;      // [16 max_bodies] (leaf, subtree) items of the pair search's second pass
     uint32_t* tstatus = nullptr; // traversal look-back status, one word per 256 bodies
     void* sort_ws = nullptr;
     size_t sort_ws_bytes = 0;
