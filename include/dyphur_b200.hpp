@@ -1,0 +1,428 @@
+// C++20 class layer over the C ABI, mirroring the reference's compute/ and
+// core/ surface so host code written against it keeps compiling:
+//   Device / Stream / Event / Buffer<T>      compute/include/compute/{device,stream,buffer}.hpp
+//   sort_by_key / sort                       compute/include/compute/sort.hpp:29,88
+//   BodyStore / ShapeStore                   core/include/core/{body_store,shape_store}.hpp
+//   integrate                                core/include/core/integrator.hpp:25
+//   Broadphase / Narrowphase / XpbdSolver    core/include/core/{broadphase,narrowphase,xpbd_solver}.hpp
+// The views (BodyView, ShapeView, ContactView, ContactPair, AABB) are the C
+// ABI's structs, which have the reference's field order. Errors throw
+// std::runtime_error where the reference throws (SYCL exceptions, no GPU);
+// there is no CPU device. Link with libdyphur_b200.so and the CUDA runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "dyphur_b200.h"
+
+extern "C" void dyph_pack_bodies(uint32_t n, const float* pos, const float* rot, const float* vel, const float* ang,
+                                 const float* mass, const float* inertia, const uint32_t* flags_in, float* state13,
+                                 float* inv_mass, float* iI6, uint32_t* flags_out);
+
+namespace dyphur {
+
+inline void check(dyph_status st, const char* what) {
+    if (st != DYPH_OK) throw std::runtime_error(std::string(what) + ": " + dyph_status_string(st));
+}
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+using BodyView = dyph_bodies;
+using ShapeView = dyph_shapes;
+using ContactView = dyph_contacts;
+using ContactPair = dyph_pair;
+using AABB = dyph_aabb;
+using BvhView = dyph_bvh_view;
+
+// ── compute ─────────────────────────────────────────────────────────────────
+
+class Event {
+public:
+    Event() = default;
+    explicit Event(cudaStream_t s) {
+        check_cuda(cudaEventCreateWithFlags(&e_, cudaEventDisableTiming), "cudaEventCreate");
+        check_cuda(cudaEventRecord(e_, s), "cudaEventRecord");
+    }
+    ~Event() {
+        if (e_) cudaEventDestroy(e_);
+    }
+    Event(const Event&) = delete;
+    Event& operator=(const Event&) = delete;
+    Event(Event&& o) noexcept : e_(std::exchange(o.e_, nullptr)) {}
+    Event& operator=(Event&& o) noexcept {
+        std::swap(e_, o.e_);
+        return *this;
+    }
+    void wait() {
+        if (e_) check_cuda(cudaEventSynchronize(e_), "Event::wait");
+    }
+
+private:
+    cudaEvent_t e_ = nullptr;
+};
+
+// In-order queue of one device (the reference's in-order sycl::queue).
+class Stream {
+public:
+    explicit Stream(int device) : dev_(device) {
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        check_cuda(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+    ~Stream() {
+        if (s_) cudaStreamDestroy(s_);
+    }
+    Stream(const Stream&) = delete;
+    Stream& operator=(const Stream&) = delete;
+    void wait() { check_cuda(cudaStreamSynchronize(s_), "Stream::wait"); }
+    cudaStream_t native() const noexcept { return s_; }
+    dyph_stream abi() const noexcept { return reinterpret_cast<dyph_stream>(s_); }
+    int device() const noexcept { return dev_; }
+
+private:
+    int dev_ = 0;
+    cudaStream_t s_ = nullptr;
+};
+
+class Device {
+public:
+    explicit Device(int ordinal) : dev_(ordinal) {}
+    // Throws when no sm_100 device is present (the reference throws from its selector).
+    static Device default_gpu() {
+        check(dyph_device_check(), "Device::default_gpu");
+        int d = 0;
+        check_cuda(cudaGetDevice(&d), "cudaGetDevice");
+        return Device(d);
+    }
+    static Device default_cpu() { throw std::runtime_error("Device::default_cpu: this build has no CPU path"); }
+    static Device preferred() { return default_gpu(); }
+    std::string name() const {
+        cudaDeviceProp p{};
+        check_cuda(cudaGetDeviceProperties(&p, dev_), "cudaGetDeviceProperties");
+        return p.name;
+    }
+    bool is_gpu() const { return true; }
+    bool is_cpu() const { return false; }
+    size_t max_compute_units() const {
+        int v = 0;
+        check_cuda(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev_), "attribute");
+        return static_cast<size_t>(v);
+    }
+    size_t global_mem_bytes() const {
+        cudaDeviceProp p{};
+        check_cuda(cudaGetDeviceProperties(&p, dev_), "cudaGetDeviceProperties");
+        return p.totalGlobalMem;
+    }
+    Stream make_stream() const { return Stream(dev_); }
+    int ordinal() const noexcept { return dev_; }
+
+private:
+    int dev_ = 0;
+};
+
+// Move-only device array (compute/include/compute/buffer.hpp:10-55).
+template <typename T>
+class Buffer {
+public:
+    Buffer() = default;
+    Buffer(Stream& s, size_t n) : s_(&s), n_(n) {
+        if (n > 0) check_cuda(cudaMalloc(reinterpret_cast<void**>(&data_), n * sizeof(T)), "Buffer");
+    }
+    ~Buffer() {
+        if (data_) cudaFree(data_);
+    }
+    Buffer(const Buffer&) = delete;
+    Buffer& operator=(const Buffer&) = delete;
+    Buffer(Buffer&& o) noexcept : s_(o.s_), n_(std::exchange(o.n_, 0)), data_(std::exchange(o.data_, nullptr)) {}
+    Buffer& operator=(Buffer&& o) noexcept {
+        if (this != &o) {
+            if (data_) cudaFree(data_);
+            s_ = o.s_;
+            n_ = std::exchange(o.n_, 0);
+            data_ = std::exchange(o.data_, nullptr);
+        }
+        return *this;
+    }
+    T* data() noexcept { return data_; }
+    const T* data() const noexcept { return data_; }
+    size_t size() const noexcept { return n_; }
+    bool empty() const noexcept { return n_ == 0; }
+    Event upload(const T* src, size_t count = 0) {
+        check_cuda(cudaMemcpyAsync(data_, src, (count ? count : n_) * sizeof(T), cudaMemcpyHostToDevice,
+                                   s_->native()),
+                   "Buffer::upload");
+        return Event(s_->native());
+    }
+    void download(T* dst, size_t count = 0) const {
+        check(dyph_copy_to_host(dst, data_, (count ? count : n_) * sizeof(T), s_->abi()), "Buffer::download");
+    }
+
+private:
+    Stream* s_ = nullptr;
+    size_t n_ = 0;
+    T* data_ = nullptr;
+};
+
+// Stable ascending sorts; unlike the reference, n need not be a power of two.
+inline void sort_by_key(Stream& s, uint64_t* keys, uint32_t* values, size_t n) {
+    Buffer<uint8_t> ws(s, dyph_sort_workspace_bytes(n));
+    check(dyph_sort_by_key_u64_u32(keys, values, n, ws.data(), ws.size(), s.abi()), "sort_by_key");
+    s.wait();  // the workspace is freed on return
+}
+inline void sort_by_key(Stream& s, uint32_t* keys, uint32_t* values, size_t n) {
+    Buffer<uint8_t> ws(s, dyph_sort_workspace_bytes(n));
+    check(dyph_sort_by_key_u32_u32(keys, values, n, 32, ws.data(), ws.size(), s.abi()), "sort_by_key");
+    s.wait();
+}
+inline void sort(Stream& s, uint64_t* keys, size_t n) {
+    Buffer<uint8_t> ws(s, dyph_sort_workspace_bytes(n));
+    check(dyph_sort_u64(keys, n, ws.data(), ws.size(), s.abi()), "sort");
+    s.wait();
+}
+
+// ── core ────────────────────────────────────────────────────────────────────
+
+constexpr uint32_t kBodyStatic = 1u;  // BodyFlag::Static (core/include/core/body.hpp:9)
+
+// BodyParams (core/include/core/body.hpp:16-25) with plain arrays for the math types.
+struct BodyParams {
+    float position[3] = {0.f, 0.f, 0.f};
+    float rotation[4] = {1.f, 0.f, 0.f, 0.f};  // w, x, y, z
+    float linear_velocity[3] = {0.f, 0.f, 0.f};
+    float angular_velocity[3] = {0.f, 0.f, 0.f};
+    float mass = 1.f;
+    float inertia[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};  // row-major, body frame
+    uint32_t shape_handle = 0;
+    uint32_t flags = 0;
+};
+
+// core/include/core/body_store.hpp:21-73. add() inverts the inertia on the
+// host in float exactly as the reference's Mat3::inverse does.
+class BodyStore {
+public:
+    BodyStore(Stream& s, uint32_t capacity) : s_(&s), cap_(capacity), d_f_(s, size_t(20) * capacity),
+                                             d_u_(s, size_t(2) * capacity) {}
+    uint32_t add(const BodyParams& p) {
+        if (count_ >= cap_) throw std::runtime_error("BodyStore::add: capacity exceeded");
+        h_.push_back(p);
+        return count_++;
+    }
+    void upload() {
+        const uint32_t n = count_;
+        std::vector<float> pos(3 * n), rot(4 * n), vel(3 * n), ang(3 * n), mass(n), inertia(9 * n);
+        std::vector<uint32_t> flags(n), shape(n), flags_out(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const BodyParams& p = h_[i];
+            for (int k = 0; k < 3; ++k) {
+                pos[3 * i + k] = p.position[k];
+                vel[3 * i + k] = p.linear_velocity[k];
+                ang[3 * i + k] = p.angular_velocity[k];
+            }
+            for (int k = 0; k < 4; ++k) rot[4 * i + k] = p.rotation[k];
+            for (int k = 0; k < 9; ++k) inertia[9 * i + k] = p.inertia[k];
+            mass[i] = p.mass;
+            flags[i] = p.flags;
+            shape[i] = p.shape_handle;
+        }
+        // rows 0..12 state, 13 inverse mass, 14..19 inverse inertia, each `cap` long
+        std::vector<float> st(size_t(13) * n), im(n), ii(size_t(6) * n);
+        dyph_pack_bodies(n, pos.data(), rot.data(), vel.data(), ang.data(), mass.data(), inertia.data(),
+                         flags.data(), st.data(), im.data(), ii.data(), flags_out.data());
+        for (int r = 0; r < 13; ++r) copy_row(r, st.data() + size_t(r) * n, n);
+        copy_row(13, im.data(), n);
+        for (int r = 0; r < 6; ++r) copy_row(14 + r, ii.data() + size_t(r) * n, n);
+        check_cuda(cudaMemcpyAsync(d_u_.data(), shape.data(), n * 4, cudaMemcpyHostToDevice, s_->native()), "upload");
+        check_cuda(cudaMemcpyAsync(d_u_.data() + cap_, flags_out.data(), n * 4, cudaMemcpyHostToDevice,
+                                   s_->native()),
+                   "upload");
+        s_->wait();
+    }
+    BodyView view() noexcept {
+        float* f = d_f_.data();
+        auto row = [&](int r) { return f + size_t(r) * cap_; };
+        return BodyView{row(0),  row(1),  row(2),  row(3),  row(4),  row(5),  row(6),
+                        row(7),  row(8),  row(9),  row(10), row(11), row(12), row(13),
+                        row(14), row(15), row(16), row(17), row(18), row(19), d_u_.data(),
+                        d_u_.data() + cap_, count_};
+    }
+    uint32_t count() const noexcept { return count_; }
+    uint32_t capacity() const noexcept { return cap_; }
+
+private:
+    void copy_row(int r, const float* src, uint32_t n) {
+        check_cuda(cudaMemcpyAsync(d_f_.data() + size_t(r) * cap_, src, n * 4, cudaMemcpyHostToDevice, s_->native()),
+                   "upload");
+    }
+    Stream* s_;
+    uint32_t cap_, count_ = 0;
+    Buffer<float> d_f_;
+    Buffer<uint32_t> d_u_;
+    std::vector<BodyParams> h_;
+};
+
+// ShapeParams / ShapeStore (core/include/core/shapes.hpp, shape_store.hpp):
+// boxes (half extents) and spheres (radius in half_x).
+enum class ShapeType : uint32_t { Box = 0, Sphere = 1 };
+struct ShapeParams {
+    ShapeType type = ShapeType::Box;
+    float half_x = 0.5f, half_y = 0.5f, half_z = 0.5f;
+};
+
+class ShapeStore {
+public:
+    ShapeStore(Stream& s, uint32_t capacity)
+        : s_(&s), cap_(capacity), d_type_(s, capacity), d_half_(s, size_t(3) * capacity), d_ext_(s, capacity) {}
+    uint32_t add(const ShapeParams& p) {
+        if (count_ >= cap_) throw std::runtime_error("ShapeStore::add: capacity exceeded");
+        h_.push_back(p);
+        return count_++;
+    }
+    void upload() {
+        std::vector<uint32_t> type(count_), ext(count_, 0u);
+        std::vector<float> half(size_t(3) * cap_, 0.f);
+        for (uint32_t i = 0; i < count_; ++i) {
+            type[i] = static_cast<uint32_t>(h_[i].type);
+            half[i] = h_[i].half_x;
+            half[cap_ + i] = h_[i].half_y;
+            half[2 * size_t(cap_) + i] = h_[i].half_z;
+        }
+        if (count_) {
+            d_type_.upload(type.data(), count_);
+            d_ext_.upload(ext.data(), count_);
+        }
+        d_half_.upload(half.data());
+        s_->wait();
+    }
+    ShapeView view() noexcept {
+        return ShapeView{d_type_.data(), d_half_.data(), d_half_.data() + cap_, d_half_.data() + 2 * size_t(cap_),
+                         d_ext_.data(), count_};
+    }
+    uint32_t count() const noexcept { return count_; }
+    uint32_t capacity() const noexcept { return cap_; }
+
+private:
+    Stream* s_;
+    uint32_t cap_, count_ = 0;
+    Buffer<uint32_t> d_type_;
+    Buffer<float> d_half_;
+    Buffer<uint32_t> d_ext_;
+    std::vector<ShapeParams> h_;
+};
+
+struct IntegratorParams {
+    float gravity[3] = {0.f, -9.81f, 0.f};
+    float dt = 1.f / 60.f;
+    int32_t n_substeps = 1;
+};
+
+inline void integrate(Stream& s, BodyView bodies, const IntegratorParams& p) {
+    const dyph_integrator_params c{{p.gravity[0], p.gravity[1], p.gravity[2]}, p.dt, p.n_substeps};
+    check(dyph_integrate(&bodies, &c, s.abi()), "integrate");
+}
+
+class Broadphase {
+public:
+    Broadphase(Stream& s, uint32_t max_bodies, uint32_t max_pairs) {
+        (void)s;
+        check(dyph_broadphase_create(max_bodies, max_pairs, &h_), "Broadphase");
+    }
+    ~Broadphase() { dyph_broadphase_destroy(h_); }
+    Broadphase(const Broadphase&) = delete;
+    Broadphase& operator=(const Broadphase&) = delete;
+    void build_and_query(Stream& s, const BodyView& bodies, const ShapeView& shapes, const AABB& scene_bounds) {
+        check(dyph_broadphase_build_and_query(h_, &bodies, &shapes, &scene_bounds, s.abi()), "build_and_query");
+    }
+    const ContactPair* pairs_ptr() const noexcept { return dyph_broadphase_pairs(h_); }
+    const uint32_t* count_ptr() const noexcept { return dyph_broadphase_count_ptr(h_); }
+    uint32_t max_pairs() const noexcept { return dyph_broadphase_max_pairs(h_); }
+    void sort_pairs(Stream& s, uint32_t n_pairs) { check(dyph_broadphase_sort_pairs(h_, n_pairs, s.abi()), "sort_pairs"); }
+    uint32_t download_count(Stream& s) const {
+        uint32_t n = 0;
+        check(dyph_broadphase_download_count(h_, s.abi(), &n), "download_count");
+        return n;
+    }
+    BvhView bvh_view(uint32_t n_active) const {
+        BvhView v{};
+        check(dyph_broadphase_bvh_view(h_, n_active, &v), "bvh_view");
+        return v;
+    }
+
+private:
+    dyph_broadphase* h_ = nullptr;
+};
+
+class Narrowphase {
+public:
+    Narrowphase(Stream& s, uint32_t max_contacts) : cap_(max_contacts) {
+        (void)s;
+        check(dyph_narrowphase_create(max_contacts, &h_), "Narrowphase");
+    }
+    ~Narrowphase() { dyph_narrowphase_destroy(h_); }
+    Narrowphase(const Narrowphase&) = delete;
+    Narrowphase& operator=(const Narrowphase&) = delete;
+    void run(Stream& s, const ContactPair* d_pairs, uint32_t n_pairs, const BodyView& bodies, const ShapeView& shapes) {
+        check(dyph_narrowphase_run_host_count(h_, d_pairs, n_pairs, &bodies, &shapes, s.abi()), "Narrowphase::run");
+        uint32_t stored = 0;
+        check(dyph_narrowphase_download_count(h_, s.abi(), &stored, &last_count_), "download_count");
+    }
+    void run(Stream& s, const ContactPair* d_pairs, const uint32_t* d_n_pairs, const BodyView& bodies,
+             const ShapeView& shapes) {
+        check(dyph_narrowphase_run(h_, d_pairs, d_n_pairs, &bodies, &shapes, s.abi()), "Narrowphase::run");
+    }
+    ContactView contacts() {
+        ContactView v{};
+        check(dyph_narrowphase_contacts(h_, &v), "contacts");
+        return v;
+    }
+    uint32_t download_count(Stream& s) const {
+        uint32_t stored = 0, total = 0;
+        check(dyph_narrowphase_download_count(h_, s.abi(), &stored, &total), "download_count");
+        return stored;
+    }
+    uint32_t last_contact_count() const noexcept { return last_count_; }
+    bool overflowed() const noexcept { return last_count_ > cap_; }
+
+private:
+    dyph_narrowphase* h_ = nullptr;
+    uint32_t cap_ = 0, last_count_ = 0;
+};
+
+class XpbdSolver {
+public:
+    static constexpr uint32_t kSerialThreshold = 256;  // xpbd_solver.hpp:43
+    explicit XpbdSolver(Stream& s, int n_iters = 10, uint32_t max_contacts = 16384, float friction = 0.5f,
+                        uint32_t max_bodies = 1u << 16) {
+        (void)s;
+        check(dyph_xpbd_create(n_iters, max_contacts, max_bodies, friction, &h_), "XpbdSolver");
+    }
+    ~XpbdSolver() { dyph_xpbd_destroy(h_); }
+    XpbdSolver(const XpbdSolver&) = delete;
+    XpbdSolver& operator=(const XpbdSolver&) = delete;
+    // IConstraintSolver::solve (core/include/core/solver.hpp:17-21); no joints on this path.
+    void solve(Stream& s, const ContactView& contacts, BodyView bodies, float dt) {
+        check(dyph_xpbd_solve(h_, &contacts, &bodies, dt, s.abi()), "XpbdSolver::solve");
+    }
+    void set_force_serial(bool v) {
+        check(dyph_xpbd_set_mode(h_, v ? DYPH_SOLVER_SEQUENTIAL : DYPH_SOLVER_REFERENCE), "set_force_serial");
+    }
+
+private:
+    dyph_xpbd* h_ = nullptr;
+};
+
+// FNV-1a-64 over pos_x..rot_z (examples/stress_test_blocks/main.cpp:34-41, 301-311).
+inline uint64_t state_hash(Stream& s, const BodyView& bodies) {
+    Buffer<uint64_t> h(s, 1);
+    check(dyph_fnv1a64_state(&bodies, h.data(), s.abi()), "state_hash");
+    uint64_t out = 0;
+    h.download(&out, 1);
+    return out;
+}
+
+}  // namespace dyphur
