@@ -46,7 +46,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--frames", type=int, default=600)
+    ap.add_argument("--workload", default="single", choices=["single", "batch"],
+                    help="single: the 65k-body pile; batch: 4096 independent scenes of 8-256 bodies")
+    ap.add_argument("--scenes", type=int, default=4096)
+    ap.add_argument("--frames", type=int, default=None)
     ap.add_argument("--start-frame", type=int, default=0,
                     help="step the pile this many frames (untimed) before recording the episode")
     ap.add_argument("--bodies", type=int, default=65536)
@@ -189,7 +192,14 @@ def run_b200(args) -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     mode = {"reference": capi.SOLVER_REFERENCE, "sequential": capi.SOLVER_SEQUENTIAL,
             "colored": capi.SOLVER_COLORED}[args.mode]
-    scene = scenes.random_pile(args.bodies, seed=2 + rank)  # replicas: one scene per rank
+    if args.workload == "batch":
+        # independent scenes in one world; sequential order keeps each scene exact
+        scene = scenes.batch(args.scenes, 8, 256, seed=3 + rank)
+        if args.mode == "reference":
+            mode = capi.SOLVER_SEQUENTIAL
+            args.mode = "sequential"
+    else:
+        scene = scenes.random_pile(args.bodies, seed=2 + rank)  # replicas: one scene per rank
     n = scene.n_bodies
     w = device.World(scene, mode=mode)
     if args.start_frame > 0:
@@ -289,12 +299,45 @@ def run_b200(args) -> None:
             "gpu_launches": int(args.steps * args.frames * kernels_per_frame(n)),
             "clocks": ck, "overflow_status": st["status"],
         }
-        if not args.no_cpu_baseline and world == 1:
+        if args.workload == "batch":
+            line["config"]["workload"] = (f"batched forward: {scene.n_scenes} independent scenes (box stacks or "
+                                          f"sphere piles, 8-256 bodies log-uniform, each on its own ground), "
+                                          f"{args.frames} frames at 60 Hz, fp32, one world")
+            line["config"]["scenes"] = scene.n_scenes
+            line["per_scene"] = per_scene_baseline(scene, args.frames, mode, torch, device)
+            line["per_scene"]["batched_over_per_scene"] = value / line["per_scene"]["value"]
+        elif not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.bodies, args.cpu_frames)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def per_scene_baseline(scene, frames: int, mode: int, torch, device, sample: int = 64) -> dict:
+    """The plain per-scene GPU path on a sample of the batch: each scene its own
+    world, its frames replayed as one captured episode, scenes one after another."""
+    idx = np.linspace(0, scene.n_scenes - 1, min(sample, scene.n_scenes)).astype(int)
+    worlds = []
+    for i in idx:
+        w = device.World(scene.scene(int(i)), mode=mode)
+        w.capture_episode(frames, -1)
+        worlds.append((w, w.bodies.fbuf.clone()))
+    stream = torch.cuda.current_stream()
+    for w, init in worlds:  # warm-up
+        w.bodies.fbuf.copy_(init)
+        w.run_episode(stream)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for w, init in worlds:
+        w.bodies.fbuf.copy_(init, non_blocking=True)
+        w.run_episode(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    bodies = sum(w.scene.n_bodies for w, _ in worlds)
+    return {"value": bodies * frames / (t0.elapsed_time(t1) / 1e3), "unit": METRIC,
+            "sample": f"{len(worlds)} of the batch's scenes, each stepped alone ({frames} frames)"}
 
 
 def run_reference(args) -> None:
@@ -327,6 +370,8 @@ def run_reference(args) -> None:
 
 def main():
     args = parse()
+    if args.frames is None:
+        args.frames = 240 if args.workload == "batch" else 600
     if args.cpu_worker:
         cpu_worker(args.cpu_worker, args.bodies, args.cpu_frames)
         return

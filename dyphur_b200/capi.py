@@ -61,6 +61,9 @@ _PROTOS = {
     "dyph_sort_workspace_bytes": (C.c_size_t, [C.c_size_t]),
     "dyph_sort_by_key_u64_u32": (_st, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, _vp]),
     "dyph_sort_by_key_u64_u32_noalloc": (_st, [_vp, _vp, C.c_size_t, _vp]),
+    "dyph_broadphase_set_scenes": (_st, [_vp, C.c_uint32, _vp, _vp]),
+    "dyph_world_set_scenes": (_st, [_vp, C.c_uint32, _vp, _vp]),
+    "dyph_world_scene_hashes": (_st, [_vp, _vp, _vp, C.c_uint32]),
     "dyph_sort_u64": (_st, [_vp, C.c_size_t, _vp, C.c_size_t, _vp]),
     "dyph_sort_by_key_u32_u32": (_st, [_vp, _vp, C.c_size_t, C.c_int, _vp, C.c_size_t, _vp]),
     "dyph_broadphase_create": (_st, [C.c_uint32, C.c_uint32, C.POINTER(_vp)]),

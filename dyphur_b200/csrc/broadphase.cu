@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <new>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -24,16 +25,28 @@ constexpr int kFrontier = 128;     // pass 1a hands subtrees of at most this man
 constexpr int kFrontierItems = 16; // subtrees one query may hand on (more are walked in place)
 constexpr int kQueuePerBody = 16;  // pass 1b queue capacity per body (overflow is walked in place)
 
+// Single scene: 30-bit codes against the scene bounds. Batched scenes
+// (codes64 != null): (scene << 30 | code) against each body's scene bounds,
+// so every scene's leaves are contiguous after the sort.
 __global__ void __launch_bounds__(kBpThreads) morton_kernel(GlobalBodies B, uint32_t n, dyph_aabb bounds,
                                                             uint32_t* __restrict__ codes,
                                                             uint32_t* __restrict__ sorted_idx,
                                                             uint32_t* __restrict__ counts,
                                                             uint32_t* __restrict__ tstatus, uint32_t n_tiles,
-                                                            uint32_t* __restrict__ bucket_cnt) {
+                                                            uint32_t* __restrict__ bucket_cnt,
+                                                            uint64_t* __restrict__ codes64,
+                                                            const uint32_t* __restrict__ scene_of,
+                                                            const dyph_aabb* __restrict__ scene_bounds) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < n; i += stride) {
-        codes[i] = morton_code(B.px(i), B.py(i), B.pz(i), bounds);
+        if (codes64) {
+            const uint32_t sc = scene_of[i];
+            codes64[i] = (static_cast<uint64_t>(sc) << 30) |
+                         morton_code(B.px(i), B.py(i), B.pz(i), scene_bounds[sc]);
+        } else {
+            codes[i] = morton_code(B.px(i), B.py(i), B.pz(i), bounds);
+        }
         sorted_idx[i] = i;
         bucket_cnt[i] = 0u;
     }
@@ -46,15 +59,18 @@ __global__ void __launch_bounds__(kBpThreads) morton_kernel(GlobalBodies B, uint
     }
 }
 
-__device__ __forceinline__ uint64_t key64(const uint32_t* codes, const uint32_t* si, int i) {
+// (code << 32 | body) as in the reference; batched: (scene << 52 | code << 22 | body).
+__device__ __forceinline__ uint64_t key64(const uint32_t* codes, const uint64_t* codes64, const uint32_t* si, int i) {
+    if (codes64) return (codes64[i] << 22) | static_cast<uint64_t>(si[i]);
     return (static_cast<uint64_t>(codes[i]) << 32) | static_cast<uint64_t>(si[i]);
 }
 
 // Common-prefix length between sorted positions i and i+1 (lbvh_delta,
 // broadphase.cpp:38-41); -1 outside [0, n-1).
-__device__ __forceinline__ int boundary_delta(const uint32_t* codes, const uint32_t* si, int i, int n) {
+__device__ __forceinline__ int boundary_delta(const uint32_t* codes, const uint64_t* codes64, const uint32_t* si, int i,
+                                              int n) {
     if (i < 0 || i >= n - 1) return -1;
-    return __clzll(static_cast<long long>(key64(codes, si, i) ^ key64(codes, si, i + 1)));
+    return __clzll(static_cast<long long>(key64(codes, codes64, si, i) ^ key64(codes, codes64, si, i + 1)));
 }
 
 __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, GlobalShapes S, uint32_t n_u,
@@ -64,7 +80,8 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t body = si[k];
-    T.sorted_keys[k] = key64(codes, si, k);
+    const uint64_t* codes64 = T.codes64;
+    T.sorted_keys[k] = key64(codes, codes64, si, k);
     T.inv_sorted[body] = static_cast<uint32_t>(k);
     const uint32_t sh = B.shape(body);
     uint4 box = leaf_box(S.type(sh), B.px(body), B.py(body), B.pz(body), B.qw(body), B.qx(body), B.qy(body),
@@ -86,8 +103,8 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
     int l = k, r = k;
     while (true) {
         if (l == 0 && r == n - 1) return;  // this thread completed the root
-        const int dl = boundary_delta(codes, si, l - 1, n);
-        const int dr = boundary_delta(codes, si, r, n);
+        const int dl = boundary_delta(codes, codes64, si, l - 1, n);
+        const int dr = boundary_delta(codes, codes64, si, r, n);
         const bool is_left = dr > dl;  // merge across boundary r: we are the left child
         const int s = is_left ? r : l - 1;
         // Publish our far end (left child: slot 2s, right child: slot 2s+1) and
@@ -107,8 +124,8 @@ __global__ void __launch_bounds__(kBpThreads) build_kernel(GlobalBodies B, Globa
         if (L == 0 && R == n - 1) {
             pidx = 0;
         } else {
-            const int pdl = boundary_delta(codes, si, L - 1, n);
-            const int pdr = boundary_delta(codes, si, R, n);
+            const int pdl = boundary_delta(codes, codes64, si, L - 1, n);
+            const int pdr = boundary_delta(codes, codes64, si, R, n);
             pidx = (pdr > pdl) ? R : L;
         }
         const uint4 sib = __ldcg(&T.aabb[is_left ? ridx : lidx]);
@@ -149,6 +166,17 @@ __device__ __forceinline__ void partner_insert(Partners& p, uint32_t b) {
     p.v[pos] = b;
 }
 
+// Batched scenes: first and last sorted leaf of every scene.
+__global__ void __launch_bounds__(kBpThreads) scene_range_kernel(uint32_t n, const uint64_t* __restrict__ codes64,
+                                                                 uint32_t* __restrict__ first,
+                                                                 uint32_t* __restrict__ last) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t sc = static_cast<uint32_t>(codes64[k] >> 30);
+    if (k == 0 || static_cast<uint32_t>(codes64[k - 1] >> 30) != sc) first[sc] = k;
+    if (k == n - 1 || static_cast<uint32_t>(codes64[k + 1] >> 30) != sc) last[sc] = k;
+}
+
 // Traversal record of every node (32 bytes): box + left child / body, then
 // lo, hi and the escape node — the right child of the internal node whose
 // split is hi (the next node in pre-order once this subtree is skipped), or -1
@@ -185,7 +213,7 @@ __global__ void __launch_bounds__(kBpThreads) finalize_nodes_kernel(uint32_t n_u
 // returns true the walk hands that subtree on instead of descending into it.
 template <typename F, typename G>
 __device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const BoxF& q, int k, bool me_big, int start,
-                                           int end_leaf, F&& visit, G&& frontier) {
+                                           int begin_leaf, int end_leaf, F&& visit, G&& frontier) {
     int node = start;
     int budget = 2 * n;
     while (node >= 0) {
@@ -196,6 +224,10 @@ __device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const Box
         const uint4 r0 = __ldg(&T.trav[2 * node]);
         const uint4 r1 = __ldg(&T.trav[2 * node + 1]);
         if (static_cast<int>(r1.x) > end_leaf) return;
+        if (static_cast<int>(r1.y) < begin_leaf) {  // subtree before the query's scene
+            node = static_cast<int>(r1.z);
+            continue;
+        }
         const bool before = static_cast<int>(r1.x) < k;
         const bool has_big = r1.w != 0u;
         const bool wanted = me_big ? (has_big && before) : (before || has_big);
@@ -222,7 +254,8 @@ __device__ __forceinline__ void walk_pairs(const BvhBuffers& T, int n, const Box
 // never decrease, so the walk stops at the first node that starts at or past
 // it). `visit(body)` is called for every overlapping leaf.
 template <typename F>
-__device__ __forceinline__ void walk(const BvhBuffers& T, int n, const BoxF& q, int leaf_end, F&& visit) {
+__device__ __forceinline__ void walk(const BvhBuffers& T, int n, const BoxF& q, int leaf_begin, int leaf_end,
+                                     F&& visit) {
     int node = 0;
     // A well-formed tree visits each node at most once; anything longer (or an
     // index outside the tree) is reported instead of followed.
@@ -235,6 +268,10 @@ __device__ __forceinline__ void walk(const BvhBuffers& T, int n, const BoxF& q, 
         const uint4 r0 = __ldg(&T.trav[2 * node]);
         const uint4 r1 = __ldg(&T.trav[2 * node + 1]);
         if (static_cast<int>(r1.x) >= leaf_end) return;
+        if (static_cast<int>(r1.y) < leaf_begin) {
+            node = static_cast<int>(r1.z);
+            continue;
+        }
         const BoxF nb = unpack_box(r0);
         if (box_overlap(nb, q)) {
             if (node >= n - 1) {
@@ -250,16 +287,29 @@ __device__ __forceinline__ void walk(const BvhBuffers& T, int n, const BoxF& q, 
 
 // All overlapping partners b > lo of a query box, smallest kMaxPartners kept.
 __device__ __forceinline__ uint32_t traverse(const BvhBuffers& T, int n, const BoxF& q, uint32_t a, uint32_t lo,
-                                             Partners& p) {
+                                             Partners& p, int leaf_begin, int leaf_end) {
     uint32_t count = 0;
     p.m = 0;
-    walk(T, n, q, n, [&](uint32_t b) {
+    walk(T, n, q, leaf_begin, leaf_end, [&](uint32_t b) {
         if (b > lo && b != a) {
             ++count;
             partner_insert(p, b);
         }
     });
     return count;
+}
+
+// Sorted-leaf range [begin, end] of the scene of leaf k (the whole tree for a
+// single scene).
+__device__ __forceinline__ void scene_leaves(const BvhBuffers& T, int n, int k, int& begin, int& end) {
+    if (!T.codes64) {
+        begin = 0;
+        end = n;
+        return;
+    }
+    const uint32_t sc = static_cast<uint32_t>(T.codes64[k] >> 30);
+    begin = static_cast<int>(T.scene_first[sc]);
+    end = static_cast<int>(T.scene_last[sc]);
 }
 
 __device__ __forceinline__ void bucket_pair(const BvhBuffers& T, uint32_t me, uint32_t other) {
@@ -287,8 +337,10 @@ __global__ void __launch_bounds__(kBpThreads) pair_find_kernel(uint32_t n_u, Bvh
         const BoxF q = unpack_box(r0);
         const uint32_t me = r0.w;
         const bool me_big = r1.w != 0u;
+        int sb, se;
+        scene_leaves(T, n, k, sb, se);
         walk_pairs(
-            T, n, q, k, me_big, 0, n, [&](uint32_t other) { bucket_pair(T, me, other); },
+            T, n, q, k, me_big, 0, sb, se, [&](uint32_t other) { bucket_pair(T, me, other); },
             [&](int node) {
                 if (m < static_cast<uint32_t>(kFrontierItems)) {
                     items[m++] = static_cast<uint32_t>(node);
@@ -314,14 +366,16 @@ __global__ void __launch_bounds__(kBpThreads) pair_find_kernel(uint32_t n_u, Bvh
     const BoxF q = unpack_box(__ldg(&T.trav[2 * (n - 1 + k)]));
     const uint32_t me = __ldg(&T.trav[2 * (n - 1 + k)]).w;
     const bool me_big = __ldg(&T.trav[2 * (n - 1 + k) + 1]).w != 0u;
+    int sb, se;
+    scene_leaves(T, n, k, sb, se);
     for (uint32_t i = 0; i < m; ++i) {
         if (first + i < queue_cap) {
             queue[first + i] = make_uint2(static_cast<uint32_t>(k), items[i]);
         } else {  // queue full: walk the subtree here
             const int f = static_cast<int>(items[i]);
-            const int end_leaf = static_cast<int>(__ldg(&T.trav[2 * f + 1]).y);
+            const int end_leaf = min(static_cast<int>(__ldg(&T.trav[2 * f + 1]).y), se);
             walk_pairs(
-                T, n, q, k, me_big, f, end_leaf, [&](uint32_t other) { bucket_pair(T, me, other); },
+                T, n, q, k, me_big, f, sb, end_leaf, [&](uint32_t other) { bucket_pair(T, me, other); },
                 [](int) { return false; });
         }
     }
@@ -340,9 +394,11 @@ __global__ void __launch_bounds__(kBpThreads) pair_subtree_kernel(uint32_t n_u, 
         const bool me_big = __ldg(&T.trav[2 * (n - 1 + k) + 1]).w != 0u;
         const BoxF q = unpack_box(r0);
         const uint32_t me = r0.w;
-        const int end_leaf = static_cast<int>(__ldg(&T.trav[2 * f + 1]).y);
+        int sb, se;
+        scene_leaves(T, n, k, sb, se);
+        const int end_leaf = min(static_cast<int>(__ldg(&T.trav[2 * f + 1]).y), se);
         walk_pairs(
-            T, n, q, k, me_big, f, end_leaf, [&](uint32_t other) { bucket_pair(T, me, other); },
+            T, n, q, k, me_big, f, sb, end_leaf, [&](uint32_t other) { bucket_pair(T, me, other); },
             [](int) { return false; });
     }
 }
@@ -402,7 +458,9 @@ __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, Bv
         Partners P;
         const uint32_t leaf = __ldg(&T.inv_sorted[a]);
         const BoxF q = unpack_box(__ldg(&T.trav[2 * (n - 1 + static_cast<int>(leaf))]));
-        traverse(T, n, q, a, a, P);
+        int sb, se;
+        scene_leaves(T, n, static_cast<int>(leaf), sb, se);
+        traverse(T, n, q, a, a, P, sb, se + 1);
         uint32_t written = 0;
         while (true) {
             for (int i = 0; i < P.m; ++i) {
@@ -411,7 +469,7 @@ __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, Bv
             }
             written += static_cast<uint32_t>(P.m);
             if (written >= cnt || P.m == 0) break;
-            traverse(T, n, q, a, P.v[P.m - 1], P);
+            traverse(T, n, q, a, P.v[P.m - 1], P, sb, se + 1);
         }
     }
     __syncthreads();
@@ -474,12 +532,21 @@ dyph_status broadphase_build(dyph_broadphase* bp, const dyph_bodies* bodies, con
     GlobalShapes S{*shapes};
     const uint32_t mblocks = std::max(1u, std::min((n + kBpThreads - 1) / kBpThreads, 2048u));
     morton_kernel<<<mblocks, kBpThreads, 0, s>>>(B, n, *bounds, bp->codes, bp->bvh.sorted_idx, bp->counts,
-                                                 bp->tstatus, n_tiles, bp->bvh.bucket_cnt);
+                                                 bp->tstatus, n_tiles, bp->bvh.bucket_cnt, bp->bvh.codes64,
+                                                 bp->bvh.scene_of, bp->scene_bounds);
     DYPH_CUDA_TRY(cudaGetLastError());
     bp->last_n = n;
     if (n < 2) return DYPH_OK;
-    dyph_status st = sort_u32_u32(bp->codes, bp->bvh.sorted_idx, n, 30, bp->sort_ws, bp->sort_ws_bytes, s);
+    dyph_status st = bp->bvh.codes64
+                         ? sort_u64_u32(bp->bvh.codes64, bp->bvh.sorted_idx, n, 30 + bp->scene_bits, bp->sort_ws,
+                                        bp->sort_ws_bytes, s)
+                         : sort_u32_u32(bp->codes, bp->bvh.sorted_idx, n, 30, bp->sort_ws, bp->sort_ws_bytes, s);
     if (st != DYPH_OK) return st;
+    if (bp->bvh.codes64) {
+        scene_range_kernel<<<(n + kBpThreads - 1) / kBpThreads, kBpThreads, 0, s>>>(
+            n, bp->bvh.codes64, bp->bvh.scene_first, bp->bvh.scene_last);
+        DYPH_CUDA_TRY(cudaGetLastError());
+    }
     const uint32_t leaf_blocks = (n + kBpThreads - 1) / kBpThreads;
     build_kernel<<<leaf_blocks, kBpThreads, 0, s>>>(B, S, n, bp->codes, bp->bvh.sorted_idx, bp->bvh);
     DYPH_CUDA_TRY(cudaGetLastError());
@@ -532,12 +599,60 @@ dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broa
     return DYPH_OK;
 }
 
+dyph_status broadphase_set_scenes(dyph_broadphase* bp, uint32_t n_scenes, const uint32_t* h_body_offset,
+                                  const dyph_aabb* h_scene_bounds) {
+    if (!bp || n_scenes == 0 || !h_body_offset || !h_scene_bounds) return DYPH_ERR_INVALID;
+    // Keys are (scene << 52 | code << 22 | body): at most 4096 scenes of a
+    // tree of at most 2^22 bodies.
+    if (n_scenes > 4096u || bp->max_bodies > (1u << 22) || h_body_offset[0] != 0u ||
+        h_body_offset[n_scenes] > bp->max_bodies)
+        return DYPH_ERR_INVALID;
+    for (uint32_t i = 0; i < n_scenes; ++i)
+        if (h_body_offset[i + 1] <= h_body_offset[i]) return DYPH_ERR_INVALID;  // every scene has a body
+    const uint32_t n = h_body_offset[n_scenes];
+    int bits = 0;
+    while ((1u << bits) < n_scenes) ++bits;
+    bool ok = true;
+    if (!bp->bvh.codes64) ok = dev_alloc(&bp->bvh.codes64, bp->max_bodies) == cudaSuccess &&
+                                 dev_alloc(&bp->bvh.scene_of, bp->max_bodies) == cudaSuccess;
+    if (bp->scene_bounds) cudaFree(bp->scene_bounds);
+    if (bp->bvh.scene_first) cudaFree(bp->bvh.scene_first);
+    if (bp->bvh.scene_last) cudaFree(bp->bvh.scene_last);
+    if (bp->body_offset) cudaFree(bp->body_offset);
+    bp->scene_bounds = nullptr;
+    bp->bvh.scene_first = bp->bvh.scene_last = bp->body_offset = nullptr;
+    ok = ok && dev_alloc(&bp->scene_bounds, n_scenes) == cudaSuccess &&
+         dev_alloc(&bp->bvh.scene_first, n_scenes) == cudaSuccess &&
+         dev_alloc(&bp->bvh.scene_last, n_scenes) == cudaSuccess &&
+         dev_alloc(&bp->body_offset, n_scenes + 1) == cudaSuccess;
+    if (!ok) return DYPH_ERR_NOMEM;
+    std::vector<uint32_t> scene_of(n);
+    for (uint32_t sc = 0; sc < n_scenes; ++sc)
+        for (uint32_t i = h_body_offset[sc]; i < h_body_offset[sc + 1]; ++i) scene_of[i] = sc;
+    DYPH_CUDA_TRY(cudaMemcpy(bp->bvh.scene_of, scene_of.data(), n * 4, cudaMemcpyHostToDevice));
+    DYPH_CUDA_TRY(cudaMemcpy(bp->scene_bounds, h_scene_bounds, n_scenes * sizeof(dyph_aabb), cudaMemcpyHostToDevice));
+    DYPH_CUDA_TRY(cudaMemcpy(bp->body_offset, h_body_offset, (n_scenes + 1) * 4, cudaMemcpyHostToDevice));
+    const size_t ws = sort_workspace_bytes(bp->max_bodies, 8);
+    if (ws > bp->sort_ws_bytes) {
+        if (bp->sort_ws) cudaFree(bp->sort_ws);
+        bp->sort_ws = nullptr;
+        bp->sort_ws_bytes = 0;
+        if (cudaMalloc(&bp->sort_ws, ws) != cudaSuccess) return DYPH_ERR_NOMEM;
+        bp->sort_ws_bytes = ws;
+    }
+    bp->n_scenes = n_scenes;
+    bp->scene_bits = bits;
+    return DYPH_OK;
+}
+
 void broadphase_destroy(dyph_broadphase* bp) {
     if (!bp) return;
     void* ptrs[] = {bp->codes, bp->bvh.sorted_idx, bp->bvh.sorted_keys, bp->bvh.inv_sorted, bp->bvh.left,
                     bp->bvh.right, bp->bvh.parent, bp->bvh.root, bp->bvh.aabb, bp->bvh.range_hi, bp->bvh.rsplit,
                     bp->bvh.slot, bp->bvh.flags, bp->pairs, bp->counts, bp->tstatus, bp->sort_ws,
-                    bp->bvh.range_lo, bp->bvh.trav, bp->bvh.bucket_cnt, bp->bvh.bucket, bp->bvh.big, bp->queue};
+                    bp->bvh.range_lo, bp->bvh.trav, bp->bvh.bucket_cnt, bp->bvh.bucket, bp->bvh.big, bp->queue,
+                    bp->bvh.codes64, bp->bvh.scene_of, bp->bvh.scene_first, bp->bvh.scene_last,
+                    bp->scene_bounds, bp->body_offset};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete bp;
@@ -586,4 +701,9 @@ extern "C" dyph_status dyph_broadphase_bvh_view(const dyph_broadphase* bp, uint3
     out->sorted_keys = bp->bvh.sorted_keys;
     out->n = n_active;
     return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_broadphase_set_scenes(dyph_broadphase* bp, uint32_t n_scenes, const uint32_t* body_offset,
+                                                  const dyph_aabb* scene_bounds) {
+    return dyph::broadphase_set_scenes(bp, n_scenes, body_offset, scene_bounds);
 }

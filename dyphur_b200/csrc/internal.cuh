@@ -30,6 +30,11 @@ struct BvhBuffers {
     uint32_t* big;          // [2n-1] 1 when the subtree holds a static body's leaf
     uint32_t* bucket_cnt;   // [n] candidate partners b > a found for body a
     uint32_t* bucket;       // [n * kBucket] first kBucket partners of body a (unordered)
+    // Batched scenes only (null for one scene):
+    uint64_t* codes64;      // [n] (scene << 30 | Morton code), sorted in place
+    uint32_t* scene_of;     // [n] scene of each body
+    uint32_t* scene_first;  // [n_scenes] first sorted leaf of each scene
+    uint32_t* scene_last;   // [n_scenes] last sorted leaf of each scene
 };
 
 // Partners kept per body by the Morton-order pass (a multiple of 32); bodies
@@ -48,6 +53,10 @@ struct dyph_broadphase {
     uint32_t* tstatus = nullptr; // traversal look-back status, one word per 256 bodies
     void* sort_ws = nullptr;
     size_t sort_ws_bytes = 0;
+    uint32_t n_scenes = 0;              // 0: one scene (bounds passed per build)
+    int scene_bits = 0;                 // bits of a scene index
+    dyph_aabb* scene_bounds = nullptr;  // [n_scenes] Morton bounds of each scene
+    uint32_t* body_offset = nullptr;    // [n_scenes + 1] first body of each scene
 };
 
 struct dyph_narrowphase {
@@ -94,6 +103,9 @@ dyph_status broadphase_create(uint32_t max_bodies, uint32_t max_pairs, dyph_broa
 void broadphase_destroy(dyph_broadphase* bp);
 dyph_status broadphase_build(dyph_broadphase* bp, const dyph_bodies* bodies, const dyph_shapes* shapes,
                              const dyph_aabb* bounds, cudaStream_t s);
+// Switch the broadphase to batched scenes (allocates; call outside graph capture).
+dyph_status broadphase_set_scenes(dyph_broadphase* bp, uint32_t n_scenes, const uint32_t* h_body_offset,
+                                  const dyph_aabb* h_scene_bounds);
 
 dyph_status narrowphase_create(uint32_t max_contacts, dyph_narrowphase** out);
 void narrowphase_destroy(dyph_narrowphase* np);

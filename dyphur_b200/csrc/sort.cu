@@ -320,6 +320,11 @@ dyph_status sort_u32_u32(uint32_t* keys, uint32_t* vals, size_t n, int key_bits,
     return radix_sort<uint32_t, true>(keys, vals, n, key_bits, ws, ws_size, s);
 }
 
+dyph_status sort_u64_u32(uint64_t* keys, uint32_t* vals, size_t n, int key_bits, void* ws, size_t ws_size,
+                         cudaStream_t s) {
+    return radix_sort<uint64_t, true>(keys, vals, n, key_bits, ws, ws_size, s);
+}
+
 }  // namespace dyph
 
 extern "C" size_t dyph_sort_workspace_bytes(size_t n) { return dyph::sort_workspace_bytes(n, 8); }

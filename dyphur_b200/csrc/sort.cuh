@@ -17,5 +17,7 @@ dyph_status sort_prepare();
 // Stable ascending sort of (keys, vals) on the low key_bits bits of keys.
 dyph_status sort_u32_u32(uint32_t* keys, uint32_t* vals, size_t n, int key_bits, void* ws, size_t ws_size,
                          cudaStream_t s);
+dyph_status sort_u64_u32(uint64_t* keys, uint32_t* vals, size_t n, int key_bits, void* ws, size_t ws_size,
+                         cudaStream_t s);
 
 }  // namespace dyph

@@ -23,6 +23,7 @@ struct dyph_world {
     cudaGraphExec_t graph = nullptr;
     cudaGraphExec_t episode = nullptr;  // n_frames frames in one graph (dyph_world_capture_episode)
     int32_t episode_frames = 0;
+    uint64_t* scene_hash = nullptr;  // [n_scenes] per-scene FNV-1a results
 };
 
 namespace dyph {
@@ -91,6 +92,7 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     if (w->ev_out) cudaEventDestroy(w->ev_out);
     if (w->stream) cudaStreamDestroy(w->stream);
     if (w->stats) cudaFree(w->stats);
+    if (w->scene_hash) cudaFree(w->scene_hash);
     broadphase_destroy(w->bp);
     narrowphase_destroy(w->np);
     xpbd_destroy(w->sv);
@@ -269,5 +271,36 @@ extern "C" dyph_status dyph_world_narrowphase(dyph_world* w, dyph_narrowphase** 
 extern "C" dyph_status dyph_world_solver(dyph_world* w, dyph_xpbd** out) {
     if (!w || !out) return DYPH_ERR_INVALID;
     *out = w->sv;
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset,
+                                             const dyph_aabb* scene_bounds) {
+    if (!w || !body_offset || n_scenes == 0 || body_offset[n_scenes] != w->desc.bodies.n) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    dyph_status st = broadphase_set_scenes(w->bp, n_scenes, body_offset, scene_bounds);
+    if (st != DYPH_OK) return st;
+    // Captured frames launch the single-scene form: record them again.
+    if (w->graph) cudaGraphExecDestroy(w->graph);
+    if (w->episode) cudaGraphExecDestroy(w->episode);
+    w->graph = nullptr;
+    w->episode = nullptr;
+    w->episode_frames = 0;
+    if (w->scene_hash) cudaFree(w->scene_hash);
+    w->scene_hash = nullptr;
+    if (cudaMalloc(&w->scene_hash, n_scenes * sizeof(uint64_t)) != cudaSuccess) return DYPH_ERR_NOMEM;
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uint64_t* host_out, uint32_t cap) {
+    if (!w || !host_out) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    const uint32_t n = w->bp->n_scenes ? w->bp->n_scenes : 1u;
+    if (cap < n) return DYPH_ERR_INVALID;
+    if (!w->scene_hash && cudaMalloc(&w->scene_hash, sizeof(uint64_t)) != cudaSuccess) return DYPH_ERR_NOMEM;
+    dyph_status st = fnv_state(&w->desc.bodies, w->bp->n_scenes ? w->bp->body_offset : nullptr, n, w->scene_hash, cs);
+    if (st != DYPH_OK) return st;
+    DYPH_CUDA_TRY(cudaMemcpyAsync(host_out, w->scene_hash, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
     return DYPH_OK;
 }

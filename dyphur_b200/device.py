@@ -297,6 +297,9 @@ class World:
         d.shapes = self.shapes.view
         d.scene_bounds = aabb(scene.bounds[0])
         d.integrator = capi.IntegratorParams((C.c_float * 3)(*scene.gravity), scene.dt, scene.n_substeps)
+        if scene.n_scenes > 1:  # capacities for all scenes together
+            max_pairs = max_pairs or 48 * scene.n_bodies + 64 * scene.n_scenes
+            max_contacts = max_contacts or 16 * scene.n_bodies + 64 * scene.n_scenes
         d.max_pairs = int(max_pairs or scene.max_pairs)
         d.max_contacts = int(max_contacts or scene.max_contacts)
         d.n_iters = scene.n_iters
@@ -306,6 +309,13 @@ class World:
         h = C.c_void_p()
         check(capi.lib().dyph_world_create(C.byref(d), None, C.byref(h)), "dyph_world_create")
         self.h = h
+        if scene.n_scenes > 1:
+            # Batched scenes: one tree over all scenes, pairs kept inside each scene.
+            off = np.ascontiguousarray(scene.body_offset, np.uint32)
+            bnds = (capi.AABB * scene.n_scenes)(*[aabb(b) for b in scene.bounds])
+            self._scene_offset = off
+            check(capi.lib().dyph_world_set_scenes(h, scene.n_scenes, off.ctypes.data, bnds),
+                  "dyph_world_set_scenes")
         bp, np_, sv = C.c_void_p(), C.c_void_p(), C.c_void_p()
         check(capi.lib().dyph_world_broadphase(h, C.byref(bp)))
         check(capi.lib().dyph_world_narrowphase(h, C.byref(np_)))
@@ -384,6 +394,13 @@ class World:
 
     def hash(self) -> int:
         return state_hash(self.bodies)
+
+    def scene_hashes(self, stream=None) -> np.ndarray:
+        """FNV-1a-64 of every scene's poses (uint64 array, one per scene)."""
+        n = self.scene.n_scenes
+        out = np.zeros(n, np.uint64)
+        check(capi.lib().dyph_world_scene_hashes(self.h, _stream_ptr(stream), out.ctypes.data, n))
+        return out
 
     def pairs(self) -> np.ndarray:
         L = capi.lib()

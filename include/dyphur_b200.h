@@ -204,6 +204,15 @@ const dyph_pair* dyph_broadphase_pairs(const dyph_broadphase* bp);
 const uint32_t* dyph_broadphase_count_ptr(const dyph_broadphase* bp);
 uint32_t dyph_broadphase_max_pairs(const dyph_broadphase* bp);
 dyph_status dyph_broadphase_bvh_view(const dyph_broadphase* bp, uint32_t n_active, dyph_bvh_view* out);
+/* Batched scenes (no reference counterpart: the reference steps one scene).
+ * Bodies [body_offset[s], body_offset[s+1]) form scene s, which is quantised
+ * against scene_bounds[s] and never paired with another scene. Morton keys
+ * become (scene << 30 | code) and sort scene-major, so every scene's leaves
+ * are contiguous. Each scene's pair list equals the pair list it has alone,
+ * shifted by its first body index. At most 4096 scenes and 2^22 bodies. Host
+ * arrays; allocates, so call outside stream capture. */
+dyph_status dyph_broadphase_set_scenes(dyph_broadphase* bp, uint32_t n_scenes, const uint32_t* body_offset,
+                                       const dyph_aabb* scene_bounds);
 
 /* ── narrowphase — replaces class Narrowphase
  *    (core/include/core/narrowphase.hpp:26-73, core/src/narrowphase.cpp:1053-1144).
@@ -273,6 +282,17 @@ dyph_status dyph_world_create(const dyph_world_desc* desc, dyph_stream s, dyph_w
 void dyph_world_destroy(dyph_world* w);
 /* Queue n_frames frame steps (graph-replayed after the first call). */
 dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_stream s);
+/* Batched scenes in one world (dyph_broadphase_set_scenes; desc.scene_bounds is
+ * then unused). Narrowphase and solver run over all scenes at once: contacts
+ * never join two scenes, so in DYPH_SOLVER_SEQUENTIAL every scene evolves
+ * bit-identically to stepping it alone. The coloured modes colour the whole
+ * batch (priorities are global contact indices), so their results differ from
+ * a scene stepped alone by the colouring's drift. Drops captured graphs. */
+dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset,
+                                  const dyph_aabb* scene_bounds);
+/* Blocking: FNV-1a-64 of every scene's pose arrays (one value for a single
+ * scene); cap >= number of scenes. */
+dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uint64_t* host_out, uint32_t cap);
 /* Blocking: peak pair / contact counts and the sticky status of the frames
  * stepped so far (overflow or timeout). */
 dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* last_pairs,
