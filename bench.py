@@ -177,6 +177,16 @@ def committed_traffic(stage: str, mean_algorithmic_bytes: float):
         return None
 
 
+def max_over_ranks(values, device="cpu"):
+    """Element-wise max of per-rank timings over the process group (the
+    slowest rank sets a multi-GPU step's time)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -262,9 +272,7 @@ def run_b200(args) -> None:
     e2e_ms = e0.elapsed_time(e1)
 
     if world > 1:
-        t = torch.tensor([ms, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+        ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
     body_steps = world * args.steps * args.frames * n
     value = body_steps / (ms / 1e3)
     e2e = body_steps / (e2e_ms / 1e3)
