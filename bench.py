@@ -365,8 +365,9 @@ def run_reference(args) -> None:
         vals.append(r["value"])
     vals = vals[max(args.warmup, 3):]
     value = statistics.mean(vals)
+    ms_step = (args.bodies + 1) * frames / value * 1e3 if value else None  # one sample of `frames` frames
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "bodies": args.bodies + 1, "parallelism": "host OpenMP"},
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores if which == "ref" else 1,

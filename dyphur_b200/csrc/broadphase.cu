@@ -406,9 +406,9 @@ __global__ void __launch_bounds__(kBpThreads) pair_subtree_kernel(uint32_t n_u, 
 // Pass 2, one thread per body in body order: place each body's pairs with a
 // block scan + decoupled look-back (the counts are final after pass 1, so
 // every tile publishes its aggregate at once), then write them sorted by b.
-// Buckets of up to kMaxPartners are sorted by their own thread; larger ones
-// go to a block queue and each warp ranks one bucket at a time; buckets that
-// overflowed are rebuilt by a full traversal from the body's own leaf.
+// Buckets go to a block queue and each warp ranks one bucket at a time
+// (coalesced loads and stores); buckets that overflowed are rebuilt by a full
+// traversal from the body's own leaf.
 __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, BvhBuffers T, uint2* __restrict__ pairs,
                                                                 uint32_t max_pairs, uint32_t* __restrict__ counts,
                                                                 uint32_t* __restrict__ tstatus) {
@@ -440,20 +440,11 @@ __global__ void __launch_bounds__(kBpThreads) pair_write_kernel(uint32_t n_u, Bv
     }
     __syncthreads();
     const uint32_t off = s_excl + excl_block;
-    if (cnt > static_cast<uint32_t>(kMaxPartners) && cnt <= static_cast<uint32_t>(kBucket)) {
+    if (cnt != 0u && cnt <= static_cast<uint32_t>(kBucket)) {
         const uint32_t qi = atomicAdd(&s_nbig, 1u);
         s_big[qi] = a;
         s_big_off[qi] = off;
         s_big_cnt[qi] = cnt;
-    }
-    if (cnt != 0u && cnt <= static_cast<uint32_t>(kMaxPartners)) {
-        Partners P;
-        P.m = 0;
-        for (uint32_t i = 0; i < cnt; ++i) partner_insert(P, T.bucket[static_cast<size_t>(a) * kBucket + i]);
-        for (int i = 0; i < P.m; ++i) {
-            const uint32_t pos = off + static_cast<uint32_t>(i);
-            if (pos < max_pairs) pairs[pos] = make_uint2(a, P.v[i]);
-        }
     } else if (cnt > static_cast<uint32_t>(kBucket)) {
         Partners P;
         const uint32_t leaf = __ldg(&T.inv_sorted[a]);
