@@ -118,7 +118,8 @@ typedef enum dyph_solver_mode {
      * colour order. Bit-identical to the reference. */
     DYPH_SOLVER_REFERENCE = 0,
     /* XpbdSolver::set_force_serial(true) (core/include/core/xpbd_solver.hpp:48):
-     * sorted contact order, run as a level schedule (bit-identical). */
+     * sorted contact order, run as a dependency schedule on per-body contact
+     * lists (one block at <= 2048 contacts), bit-identical to the serial loop. */
     DYPH_SOLVER_SEQUENTIAL = 1,
     /* Jones–Plassmann colours at every contact count (no sequential threshold):
      * the fast mode for batched small scenes; its drift against the
