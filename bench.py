@@ -148,9 +148,13 @@ def stage_bytes(stage: str, n: int, pairs: np.ndarray, contacts: np.ndarray) -> 
     return 300.0 * c + 32.0 * n  # solver: contact rows + both bodies read/written, renormalise
 
 
-def kernels_per_frame(n: int) -> int:
+def kernels_per_frame(n: int, n_scenes: int = 1) -> int:
     """Library kernels one frame launches (matches the ncu launch list in profiles/)."""
-    sort = 1 if n <= 4096 else 5  # one-block sort, or histogram + 4 onesweep passes
+    if n_scenes > 1:  # (scene << 30 | code) keys: histogram + one pass per 8 key bits, + scene ranges
+        key_bits = 30 + max(1, (n_scenes - 1).bit_length())
+        sort = (1 if n <= 4096 else 1 + (key_bits + 7) // 8) + 1
+    else:
+        sort = 1 if n <= 4096 else 5  # one-block sort, or histogram + 4 onesweep passes
     # integrate, morton, sort, build, finalize, pair find (two passes), pair write, narrowphase,
     # solver (dataflow, round-synchronous, sequential: two of them return at once), stats
     return 1 + 1 + sort + 1 + 1 + 2 + 1 + 1 + 3 + 1
@@ -305,7 +309,7 @@ def run_b200(args) -> None:
                          "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic,
                          "stage_ms_per_frame": float(probe.mean()),
                          "stage_share_of_step": float(probe.sum() / (ms / args.steps))},
-            "gpu_launches": int(args.steps * args.frames * kernels_per_frame(n)),
+            "gpu_launches": int(args.steps * args.frames * kernels_per_frame(n, scene.n_scenes)),
             "clocks": ck, "overflow_status": st["status"],
         }
         if args.workload == "batch":
