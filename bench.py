@@ -1,26 +1,41 @@
 #!/usr/bin/env python3
 """Frame-step benchmark (body-steps/s) on B200.
 
-Workload: the large single-scene stress — 65536 bodies (70 % boxes with half
-extents U[0.1, 0.5] m, 30 % spheres with r U[0.1, 0.4] m, density 500 kg/m^3)
-dropped from a 40 m cube onto an 80 x 1 x 80 m ground, 600 frames at 60 Hz,
-fp32, synthetic seeded input. One step = one 600-frame episode from the
-initial state (the state is reset at the start of every step), replayed as one
-CUDA graph through the library's world API.
+Default workload — the batched forward configuration the headline metric
+("batched vs per-scene at <= 1e-3 m drift") is quoted on: 4096 independent
+scenes (box stacks or sphere piles, 8-256 bodies log-uniform, seed 3, each on
+its own ground) stepped together as one world, 240 frames at 60 Hz, fp32,
+synthetic seeded input. One step = one 240-frame episode of the whole batch
+from its initial state, replayed as one CUDA graph.
 
-  value  device-resident body-steps/s: the initial state is already in HBM.
-  e2e    the same through the C-ABI world with host buffers: every step uploads
-         the bodies from pinned host memory and downloads the final state.
+  value       device-resident body-steps/s of the batch in sequential order
+              (every scene bit-identical to the reference's sequential
+              order: pose drift 0)
+  per_scene   the plain per-scene GPU path (each scene its own world) on a
+              sample of the same scenes, and the batched / per-scene ratio
+  colored     the batch in the Jones-Plassmann coloured order: its
+              body-steps/s and its pose drift and penetration against the
+              sequential order
+  e2e         the same metric through the C-ABI world with host buffers:
+              every step uploads the initial state from pinned host memory,
+              downloads the poses every other frame (the reference loop's
+              trajectory, examples/stress_test_blocks/main.cpp:275-278) and
+              reads the final state back
+  single_scene  the large single-scene stress (65,536 bodies, 600 frames) on
+              the same terms, with its own CPU baseline
 
-Multi-GPU (torchrun): replicas only — each rank simulates its own scene, no
-collective on the data path; the timed region is the max over ranks.
-`--impl reference` times the reference's own frame-step sources (built on the
-host SYCL shim with OpenMP) on the host cores instead.
+`--workload single` prints the single-scene line alone.
+Multi-GPU (torchrun): replicas only — each rank runs its own copy of the
+workload (its own seed), no collective on the data path; the timed region is
+the max over ranks. `--impl reference` times the reference's own frame-step
+sources (built on the host with the SYCL shim, oracle/_ref) on the host cores
+on the same workload; that arm never loads the GPU library.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import multiprocessing as mp
 import os
 import statistics
 import subprocess
@@ -33,11 +48,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-WORKLOAD = ("large single-scene stress: 65536 bodies (70% boxes half-extent U[0.1,0.5] m, 30% spheres "
-            "r U[0.1,0.4] m, 500 kg/m^3, random rotations, v N(0,0.5) m/s) in a 40 m cube over an "
-            "80x1x80 m ground, 600 frames at 60 Hz, fp32")
 METRIC = "body-steps/s"
-STAGES = ("integrate", "broadphase", "narrowphase", "solver")
+BATCH = dict(n_scenes=4096, lo=8, hi=256, seed=3, frames=240)
+SINGLE = dict(bodies=65536, seed=2, frames=600)
+BATCH_WORKLOAD = ("batched forward: 4096 independent scenes (jittered box stacks or sphere piles, 8-256 bodies "
+                  "log-uniform, h = r = 0.4 m, each on its own ground), 240 frames at 60 Hz, fp32, one world")
+SINGLE_WORKLOAD = ("large single-scene stress: 65536 bodies (70% boxes half-extent U[0.1,0.5] m, 30% spheres "
+                   "r U[0.1,0.4] m, 500 kg/m^3, random rotations, v N(0,0.5) m/s) in a 40 m cube over an "
+                   "80x1x80 m ground, 600 frames at 60 Hz, fp32")
+STAGES = ("integrate", "broadphase", "narrowphase", "solver", "flow_solve_kernel")
+MODES = {"reference": 0, "sequential": 1, "colored": 2}
+FLOW_THREADS = 148 * 2 * 256  # resident threads of the dataflow solver kernel (2 blocks x 256 per SM)
 
 
 def parse():
@@ -46,52 +67,190 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="single", choices=["single", "batch"],
-                    help="single: the 65k-body pile; batch: 4096 independent scenes of 8-256 bodies")
-    ap.add_argument("--scenes", type=int, default=4096)
+    ap.add_argument("--workload", default="batch", choices=["batch", "single"])
+    ap.add_argument("--mode", default=None, choices=list(MODES),
+                    help="solver order (default: sequential for the batch, reference for the single scene)")
     ap.add_argument("--frames", type=int, default=None)
-    ap.add_argument("--start-frame", type=int, default=0,
-                    help="step the pile this many frames (untimed) before recording the episode")
-    ap.add_argument("--bodies", type=int, default=65536)
-    ap.add_argument("--probe-stage", default="solver", choices=STAGES)
-    ap.add_argument("--mode", default="reference", choices=["reference", "sequential", "colored"])
+    ap.add_argument("--no-single", action="store_true", help="batch line without the single-scene object")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--cpu-frames", type=int, default=60)
+    ap.add_argument("--cpu-single-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
-# ── CPU baseline (reference build or oracle port), run in a child process ────
+_T0 = time.perf_counter()
 
-def cpu_worker(which: str, bodies: int, frames: int) -> None:
+
+def note(msg: str) -> None:
+    """Progress of the run on stderr (wall seconds since start)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ── CPU side: the reference's own sources (oracle/_ref) on the host cores ────
+
+def checker_kind():
+    from oracle import oracle
+    return "ref" if oracle.ref_available() else "oracle"
+
+
+_POOL_STATE = {}
+
+
+def _batch_worker_init(which: str, cfg: dict) -> None:
     from dyphur_b200 import scenes
     from oracle import oracle
-    s = scenes.random_pile(bodies)
-    w = oracle.World(s, which)
-    t0 = time.perf_counter()
-    rc = w.step(frames)
-    dt = time.perf_counter() - t0
-    print(json.dumps({"rc": rc, "seconds": dt, "frames": frames, "bodies": s.n_bodies}))
+    _POOL_STATE["which"] = which
+    _POOL_STATE["batch"] = scenes.batch(cfg["n_scenes"], cfg["lo"], cfg["hi"], cfg["seed"],
+                                        builder=oracle.scene_builder(which))
 
 
-def cpu_baseline(bodies: int, frames: int) -> dict | None:
+def _batch_worker_scene(job):
+    """Step one scene of the batch alone on one host thread in the given solver
+    order (1: XpbdSolver::set_force_serial(true)); returns (body-steps, seconds, rc)."""
     from oracle import oracle
-    which = "ref" if oracle.ref_available() else "oracle"
+    i, frames, mode = job
+    sc = _POOL_STATE["batch"].scene(i)
+    w = oracle.World(sc, _POOL_STATE["which"])
+    t0 = time.perf_counter()
+    rc = w.step(frames, mode)
+    dt = time.perf_counter() - t0
+    w.close()
+    return sc.n_bodies * frames, dt, rc
+
+
+class BatchCpu:
+    """The reference build stepping scenes of the batch one per host core (the
+    reference steps one scene at a time; independent scenes run side by side)."""
+
+    def __init__(self, cfg: dict, cores: int):
+        self.which = checker_kind()
+        self.cfg = cfg
+        self.cores = cores
+        env_omp = os.environ.get("OMP_NUM_THREADS")
+        os.environ["OMP_NUM_THREADS"] = "1"  # one thread per scene; inherited by the spawned workers
+        ctx = mp.get_context("spawn")
+        self.pool = ctx.Pool(cores, initializer=_batch_worker_init, initargs=(self.which, cfg))
+        if env_omp is None:
+            del os.environ["OMP_NUM_THREADS"]
+        else:
+            os.environ["OMP_NUM_THREADS"] = env_omp
+
+    def run(self, scene_ids, frames: int, mode: int = 1):
+        """Whole-job wall time of stepping these scenes on all workers."""
+        t0 = time.perf_counter()
+        res = self.pool.map(_batch_worker_scene, [(int(i), frames, mode) for i in scene_ids], chunksize=1)
+        wall = time.perf_counter() - t0
+        if any(r[2] != 0 for r in res):
+            raise RuntimeError("reference build returned an error")
+        return sum(r[0] for r in res), wall, sum(r[1] for r in res)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def batch_cpu_baseline(cfg: dict, sample_stride: int = 4) -> dict | None:
     cores = os.cpu_count() or 1
-    env = dict(os.environ)
-    env["OMP_NUM_THREADS"] = str(cores if which == "ref" else 1)
-    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", which, "--bodies", str(bodies),
-           "--cpu-frames", str(frames)]
     try:
-        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900, check=True)
-        r = json.loads(out.stdout.strip().splitlines()[-1])
+        cpu = BatchCpu(cfg, cores)
+        ids = np.arange(0, cfg["n_scenes"], sample_stride)
+        bs, wall, _ = cpu.run(ids, cfg["frames"])
+        one = np.arange(0, cfg["n_scenes"], cfg["n_scenes"] // 16)
+        bs1, _, busy1 = cpu.run(one, cfg["frames"])
+        cpu.close()
     except Exception as e:  # the baseline is reported, not required
         print(f"cpu baseline failed: {e}", file=sys.stderr)
         return None
-    return {"value": r["bodies"] * r["frames"] / r["seconds"], "unit": METRIC,
-            "cores": cores if which == "ref" else 1, "kind": "reference" if which == "ref" else "port",
-            "sample": f"frames 0-{frames - 1} of the same 600-frame episode ({r['seconds']:.1f} s, "
-                      f"{'reference sources, OpenMP' if which == 'ref' else 'C oracle, 1 thread'})"}
+    kind = "reference" if cpu.which == "ref" else "port"
+    return {"value": bs / wall, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"every {sample_stride}th scene of the batch ({len(ids)} scenes, {cfg['frames']} frames each, "
+                      f"{wall:.1f} s), one scene per host core, sequential order (set_force_serial)",
+            "single_thread": {"value": bs1 / busy1, "unit": METRIC, "cores": 1,
+                              "sample": f"{len(one)} scenes, {cfg['frames']} frames each, per-scene step time"}}
+
+
+def _single_cpu_worker(spec: str) -> None:
+    """Child process: the reference build on the pile. spec = 'full:<frames>'
+    times frames 0..frames-1; 'windows:<w>:<n>:<total>' steps the episode
+    untimed saving checkpoints every w frames, then times n windows of w
+    frames each, cycling over the episode from its checkpoints;
+    'ckpt:<file.npy>:<w>' times a window of w frames from each state in the
+    file (states the GPU path produced; it is bit-identical to the reference at
+    every frame of this episode, tests/test_gpu_late_frames.py)."""
+    from dyphur_b200 import scenes
+    from oracle import oracle
+    which = checker_kind()
+    s = scenes.random_pile(SINGLE["bodies"], SINGLE["seed"], builder=oracle.scene_builder(which))
+    w = oracle.World(s, which)
+    parts = spec.split(":")
+    out = {"bodies": s.n_bodies, "which": which}
+    if parts[0] == "full":
+        frames = int(parts[1])
+        t0 = time.perf_counter()
+        rc = w.step(frames, 0)
+        out.update(rc=rc, seconds=time.perf_counter() - t0, frames=frames)
+        print(json.dumps(out), flush=True)
+        return
+    if parts[0] == "ckpt":
+        ckpt = list(np.load(parts[1]))
+        win, n_win = int(parts[2]), len(ckpt)
+    else:
+        win, n_win, total = int(parts[1]), int(parts[2]), int(parts[3])
+        ckpt = []
+        for f in range(0, total, win):
+            ckpt.append(w.state())
+            w.step(win, 0)
+    secs = []
+    for k in range(n_win):
+        w.set_state(ckpt[k % len(ckpt)])
+        t0 = time.perf_counter()
+        rc = w.step(win, 0)
+        secs.append(time.perf_counter() - t0)
+        if rc != 0:
+            out["rc"] = rc
+            break
+    out.update(rc=out.get("rc", 0), window_seconds=secs, frames=win)
+    print(json.dumps(out), flush=True)
+
+
+def run_single_cpu(spec: str, threads: int, timeout: int = 1200) -> dict:
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(threads)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-single-worker", spec]
+    out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=timeout, check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def single_cpu_baseline(frames: int, ckpt_states: np.ndarray, ckpt_frames, win: int) -> dict | None:
+    """The reference build on windows of `win` frames spread over the episode,
+    each started from the GPU path's state at that frame, OpenMP on every core;
+    plus frames 0-9 on one thread."""
+    import tempfile
+    cores = os.cpu_count() or 1
+    try:
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "ckpt.npy")
+            np.save(path, ckpt_states)
+            r = run_single_cpu(f"ckpt:{path}:{win}", cores)
+        r1 = run_single_cpu("full:10", 1)
+    except Exception as e:
+        print(f"cpu baseline failed: {e}", file=sys.stderr)
+        return None
+    if r["rc"] != 0 or r1["rc"] != 0:
+        return None
+    kind = "reference" if r["which"] == "ref" else "port"
+    secs = sum(r["window_seconds"])
+    return {"value": r["bodies"] * win * len(r["window_seconds"]) / secs, "unit": METRIC, "cores": cores,
+            "kind": kind,
+            "sample": f"{len(ckpt_frames)} windows of {win} frames starting at frames {list(ckpt_frames)} of the "
+                      f"{frames}-frame episode ({secs:.1f} s), each from the state the GPU path reached there, "
+                      f"OpenMP on every core",
+            "single_thread": {"value": r1["bodies"] * 10 / r1["seconds"], "unit": METRIC, "cores": 1,
+                              "sample": "frames 0-9 of the episode, one thread"}}
 
 
 # ── clocks sampler ───────────────────────────────────────────────────────────
@@ -132,20 +291,29 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
 
 
-# ── algorithmic bytes per stage launch (per frame) ──────────────────────────
+# ── algorithmic bytes ────────────────────────────────────────────────────────
 
-def stage_bytes(stage: str, n: int, pairs: np.ndarray, contacts: np.ndarray) -> np.ndarray:
-    """Compulsory bytes of one frame's stage: each input read once, each output
-    written once (per body / pair / contact figures of the frame-step data)."""
-    p = pairs.astype(np.float64)
-    c = contacts.astype(np.float64)
-    if stage == "integrate":
-        return np.full_like(p, 100.0 * n)
-    if stage == "broadphase":
-        return 160.0 * n + 8.0 * p
-    if stage == "narrowphase":
-        return 72.0 * p + 36.0 * c
-    return 300.0 * c + 32.0 * n  # solver: contact rows + both bodies read/written, renormalise
+def frame_bytes(n: int, pairs: np.ndarray, contacts: np.ndarray) -> np.ndarray:
+    """Compulsory bytes of one frame (each input read once, each output written
+    once): 424 per body, 32 per candidate pair, 72 per contact."""
+    return 424.0 * n + 32.0 * pairs.astype(np.float64) + 72.0 * contacts.astype(np.float64)
+
+
+def flow_kernel_bytes(n: int, contacts: np.ndarray) -> np.ndarray:
+    """Compulsory bytes of one dataflow-solver launch: per body the state it
+    reads (80 B: pose, velocities, inverse mass and inertia) and writes (52 B),
+    per contact its 36-byte row."""
+    return 132.0 * n + 36.0 * contacts.astype(np.float64)
+
+
+def flow_kernel_active(contacts: np.ndarray, mode: int) -> np.ndarray:
+    """Frames on which the dataflow kernel does the solve: the sequential order
+    at <= 2048 contacts and the reference order at <= 256 run the one-block
+    kernel, empty frames nothing, more than 16 contacts per resident thread the
+    round-synchronous kernel."""
+    c = contacts.astype(np.int64)
+    seq = (mode == 1) | ((mode == 0) & (c <= 256))
+    return (c > 0) & ~(seq & (c <= 2048)) & (c <= 16 * FLOW_THREADS)
 
 
 def kernels_per_frame(n: int, n_scenes: int = 1) -> int:
@@ -168,14 +336,13 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def committed_traffic(stage: str, mean_algorithmic_bytes: float):
-    """DRAM bytes per launch of the stage, from the committed ncu capture
+def committed_traffic(key: str, mean_algorithmic_bytes: float):
+    """DRAM bytes per launch of the kernel from the committed ncu capture
     (profiles/traffic.json), scaled from the captured launch's units to the
-    episode's mean launch by the ratio of algorithmic bytes."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+    mean launch by the ratio of algorithmic bytes."""
     try:
-        with open(path) as f:
-            rec = json.load(f).get(stage)
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            rec = json.load(f)[key]
         return float(rec["dram_bytes"]) * mean_algorithmic_bytes / float(rec["algorithmic_bytes"])
     except Exception:
         return None
@@ -191,35 +358,10 @@ def max_over_ranks(values, device="cpu"):
     return [float(x) for x in t.cpu()]
 
 
-def run_b200(args) -> None:
-    import torch
-    import torch.distributed as dist
+# ── GPU side ─────────────────────────────────────────────────────────────────
 
-    from dyphur_b200 import capi, device, scenes
-
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    mode = {"reference": capi.SOLVER_REFERENCE, "sequential": capi.SOLVER_SEQUENTIAL,
-            "colored": capi.SOLVER_COLORED}[args.mode]
-    if args.workload == "batch":
-        # independent scenes in one world; sequential order keeps each scene exact
-        scene = scenes.batch(args.scenes, 8, 256, seed=3 + rank)
-        if args.mode == "reference":
-            mode = capi.SOLVER_SEQUENTIAL
-            args.mode = "sequential"
-    else:
-        scene = scenes.random_pile(args.bodies, seed=2 + rank)  # replicas: one scene per rank
-    n = scene.n_bodies
-    w = device.World(scene, mode=mode)
-    if args.start_frame > 0:
-        w.step(args.start_frame)
-    stage_idx = STAGES.index(args.probe_stage)
-    w.capture_episode(args.frames, stage_idx)
+def timed_episodes(w, steps, warmup, torch, barrier, clocks=None):
+    """Device time (ms) of `steps` episodes, each from the world's initial state."""
     fb = w.bodies.fbuf
     init = fb.clone()
     stream = torch.cuda.current_stream()
@@ -228,108 +370,162 @@ def run_b200(args) -> None:
         fb.copy_(init, non_blocking=True)
         w.run_episode(stream)
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         episode()
     torch.cuda.synchronize()
-    assert w.stats()["status"] == 0, "overflow during warm-up"
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    # ── device-resident timed region ──
-    clocks = Clocks(local)
     barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    if clocks:
+        clocks.start()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         episode()
     t1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ck = clocks.stop()
-    ms = t0.elapsed_time(t1)
-    probe = w.probe_ms()  # per-frame probed-stage durations of the last timed episode
-    pairs, contacts = w.history(args.frames)
-    st = w.stats()
+    ck = clocks.stop() if clocks else None
+    fb.copy_(init)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1), ck, init
 
-    # ── end-to-end through the C-ABI world with host buffers ──
+
+def e2e_episodes(w, init, frames, steps, torch, barrier):
+    """The same episodes through the C-ABI world with host buffers: initial
+    state uploaded from pinned memory, poses downloaded every other frame into
+    a pinned trajectory buffer, final state read back."""
+    fb = w.bodies.fbuf
+    n = w.bodies.n
+    stream = torch.cuda.current_stream()
     host_in = init.cpu().pin_memory()
     host_out = torch.empty((13, fb.shape[1]), dtype=torch.float32).pin_memory()
-    for _ in range(2):
+    records = (frames + 1) // 2
+    traj = torch.empty((records, n, 7), dtype=torch.float32).pin_memory()
+    w.set_trajectory(traj, 2)
+    w.capture_episode(frames, -1)
+
+    def step():
         fb.copy_(host_in, non_blocking=True)
         w.run_episode(stream)
         host_out.copy_(fb[:13], non_blocking=True)
+
+    for _ in range(2):
+        step()
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        fb.copy_(host_in, non_blocking=True)
-        w.run_episode(stream)
-        host_out.copy_(fb[:13], non_blocking=True)
+    for _ in range(steps):
+        step()
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-
-    if world > 1:
-        ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
-    body_steps = world * args.steps * args.frames * n
-    value = body_steps / (ms / 1e3)
-    e2e = body_steps / (e2e_ms / 1e3)
-
-    if rank == 0:
-        bytes_f = stage_bytes(args.probe_stage, n, pairs, contacts)
-        achieved = float(bytes_f.sum() / (probe.sum() / 1e3) / 1e9) if probe.sum() > 0 else None
-        peak, peak_kind = peaks()
-        traffic = committed_traffic(args.probe_stage, float(bytes_f.mean())) if len(bytes_f) else None
-        line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bodies": n, "frames_per_step": args.frames,
-                       "start_frame": args.start_frame,
-                       "solver_mode": args.mode, "parallelism": f"replicas{world}",
-                       "l2": "no flush: each step re-simulates the whole episode from its initial state, and "
-                             "a frame's data (~50-130 MB touched per frame at 65k bodies, about the 126 MB L2) "
-                             "is produced on the device by the previous stage or frame",
-                       "mean_pairs_per_frame": float(pairs.mean()) if len(pairs) else None,
-                       "mean_contacts_per_frame": float(contacts.mean()) if len(contacts) else None,
-                       "contacts_per_s": float(contacts.sum() * world * args.steps / (ms / 1e3))
-                       if len(contacts) else None},
-            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": int(host_in.numel() * 4),
-                    "d2h_bytes_per_step": int(host_out.numel() * 4)},
-            "roofline": {"bound": "hbm", "kernel": f"{args.probe_stage} stage (CUDA events per frame, last "
-                                                    f"timed step, {len(probe)} launches)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None,
-                         "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic,
-                         "stage_ms_per_frame": float(probe.mean()),
-                         "stage_share_of_step": float(probe.sum() / (ms / args.steps))},
-            "gpu_launches": int(args.steps * args.frames * kernels_per_frame(n, scene.n_scenes)),
-            "clocks": ck, "overflow_status": st["status"],
-        }
-        if args.workload == "batch":
-            line["config"]["workload"] = (f"batched forward: {scene.n_scenes} independent scenes (box stacks or "
-                                          f"sphere piles, 8-256 bodies log-uniform, each on its own ground), "
-                                          f"{args.frames} frames at 60 Hz, fp32, one world")
-            line["config"]["scenes"] = scene.n_scenes
-            line["per_scene"] = per_scene_baseline(scene, args.frames, mode, torch, device)
-            line["per_scene"]["batched_over_per_scene"] = value / line["per_scene"]["value"]
-        elif not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(args.bodies, args.cpu_frames)
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ms = e0.elapsed_time(e1)
+    w.set_trajectory(None)
+    h2d = host_in.numel() * 4
+    d2h = host_out.numel() * 4 + traj.numel() * 4
+    return ms, h2d, d2h
 
 
-def per_scene_baseline(scene, frames: int, mode: int, torch, device, sample: int = 64) -> dict:
+def probe_flow_kernel(w, frames, mode, torch):
+    """Per-frame device time of the dataflow solver kernel alone (events in the
+    episode graph around that launch), the counts of the frames, and the
+    roofline of that kernel."""
+    stream = torch.cuda.current_stream()
+    fb = w.bodies.fbuf
+    init = fb.clone()
+    w.capture_episode(frames, STAGES.index("flow_solve_kernel"))
+    for _ in range(2):
+        fb.copy_(init)
+        w.run_episode(stream)
+    torch.cuda.synchronize()
+    probe = w.probe_ms()
+    pairs, contacts = w.history(frames)
+    fb.copy_(init)
+    torch.cuda.synchronize()
+    n = w.bodies.n
+    act = flow_kernel_active(contacts, mode)
+    b = flow_kernel_bytes(n, contacts)
+    peak, peak_kind = peaks()
+    achieved = float(b[act].sum() / (probe[act].sum() / 1e3) / 1e9) if act.any() and probe[act].sum() > 0 else None
+    return {"bound": "hbm", "kernel": "flow_solve_kernel",
+            "launches_timed": int(act.sum()),
+            "algorithmic_bytes_per_launch": float(b[act].mean()) if act.any() else None,
+            "bytes_rule": "132 B per body (read 80, write 52) + 36 B per contact row",
+            "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_source": f"{peak_kind} hbm_gbs",
+            "traffic": committed_traffic("flow_solve_kernel", float(b[act].mean())) if act.any() else None,
+            "kernel_ms_per_launch": float(probe[act].mean()) if act.any() else None}, pairs, contacts, probe
+
+
+def gpu_workload(scene, mode, frames, args, torch, barrier, clocks=None, roofline=True):
+    from dyphur_b200 import device
+    w = device.World(scene, mode=mode)
+    w.capture_episode(frames, -1)
+    ms, ck, init = timed_episodes(w, args.steps, args.warmup, torch, barrier, clocks)
+    st = w.stats()
+    out = {"ms": ms, "clocks": ck, "status": st["status"], "world": w, "init": init}
+    if roofline:
+        out["roofline"], out["pairs"], out["contacts"], _ = probe_flow_kernel(w, frames, mode, torch)
+    return out
+
+
+def final_state(scene, mode, frames, torch):
+    from dyphur_b200 import device
+    w = device.World(scene, mode=mode)
+    w.step(frames)
+    torch.cuda.synchronize()
+    st = w.state()
+    _, p7 = w.contacts()
+    w.close()
+    return st, p7
+
+
+def drift_report(scene, frames, torch) -> dict:
+    """Coloured order against the sequential order on the batch: pose drift
+    (max over bodies of the position distance, and of the rotation angle) at
+    a few frames and after the episode, the one-frame drift from a shared
+    state, and the penetration (contact depth) after the last frame."""
+    from dyphur_b200 import device
+    ws, wc = device.World(scene, mode=1), device.World(scene, mode=2)
+    at, out, cur = (10, 30, 60, 120, frames), {}, 0
+    for f in at:
+        ws.step(f - cur)
+        wc.step(f - cur)
+        cur = f
+        a, b = ws.state(), wc.state()
+        dp = np.sqrt(((a[:3] - b[:3]) ** 2).sum(0))
+        dq = np.abs((a[3:7] * b[3:7]).sum(0)).clip(0.0, 1.0)
+        out[f] = (float(dp.max()), float(2.0 * np.arccos(dq).max()))
+    one = []
+    sq = device.World(scene, mode=1)
+    cur = 0
+    for f in (30, 120, frames - 2):
+        sq.step(f - cur)
+        wc.bodies.set_state(sq.state())
+        sq.step(1)
+        wc.step(1)
+        cur = f + 1
+        one.append(float(np.sqrt(((sq.state()[:3] - wc.state()[:3]) ** 2).sum(0)).max()))
+    _, cs = ws.contacts()
+    _, cc = wc.contacts()
+    for x in (ws, wc, sq):
+        x.close()
+    return {"vs": "sequential order, same scenes, same initial state",
+            "max_pose_drift_m": out[frames][0], "max_rot_drift_rad": out[frames][1],
+            "max_pose_drift_m_at_frame": {str(f): out[f][0] for f in at},
+            "one_frame_drift_m": one, "one_frame_drift_frames": [30, 120, frames - 2],
+            "penetration_after_settling_m": {"colored_max": float(cc[:, 6].max()) if len(cc) else 0.0,
+                                             "colored_mean": float(cc[:, 6].mean()) if len(cc) else 0.0,
+                                             "sequential_max": float(cs[:, 6].max()) if len(cs) else 0.0,
+                                             "sequential_mean": float(cs[:, 6].mean()) if len(cs) else 0.0},
+            "within_1e-3_m": out[frames][0] <= 1e-3}
+
+
+def per_scene_baseline(scene, frames: int, mode: int, torch, sample: int = 32) -> dict:
     """The plain per-scene GPU path on a sample of the batch: each scene its own
     world, its frames replayed as one captured episode, scenes one after another."""
+    from dyphur_b200 import device
     idx = np.linspace(0, scene.n_scenes - 1, min(sample, scene.n_scenes)).astype(int)
     worlds = []
     for i in idx:
@@ -349,46 +545,227 @@ def per_scene_baseline(scene, frames: int, mode: int, torch, device, sample: int
     t1.record(stream)
     torch.cuda.synchronize()
     bodies = sum(w.scene.n_bodies for w, _ in worlds)
+    for w, _ in worlds:
+        w.close()
     return {"value": bodies * frames / (t0.elapsed_time(t1) / 1e3), "unit": METRIC,
-            "sample": f"{len(worlds)} of the batch's scenes, each stepped alone ({frames} frames)"}
+            "sample": f"{len(worlds)} of the batch's scenes, each stepped alone as its own world ({frames} frames)"}
 
+
+def single_line(args, torch, barrier, world, rank, local, seed, frames, mode_name, nested) -> dict:
+    from dyphur_b200 import scenes
+    mode = MODES[mode_name]
+    scene = scenes.random_pile(SINGLE["bodies"], seed=seed)
+    n = scene.n_bodies
+    steps = args.steps if not nested else min(args.steps, 5)
+    a = argparse.Namespace(steps=steps, warmup=args.warmup if not nested else 3)
+    clocks = Clocks(local) if not nested else None
+    r = gpu_workload(scene, mode, frames, a, torch, barrier, clocks)
+    w = r["world"]
+    e2e_ms, h2d, d2h = e2e_episodes(w, r["init"], frames, steps, torch, barrier)
+    ms = r["ms"]
+    if world > 1:
+        ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
+    body_steps = world * steps * frames * n
+    pairs, contacts = r["pairs"], r["contacts"]
+    fb_ = frame_bytes(n, pairs, contacts)
+    peak, peak_kind = peaks()
+    frame_ach = float(fb_.sum() / (ms / steps / 1e3) / 1e9)
+    line = {"metric": METRIC, "value": body_steps / (ms / 1e3), "unit": METRIC, "n_gpus": world, "steps": steps,
+            "warmup": a.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": SINGLE_WORKLOAD, "bodies": n, "frames_per_step": frames, "seed": seed,
+                       "solver_mode": mode_name, "parallelism": f"replicas{world}",
+                       "l2": "no flush: each step re-simulates the whole episode from its initial state; a frame "
+                             "touches ~50-130 MB (about the 126 MB L2), produced on the device by the frame before",
+                       "mean_pairs_per_frame": float(pairs.mean()), "mean_contacts_per_frame": float(contacts.mean()),
+                       "contacts_per_s": float(contacts.sum() * world * steps / (ms / 1e3))},
+            "e2e": {"value": body_steps / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "trajectory_every_frames": 2},
+            "roofline": r["roofline"],
+            "frame_roofline": {"bound": "hbm", "achieved": frame_ach, "peak": peak, "unit": "GB/s",
+                               "frac": frame_ach / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                               "bytes_rule": "424 B per body + 32 B per candidate pair + 72 B per contact, per frame"},
+            "gpu_launches": int(steps * frames * kernels_per_frame(n)),
+            "clocks": r["clocks"], "overflow_status": r["status"]}
+    w.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from dyphur_b200 import device
+        win, starts = 5, list(range(0, frames, max(1, frames // 10)))
+        cw = device.World(scene, mode=mode)
+        states, cur = [], 0
+        for f in starts:
+            cw.step(f - cur)
+            cur = f
+            states.append(cw.state())
+        cw.close()
+        note("single scene timed")
+        line["cpu_baseline"] = single_cpu_baseline(frames, np.stack(states), starts, win)
+    return line
+
+
+def run_b200(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    if args.workload == "single":
+        line = single_line(args, torch, barrier, world, rank, local, SINGLE["seed"] + rank, args.frames,
+                           args.mode or "reference", nested=False)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    from dyphur_b200 import scenes
+    frames = args.frames
+    mode_name = args.mode or "sequential"
+    mode = MODES[mode_name]
+    scene = scenes.batch(BATCH["n_scenes"], BATCH["lo"], BATCH["hi"], seed=BATCH["seed"] + rank)
+    n = scene.n_bodies
+    clocks = Clocks(local)
+    note("batch scene built")
+    r = gpu_workload(scene, mode, frames, args, torch, barrier, clocks)
+    note("batch timed + flow probe")
+    w = r["world"]
+    e2e_ms, h2d, d2h = e2e_episodes(w, r["init"], frames, args.steps, torch, barrier)
+    w.close()
+    note("batch e2e")
+    # the coloured order on the same batch, for the drift / speed trade
+    rc = gpu_workload(scene, MODES["colored"], frames, argparse.Namespace(steps=args.steps, warmup=3), torch,
+                      barrier, None, roofline=False)
+    rc["world"].close()
+    note("batch coloured")
+    ms, ms_c = r["ms"], rc["ms"]
+    if world > 1:
+        ms, e2e_ms, ms_c = max_over_ranks([ms, e2e_ms, ms_c], device="cuda")
+    body_steps = world * args.steps * frames * n
+    value = body_steps / (ms / 1e3)
+    value_c = body_steps / (ms_c / 1e3)
+    if rank == 0:
+        pairs, contacts = r["pairs"], r["contacts"]
+        fb_ = frame_bytes(n, pairs, contacts)
+        peak, peak_kind = peaks()
+        frame_ach = float(fb_.sum() / (ms / args.steps / 1e3) / 1e9)
+        per_scene = per_scene_baseline(scene, frames, mode, torch)
+        per_scene["batched_over_per_scene"] = value / per_scene["value"]
+        note("per-scene path")
+        drift = drift_report(scene, frames, torch)
+        note("drift")
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "scenes": scene.n_scenes, "bodies": n, "frames_per_step": frames,
+                       "seed": BATCH["seed"], "solver_mode": mode_name, "parallelism": f"replicas{world}",
+                       "pose_drift_vs_sequential_m": 0.0 if mode == 1 else None,
+                       "l2": "no flush: each step re-simulates the whole episode from its initial state; the "
+                             "batch's per-frame data (bodies 26 MB, pairs and contacts ~30 MB) is produced on the "
+                             "device by the frame before",
+                       "mean_pairs_per_frame": float(pairs.mean()), "mean_contacts_per_frame": float(contacts.mean()),
+                       "contacts_per_s": float(contacts.sum() * world * args.steps / (ms / 1e3))},
+            "per_scene": per_scene,
+            "colored": {"value": value_c, "unit": METRIC, "ms_per_step": ms_c / args.steps,
+                        "over_per_scene": value_c / per_scene["value"], "over_sequential": value_c / value,
+                        "drift": drift},
+            "e2e": {"value": body_steps / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "trajectory_every_frames": 2},
+            "roofline": r["roofline"],
+            "frame_roofline": {"bound": "hbm", "achieved": frame_ach, "peak": peak, "unit": "GB/s",
+                               "frac": frame_ach / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                               "bytes_rule": "424 B per body + 32 B per candidate pair + 72 B per contact, per frame"},
+            "gpu_launches": int(args.steps * frames * kernels_per_frame(n, scene.n_scenes)),
+            "clocks": r["clocks"], "overflow_status": r["status"],
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = batch_cpu_baseline(dict(BATCH, frames=frames))
+            note("batch cpu baseline")
+        if not args.no_single and world == 1:
+            line["single_scene"] = single_line(args, torch, barrier, 1, 0, local, SINGLE["seed"], SINGLE["frames"],
+                                               "reference", nested=True)
+            note("single scene")
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ── reference arm ────────────────────────────────────────────────────────────
 
 def run_reference(args) -> None:
-    rank = int(os.environ.get("RANK", 0))
+    rank, _, _ = rank_info()
     if rank != 0:
         return
-    from oracle import oracle
-    which = "ref" if oracle.ref_available() else "oracle"
     cores = os.cpu_count() or 1
-    frames = max(1, args.cpu_frames // 4)
-    vals = []
-    for _ in range(max(args.warmup, 3) + args.steps):
-        r = cpu_baseline(args.bodies, frames)
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build failed to run"}))
-            return
-        vals.append(r["value"])
-    vals = vals[max(args.warmup, 3):]
-    value = statistics.mean(vals)
-    ms_step = (args.bodies + 1) * frames / value * 1e3 if value else None  # one sample of `frames` frames
+    warm = max(args.warmup, 3)
+    try:
+        if args.workload == "batch":
+            cfg = dict(BATCH, frames=args.frames)
+            cpu = BatchCpu(cfg, cores)
+            which = cpu.which
+            # step k takes the next slice of the batch's scenes, so K steps cover the batch in order
+            per = -(-cfg["n_scenes"] // max(args.steps, 1))
+            ids = np.arange(cfg["n_scenes"])
+            for k in range(warm):
+                cpu.run(ids[(k * per) % cfg["n_scenes"]:][:max(1, per // 4)], cfg["frames"])
+            bs_tot, wall_tot, walls = 0, 0.0, []
+            for k in range(args.steps):
+                sl = np.take(ids, np.arange(k * per, (k + 1) * per), mode="wrap")
+                bs, wall, _ = cpu.run(sl, cfg["frames"])
+                bs_tot += bs
+                wall_tot += wall
+                walls.append(wall)
+            cpu.close()
+            value = bs_tot / wall_tot
+            config = {"workload": BATCH_WORKLOAD, "scenes": cfg["n_scenes"], "frames_per_step": cfg["frames"],
+                      "seed": cfg["seed"], "solver_mode": "sequential", "parallelism": "host, one scene per core"}
+            sample = (f"step k steps scenes [k*{per}, (k+1)*{per}) of the batch (wrapping), {cfg['frames']} frames "
+                      f"each, one scene per host core; {args.steps} steps cover "
+                      f"{min(args.steps * per, cfg['n_scenes'])} of {cfg['n_scenes']} scenes")
+            ms_step = 1e3 * wall_tot / args.steps
+        else:
+            frames = args.frames
+            win = 30
+            r = run_single_cpu(f"windows:{win}:{warm + args.steps}:{frames}", cores)
+            which = r["which"]
+            if r["rc"] != 0:
+                raise RuntimeError(f"reference build returned {r['rc']}")
+            secs = r["window_seconds"][warm:]
+            value = r["bodies"] * win * len(secs) / sum(secs)
+            config = {"workload": SINGLE_WORKLOAD, "bodies": r["bodies"], "frames_per_step": win,
+                      "seed": SINGLE["seed"], "solver_mode": "reference", "parallelism": "host OpenMP"}
+            sample = (f"step k steps frames [30k, 30k+30) of the {frames}-frame episode from a checkpoint "
+                      f"(wrapping); {args.steps} steps cover {min(args.steps * win, frames)} of {frames} frames")
+            ms_step = 1e3 * sum(secs) / len(secs)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed to run: {e}"}))
+        return
+    kind = "reference" if which == "ref" else "port"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bodies": args.bodies + 1, "parallelism": "host OpenMP"},
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores if which == "ref" else 1,
-                             "kind": "reference" if which == "ref" else "port",
-                             "sample": f"frames 0-{frames - 1} of the episode per step"},
+            "steps": args.steps, "warmup": warm, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
-    if args.frames is None:
-        args.frames = 240 if args.workload == "batch" else 600
-    if args.cpu_worker:
-        cpu_worker(args.cpu_worker, args.bodies, args.cpu_frames)
+    if args.cpu_single_worker:
+        _single_cpu_worker(args.cpu_single_worker)
         return
+    if args.frames is None:
+        args.frames = BATCH["frames"] if args.workload == "batch" else SINGLE["frames"]
     if args.impl == "reference":
         run_reference(args)
         return

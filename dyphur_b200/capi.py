@@ -99,6 +99,7 @@ _PROTOS = {
     "dyph_world_capture_episode": (_st, [_vp, C.c_int32, C.c_int32, C.POINTER(_vp), C.POINTER(_vp)]),
     "dyph_world_run_episode": (_st, [_vp, _vp]),
     "dyph_world_download_history": (_st, [_vp, _vp, _vp, _vp, C.c_uint32, _up]),
+    "dyph_world_set_trajectory": (_st, [_vp, _vp, C.c_uint32, C.c_uint32]),
     "dyph_event_create": (_st, [C.POINTER(_vp)]),
     "dyph_event_destroy": (None, [_vp]),
     "dyph_event_record": (_st, [_vp, _vp]),
@@ -109,7 +110,7 @@ _PROTOS = {
 }
 
 # Every symbol the header declares (checked by the CPU suite).
-HEADER_SYMBOLS = tuple(k for k in _PROTOS if k != "dyph_pack_bodies")
+HEADER_SYMBOLS = tuple(_PROTOS)
 
 _lib = None
 

@@ -95,6 +95,7 @@ struct dyph_xpbd {
     uint32_t* partial = nullptr;    // [4096] dataflow sequential order: per-block sums
     int coop_blocks = 0;            // co-resident blocks of the round-synchronous coloured kernel
     int flow_blocks = 0;            // co-resident blocks of the dataflow kernel
+    void* probe_flow[2] = {nullptr, nullptr};  // events recorded around the dataflow kernel (timing probe)
 };
 
 namespace dyph {

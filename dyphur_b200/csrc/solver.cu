@@ -303,8 +303,12 @@ dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_
                reinterpret_cast<unsigned long long*>(sv->hand), 2u * sv->max_contacts, sv->tail, sv->sweep_tag,
                sv->csr_off, sv->csr_cur, sv->csr, sv->partial};
     void* fargs[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &F, &sv->meta};
+    if (sv->probe_flow[0])
+        DYPH_CUDA_TRY(cudaEventRecordWithFlags(static_cast<cudaEvent_t>(sv->probe_flow[0]), s, cudaEventRecordExternal));
     DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(flow_solve_kernel), dim3(sv->flow_blocks),
                                               dim3(kFlowThreads), fargs, 0, s));
+    if (sv->probe_flow[1])
+        DYPH_CUDA_TRY(cudaEventRecordWithFlags(static_cast<cudaEvent_t>(sv->probe_flow[1]), s, cudaEventRecordExternal));
     void* args[] = {&cv, &B, &mode, &n_iters, &mu, &dt, &sv->lambda, &sv->color, &sv->order, &sv->pred,
                     &sv->bpri, &sv->bmask, &sv->meta};
     DYPH_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(color_solve_kernel), dim3(sv->coop_blocks),

@@ -24,6 +24,18 @@ struct dyph_world {
     cudaGraphExec_t episode = nullptr;  // n_frames frames in one graph (dyph_world_capture_episode)
     int32_t episode_frames = 0;
     uint64_t* scene_hash = nullptr;  // [n_scenes] per-scene FNV-1a results
+    // Trajectory recording (dyph_world_set_trajectory): pose rows packed on
+    // the frame's stream into one of two device staging buffers, copied to the
+    // caller's pinned host buffer on a side stream.
+    float* traj_host = nullptr;
+    uint32_t traj_every = 0, traj_max = 0;
+    uint64_t traj_frame = 0;              // frames stepped by dyph_world_step since the last set-up
+    float* traj_stage[2] = {nullptr, nullptr};
+    cudaStream_t traj_stream = nullptr;
+    cudaEvent_t traj_packed[2] = {nullptr, nullptr};
+    cudaEvent_t traj_copied[2] = {nullptr, nullptr};
+    bool traj_pending = false;            // a copy on the side stream not yet joined
+    bool traj_live[2] = {false, false};   // traj_copied[k] was last recorded outside a capture
 };
 
 namespace dyph {
@@ -47,6 +59,47 @@ __global__ void frame_stats_kernel(const uint32_t* __restrict__ bp_counts, const
     if (c > max_contacts) atomicCAS(&stats[4], 0u, static_cast<uint32_t>(DYPH_ERR_CONTACT_OVERFLOW));
 }
 
+// Pose rows of every body, interleaved per body as the .trajectory row
+// (x, y, z, w, qx, qy, qz), examples/stress_test_blocks/main.cpp:191-197.
+__global__ void pack_pose_kernel(GlobalBodies B, float* __restrict__ out) {
+    const uint32_t n = B.v.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float* r = out + 7ull * i;
+        r[0] = B.px(i); r[1] = B.py(i); r[2] = B.pz(i);
+        r[3] = B.qw(i); r[4] = B.qx(i); r[5] = B.qy(i); r[6] = B.qz(i);
+    }
+}
+
+// Queue trajectory record `rec` (the pose rows after the frame just queued on
+// s): pack into staging buffer rec % 2 once that buffer's previous copy is
+// done (when `wait_prev`), then copy it to the host on the side stream.
+dyph_status enqueue_trajectory_record(dyph_world* w, cudaStream_t s, uint64_t rec, bool wait_prev) {
+    const uint32_t n = w->desc.bodies.n;
+    const int k = static_cast<int>(rec & 1u);
+    if (wait_prev) DYPH_CUDA_TRY(cudaStreamWaitEvent(s, w->traj_copied[k], 0));
+    pack_pose_kernel<<<(n + 255) / 256, 256, 0, s>>>(GlobalBodies{w->desc.bodies}, w->traj_stage[k]);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    DYPH_CUDA_TRY(cudaEventRecord(w->traj_packed[k], s));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(w->traj_stream, w->traj_packed[k], 0));
+    DYPH_CUDA_TRY(cudaMemcpyAsync(w->traj_host + rec * 7ull * n, w->traj_stage[k], 7ull * n * sizeof(float),
+                                  cudaMemcpyDeviceToHost, w->traj_stream));
+    DYPH_CUDA_TRY(cudaEventRecord(w->traj_copied[k], w->traj_stream));
+    w->traj_pending = true;
+    return DYPH_OK;
+}
+
+// Order every queued trajectory copy before the work that follows on s.
+dyph_status join_trajectory(dyph_world* w, cudaStream_t s, uint64_t last_rec) {
+    if (!w->traj_pending) return DYPH_OK;
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(s, w->traj_copied[last_rec & 1u], 0));
+    w->traj_pending = false;
+    return DYPH_OK;
+}
+
+bool trajectory_frame(const dyph_world* w, uint64_t frame) {
+    return w->traj_host && frame % w->traj_every == 0 && frame / w->traj_every < w->traj_max;
+}
+
 // Records an event inside a stream capture as a real timestamp node.
 dyph_status probe_record(void* ev, cudaStream_t s) {
     if (!ev) return DYPH_OK;
@@ -55,11 +108,14 @@ dyph_status probe_record(void* ev, cudaStream_t s) {
 }
 
 // One frame; when probe_stage matches a stage (0 integrate, 1 broadphase,
-// 2 narrowphase, 3 solver) the events are recorded around it.
+// 2 narrowphase, 3 solver) the events are recorded around it; probe_stage 4
+// records them around the solver's dataflow kernel alone.
 dyph_status enqueue_frame(dyph_world* w, cudaStream_t s, int probe_stage = -1, void* ev0 = nullptr,
                           void* ev1 = nullptr) {
     const dyph_world_desc& d = w->desc;
     dyph_status st;
+    w->sv->probe_flow[0] = probe_stage == 4 ? ev0 : nullptr;
+    w->sv->probe_flow[1] = probe_stage == 4 ? ev1 : nullptr;
     for (int stage = 0; stage < 4; ++stage) {
         if (stage == probe_stage && (st = probe_record(ev0, s)) != DYPH_OK) return st;
         switch (stage) {
@@ -70,9 +126,11 @@ dyph_status enqueue_frame(dyph_world* w, cudaStream_t s, int probe_stage = -1, v
                 break;
             default: st = xpbd_solve(w->sv, &w->np->view, &d.bodies, d.integrator.dt, s); break;
         }
-        if (st != DYPH_OK) return st;
-        if (stage == probe_stage && (st = probe_record(ev1, s)) != DYPH_OK) return st;
+        if (st != DYPH_OK) break;
+        if (stage == probe_stage && (st = probe_record(ev1, s)) != DYPH_OK) break;
     }
+    w->sv->probe_flow[0] = w->sv->probe_flow[1] = nullptr;
+    if (st != DYPH_OK) return st;
     frame_stats_kernel<<<1, 1, 0, s>>>(w->bp->counts, w->np->counts, w->bp->max_pairs, w->np->max_contacts,
                                        w->stats);
     DYPH_CUDA_TRY(cudaGetLastError());
@@ -93,6 +151,13 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     if (w->stream) cudaStreamDestroy(w->stream);
     if (w->stats) cudaFree(w->stats);
     if (w->scene_hash) cudaFree(w->scene_hash);
+    if (w->traj_stream) cudaStreamSynchronize(w->traj_stream);
+    for (int k = 0; k < 2; ++k) {
+        if (w->traj_stage[k]) cudaFree(w->traj_stage[k]);
+        if (w->traj_packed[k]) cudaEventDestroy(w->traj_packed[k]);
+        if (w->traj_copied[k]) cudaEventDestroy(w->traj_copied[k]);
+    }
+    if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     broadphase_destroy(w->bp);
     narrowphase_destroy(w->np);
     xpbd_destroy(w->sv);
@@ -150,7 +215,20 @@ extern "C" dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_str
             return DYPH_ERR_CUDA;
         }
     }
-    for (int32_t f = 0; f < n_frames; ++f) DYPH_CUDA_TRY(cudaGraphLaunch(w->graph, w->stream));
+    uint64_t last_rec = 0;
+    for (int32_t f = 0; f < n_frames; ++f) {
+        DYPH_CUDA_TRY(cudaGraphLaunch(w->graph, w->stream));
+        if (trajectory_frame(w, w->traj_frame)) {
+            last_rec = w->traj_frame / w->traj_every;
+            const int k = static_cast<int>(last_rec & 1u);
+            dyph_status st = enqueue_trajectory_record(w, w->stream, last_rec, w->traj_live[k]);
+            if (st != DYPH_OK) return st;
+            w->traj_live[k] = true;
+        }
+        ++w->traj_frame;
+    }
+    dyph_status jst = join_trajectory(w, w->stream, last_rec);
+    if (jst != DYPH_OK) return jst;
     DYPH_CUDA_TRY(cudaEventRecord(w->ev_out, w->stream));
     DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->ev_out, 0));
     return DYPH_OK;
@@ -158,7 +236,7 @@ extern "C" dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_str
 
 extern "C" dyph_status dyph_world_capture_episode(dyph_world* w, int32_t n_frames, int32_t probe_stage,
                                                   void* const* ev_start, void* const* ev_end) {
-    if (!w || n_frames <= 0 || probe_stage < -1 || probe_stage > 3) return DYPH_ERR_INVALID;
+    if (!w || n_frames <= 0 || probe_stage < -1 || probe_stage > 4) return DYPH_ERR_INVALID;
     if (probe_stage >= 0 && (!ev_start || !ev_end)) return DYPH_ERR_INVALID;
     if (w->episode) {
         cudaGraphExecDestroy(w->episode);
@@ -167,9 +245,17 @@ extern "C" dyph_status dyph_world_capture_episode(dyph_world* w, int32_t n_frame
     cudaGraph_t g = nullptr;
     DYPH_CUDA_TRY(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
     dyph_status st = DYPH_OK;
-    for (int32_t f = 0; f < n_frames && st == DYPH_OK; ++f)
+    uint64_t last_rec = 0;
+    for (int32_t f = 0; f < n_frames && st == DYPH_OK; ++f) {
         st = enqueue_frame(w, w->stream, probe_stage, probe_stage >= 0 ? ev_start[f] : nullptr,
                            probe_stage >= 0 ? ev_end[f] : nullptr);
+        if (st == DYPH_OK && trajectory_frame(w, static_cast<uint64_t>(f))) {
+            last_rec = static_cast<uint64_t>(f) / w->traj_every;
+            st = enqueue_trajectory_record(w, w->stream, last_rec, last_rec >= 2);
+        }
+    }
+    if (st == DYPH_OK) st = join_trajectory(w, w->stream, last_rec);
+    w->traj_pending = false;
     cudaError_t ce = cudaStreamEndCapture(w->stream, &g);
     if (st != DYPH_OK) {
         if (g) cudaGraphDestroy(g);
@@ -302,5 +388,39 @@ extern "C" dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uin
     if (st != DYPH_OK) return st;
     DYPH_CUDA_TRY(cudaMemcpyAsync(host_out, w->scene_hash, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, cs));
     DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_set_trajectory(dyph_world* w, float* host_dst, uint32_t every,
+                                                 uint32_t max_records) {
+    if (!w || (host_dst && (every == 0 || max_records == 0))) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    if (w->traj_stream) DYPH_CUDA_TRY(cudaStreamSynchronize(w->traj_stream));
+    // A captured episode has the old recording baked in.
+    if (w->episode) {
+        cudaGraphExecDestroy(w->episode);
+        w->episode = nullptr;
+        w->episode_frames = 0;
+    }
+    w->traj_host = host_dst;
+    w->traj_every = every;
+    w->traj_max = max_records;
+    w->traj_frame = 0;
+    w->traj_pending = false;
+    w->traj_live[0] = w->traj_live[1] = false;
+    if (!host_dst) return DYPH_OK;
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, host_dst) != cudaSuccess || attr.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        w->traj_host = nullptr;
+        return DYPH_ERR_INVALID;  // pageable memory: the copies could not run asynchronously or be captured
+    }
+    const size_t bytes = 7ull * w->desc.bodies.n * sizeof(float);
+    for (int k = 0; k < 2; ++k) {
+        if (!w->traj_stage[k] && cudaMalloc(&w->traj_stage[k], bytes) != cudaSuccess) return DYPH_ERR_NOMEM;
+        if (!w->traj_packed[k]) DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->traj_packed[k], cudaEventDisableTiming));
+        if (!w->traj_copied[k]) DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->traj_copied[k], cudaEventDisableTiming));
+    }
+    if (!w->traj_stream) DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->traj_stream, cudaStreamNonBlocking));
     return DYPH_OK;
 }

@@ -336,8 +336,22 @@ class World:
     def step(self, frames: int = 1, stream=None) -> None:
         check(capi.lib().dyph_world_step(self.h, frames, _stream_ptr(stream)), "dyph_world_step")
 
+    def set_trajectory(self, host: torch.Tensor | None, every: int = 2) -> None:
+        """Record every `every`-th frame's poses into a pinned host float tensor of shape
+        (records, n, 7) (dyph_world_set_trajectory); None stops recording."""
+        if host is None:
+            check(capi.lib().dyph_world_set_trajectory(self.h, None, 0, 0), "dyph_world_set_trajectory")
+            self._traj = None
+            return
+        if not host.is_pinned() or host.dtype != torch.float32 or host.shape[1:] != (self.bodies.n, 7):
+            raise ValueError("trajectory buffer must be a pinned float32 tensor of shape (records, n, 7)")
+        check(capi.lib().dyph_world_set_trajectory(self.h, host.data_ptr(), every, host.shape[0]),
+              "dyph_world_set_trajectory")
+        self._traj = host
+
     def capture_episode(self, n_frames: int, probe_stage: int = -1) -> None:
-        """Record n_frames frames as one graph; probe_stage 0..3 times that stage per frame."""
+        """Record n_frames frames as one graph; probe_stage 0..3 times that stage per frame
+        (4: the solver's dataflow kernel alone)."""
         L = capi.lib()
         self._free_probe()
         if probe_stage >= 0:
@@ -425,3 +439,17 @@ class World:
             return bp.bvh(self.bodies.n)
         finally:
             bp.h = None
+
+    def colors(self, n: int):
+        """JP colours of the last frame's solve (UINT32_MAX on the sequential path) and the colour count."""
+        out = np.empty(max(n, 1), np.uint32)
+        nc = C.c_uint32()
+        check(capi.lib().dyph_xpbd_download_colors(self._sv, None, out.ctypes.data_as(capi._up), n, C.byref(nc)))
+        return out[:n], int(nc.value)
+
+    def solver_stats(self) -> dict:
+        """Path of the last frame's solve (0 sequential / none, 1 coloured attempt fell back to the
+        sequential order, 2 coloured), its colour count and its Jones–Plassmann rounds."""
+        v = [C.c_uint32() for _ in range(3)]
+        check(capi.lib().dyph_xpbd_download_stats(self._sv, None, *[C.byref(x) for x in v]))
+        return {"path": int(v[0].value), "colors": int(v[1].value), "rounds": int(v[2].value)}

@@ -2,6 +2,10 @@
 
 The builders live in ``csrc/scenes.cpp`` and are exported through the C ABI
 (``dyph_scene_make``); this module copies a built set into numpy arrays.
+Every builder takes an optional ``builder=(cdll, prefix)``: the CPU checkers
+in ``oracle/`` carry the same builders as ``dyo_scene_make`` /
+``dyr_scene_make``, so a CPU-only run builds identical scenes without
+loading the GPU library.
 """
 from __future__ import annotations
 
@@ -83,9 +87,9 @@ class SceneSet:
 
 
 def make(kind: int, seed: int = 1, a0: int = 0, a1: int = 0, a2: int = 0, spacing: float = 1.0,
-         jitter: float = 0.0) -> SceneSet:
-    lib = load_library()
-    fn = lib.dyph_scene_make
+         jitter: float = 0.0, builder=None) -> SceneSet:
+    lib, prefix = builder if builder is not None else (load_library(), "dyph")
+    fn = getattr(lib, prefix + "_scene_make")
     fn.restype = ctypes.POINTER(_SceneSetC)
     fn.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                    ctypes.c_float, ctypes.c_float]
@@ -111,33 +115,34 @@ def make(kind: int, seed: int = 1, a0: int = 0, a1: int = 0, a2: int = 0, spacin
         friction=float(c.friction), meta={"kind": kind, "seed": seed, "a": (a0, a1, a2),
                                           "spacing": spacing, "jitter": jitter},
     )
-    free = lib.dyph_scene_free
+    free = getattr(lib, prefix + "_scene_free")
     free.argtypes = [ctypes.POINTER(_SceneSetC)]
     free(p)
     return out
 
 
-def stress_blocks(spacing: float = 0.85, jitter: float = 0.01, seed: int = 1, grid=(8, 16, 8)) -> SceneSet:
+def stress_blocks(spacing: float = 0.85, jitter: float = 0.01, seed: int = 1, grid=(8, 16, 8),
+                  builder=None) -> SceneSet:
     """1024 boxes on an 8 x 8 footprint, 16 high, over the 20 x 0.5 x 20 ground."""
-    return make(BOX_GRID, seed, grid[0], grid[1], grid[2], spacing, jitter)
+    return make(BOX_GRID, seed, grid[0], grid[1], grid[2], spacing, jitter, builder=builder)
 
 
-def determinism(grid=(2, 2, 2)) -> SceneSet:
+def determinism(grid=(2, 2, 2), builder=None) -> SceneSet:
     """The reference's sim-determinism scene (8 boxes + ground by default)."""
-    return make(DETERMINISM, 0, grid[0], grid[1], grid[2], 1.0, 0.0)
+    return make(DETERMINISM, 0, grid[0], grid[1], grid[2], 1.0, 0.0, builder=builder)
 
 
-def random_pile(n: int = 65536, seed: int = 2) -> SceneSet:
-    return make(RANDOM_PILE, seed, n)
+def random_pile(n: int = 65536, seed: int = 2, builder=None) -> SceneSet:
+    return make(RANDOM_PILE, seed, n, builder=builder)
 
 
-def batch(n_scenes: int = 4096, lo: int = 8, hi: int = 256, seed: int = 3) -> SceneSet:
-    return make(BATCH, seed, n_scenes, lo, hi)
+def batch(n_scenes: int = 4096, lo: int = 8, hi: int = 256, seed: int = 3, builder=None) -> SceneSet:
+    return make(BATCH, seed, n_scenes, lo, hi, builder=builder)
 
 
-def push(n_scenes: int = 256, seed: int = 4) -> SceneSet:
-    return make(PUSH, seed, n_scenes)
+def push(n_scenes: int = 256, seed: int = 4, builder=None) -> SceneSet:
+    return make(PUSH, seed, n_scenes, builder=builder)
 
 
-def batch_mixed(n_scenes: int = 1024, lo: int = 16, hi: int = 512, seed: int = 5) -> SceneSet:
-    return make(BATCH_MIXED, seed, n_scenes, lo, hi)
+def batch_mixed(n_scenes: int = 1024, lo: int = 16, hi: int = 512, seed: int = 5, builder=None) -> SceneSet:
+    return make(BATCH_MIXED, seed, n_scenes, lo, hi, builder=builder)

@@ -150,6 +150,18 @@ dyph_status dyph_download_device_error_site(dyph_stream s, uint32_t* out_code, u
 dyph_status dyph_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, dyph_stream s);
 dyph_status dyph_copy_to_device(void* dev_dst, const void* host_src, size_t bytes, dyph_stream s);
 
+/* Host-side BodyStore::add for n bodies (core/src/body_store.cpp:28-69),
+ * no device work: fills the host SoA rows of a BodyView — state13 = pos xyz,
+ * rot wxyz, vel xyz, ang xyz ([13][n]), inv_mass [n], iI6 = iI_xx, iI_yy,
+ * iI_zz, iI_xy, iI_xz, iI_yz ([6][n]) and flags [n]. A body is static when
+ * flagged Static or mass <= 0: it gets inv_mass 0, a zero inverse inertia and
+ * the Static flag; otherwise the inverse inertia is Mat3::inverse (adjugate /
+ * determinant, core/include/core/math/mat3.hpp:61-79) of the body-frame
+ * inertia, in float, as the reference computes it. */
+void dyph_pack_bodies(uint32_t n, const float* pos, const float* rot, const float* vel, const float* ang,
+                      const float* mass, const float* inertia, const uint32_t* flags_in, float* state13,
+                      float* inv_mass, float* iI6, uint32_t* flags_out);
+
 /* ── integrate — replaces integrate(Stream&, BodyView, const IntegratorParams&)
  *    (core/include/core/integrator.hpp:25, core/src/integrator.cpp:7-71) ──── */
 dyph_status dyph_integrate(const dyph_bodies* bodies, const dyph_integrator_params* params, dyph_stream s);
@@ -302,7 +314,8 @@ dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* la
 /* Capture n_frames consecutive frames as one graph (an "episode"); with
  * probe_stage 0..3 (integrate, broadphase, narrowphase, solver) the caller's
  * events ev_start[f] / ev_end[f] (from dyph_event_create) are recorded around
- * that stage of frame f — the per-stage timing of the reference's --profile
+ * that stage of frame f (probe_stage 4: around the solver's dataflow kernel
+ * alone) — the per-stage timing of the reference's --profile
  * mode (examples/stress_test_blocks/main.cpp:199-254) without host fences.
  * probe_stage -1 records nothing. */
 dyph_status dyph_world_capture_episode(dyph_world* w, int32_t n_frames, int32_t probe_stage,
@@ -318,6 +331,20 @@ dyph_status dyph_event_elapsed_ms(void* start, void* end, float* ms);
  * frames (oldest first) and the number of frames stepped so far. */
 dyph_status dyph_world_download_history(dyph_world* w, dyph_stream s, uint32_t* pairs, uint32_t* contacts,
                                         uint32_t cap, uint32_t* frames_total);
+/* Trajectory recording: replaces the example loop's download_state() +
+ * write_traj_frame() every other frame (examples/stress_test_blocks/
+ * main.cpp:182-197, 275-278). While set, after every frame f with
+ * f % every == 0 and f / every < max_records, the pose of every body is
+ * written to host_dst + (f / every) * 7 * n as n rows of x, y, z, w, qx, qy,
+ * qz (the .trajectory row layout). Frames are counted by dyph_world_step from
+ * this call on, and within an episode from the episode's first frame (the
+ * recording is captured into the episode, so set it before
+ * dyph_world_capture_episode; this call drops a captured episode). The copies
+ * run on a side stream, overlapped with the next frames, and are complete when
+ * the step or episode is. host_dst must be pinned host memory (cudaHostAlloc
+ * or cudaHostRegister) of max_records * 7 * n floats; NULL stops recording.
+ * Blocking (synchronises the world's streams). */
+dyph_status dyph_world_set_trajectory(dyph_world* w, float* host_dst, uint32_t every, uint32_t max_records);
 dyph_status dyph_world_broadphase(dyph_world* w, dyph_broadphase** out);
 dyph_status dyph_world_narrowphase(dyph_world* w, dyph_narrowphase** out);
 dyph_status dyph_world_solver(dyph_world* w, dyph_xpbd** out);

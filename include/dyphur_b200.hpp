@@ -21,10 +21,6 @@
 
 #include "dyphur_b200.h"
 
-extern "C" void dyph_pack_bodies(uint32_t n, const float* pos, const float* rot, const float* vel, const float* ang,
-                                 const float* mass, const float* inertia, const uint32_t* flags_in, float* state13,
-                                 float* inv_mass, float* iI6, uint32_t* flags_out);
-
 namespace dyphur {
 
 inline void check(dyph_status st, const char* what) {

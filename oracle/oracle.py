@@ -47,6 +47,16 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+def scene_builder(which: str | None = None):
+    """(cdll, prefix) of the scene builders inside a checker library, for
+    dyphur_b200.scenes(..., builder=...): the reference build's copy when it
+    exists, else the C restatement's."""
+    which = which or ("ref" if ref_available() else "oracle")
+    if which == "ref":
+        return ctypes.CDLL(REF_SO), "dyr"
+    return ctypes.CDLL(build_oracle()), "dyo"
+
+
 class Checker:
     def __init__(self, which: str = "oracle"):
         if which == "oracle":

@@ -25,7 +25,7 @@ def test_library_exports_every_header_symbol():
     assert len(names) > 30
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
-    assert set(names) <= set(capi.HEADER_SYMBOLS) | {"dyph_pack_bodies"}
+    assert set(names) == set(capi.HEADER_SYMBOLS)
 
 
 def test_status_strings_without_gpu():
