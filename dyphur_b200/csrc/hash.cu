@@ -52,12 +52,14 @@ extern "C" dyph_status dyph_xpbd_download_stats(dyph_xpbd* sv, dyph_stream s, ui
                                                 uint32_t* rounds) {
     if (!sv) return DYPH_ERR_INVALID;
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
-    uint32_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t meta[16] = {};
     DYPH_CUDA_TRY(cudaMemcpyAsync(meta, sv->meta, sizeof(meta), cudaMemcpyDeviceToHost, cs));
     DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
-    // decision word: 2 coloured; 4 fallback / 5 sequential order run by the dataflow kernel
-    if (path) *path = meta[0] == 4u ? 1u : (meta[0] == 5u ? 0u : meta[0]);
-    if (n_colors) *n_colors = meta[0] == 2u ? meta[3] + 1u : 0u;
+    // decision word: 2 coloured; 4 fallback / 5 sequential order run by the dataflow kernel;
+    // 6 batched scenes, one per block (coloured when some scene was: word 13)
+    const bool colored = meta[0] == 2u || (meta[0] == 6u && meta[13] != 0u);
+    if (path) *path = meta[0] == 4u ? 1u : (meta[0] == 5u || meta[0] == 6u ? (colored ? 2u : 0u) : meta[0]);
+    if (n_colors) *n_colors = colored ? meta[3] + 1u : 0u;
     if (rounds) *rounds = meta[7];
     return DYPH_OK;
 }
@@ -78,10 +80,12 @@ extern "C" dyph_status dyph_xpbd_download_colors(dyph_xpbd* sv, dyph_stream s, u
                                                  uint32_t* n_colors) {
     if (!sv) return DYPH_ERR_INVALID;
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
-    uint32_t meta[4] = {0, 0, 0, 0};
+    uint32_t meta[16] = {};
     DYPH_CUDA_TRY(cudaMemcpyAsync(meta, sv->meta, sizeof(meta), cudaMemcpyDeviceToHost, cs));
     DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
-    const bool colored = meta[0] == 2u;  // the coloured path finished
+    // the coloured path finished, or batched scenes of which some were coloured
+    // (the others' entries hold UINT32_MAX)
+    const bool colored = meta[0] == 2u || (meta[0] == 6u && meta[13] != 0u);
     if (n_colors) *n_colors = colored ? meta[3] + 1u : 0u;
     if (host_colors && cap) {
         if (colored) {

@@ -96,6 +96,15 @@ struct dyph_xpbd {
     int coop_blocks = 0;            // co-resident blocks of the round-synchronous coloured kernel
     int flow_blocks = 0;            // co-resident blocks of the dataflow kernel
     void* probe_flow[2] = {nullptr, nullptr};  // events recorded around the dataflow kernel (timing probe)
+    // Batched scenes solved one scene per block (xpbd_set_scenes); 0 = off.
+    uint32_t scene_n = 0;
+    const uint32_t* scene_offset = nullptr;  // [scene_n + 1] device, owned by the broadphase
+    const uint32_t* scene_of = nullptr;      // [bodies] device, owned by the broadphase
+    uint32_t* scene_range = nullptr;         // [2 scene_n] first / end contact of each scene
+    uint32_t* scene_order = nullptr;         // [scene_n] scenes by descending body count
+    uint32_t* scene_scratch = nullptr;       // [13][scene_stride] per-contact words of large scenes
+    uint32_t scene_stride = 0;               // max_contacts + scene_n
+    uint32_t scene_smem = 0;                 // dynamic shared memory per block
 };
 
 namespace dyph {
@@ -121,6 +130,12 @@ dyph_status xpbd_create(int32_t n_iters, uint32_t max_contacts, uint32_t max_bod
 void xpbd_destroy(dyph_xpbd* sv);
 dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_bodies* bodies, float dt,
                        cudaStream_t s);
+// Solve batched scenes one scene per thread block (device arrays of the
+// broadphase's scene set; allocates, call outside graph capture). Returns
+// DYPH_ERR_TOO_LARGE, and leaves the whole-batch kernels in charge, when the
+// largest scene's bodies do not fit one block's shared memory.
+dyph_status xpbd_set_scenes(dyph_xpbd* sv, uint32_t n_scenes, const uint32_t* h_body_offset,
+                            const uint32_t* d_body_offset, const uint32_t* d_scene_of);
 
 // Pre-set kernel attributes of the sort (call once, outside graph capture).
 dyph_status sort_prepare();

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <new>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -41,6 +42,8 @@ constexpr int kMetaRounds = 7;    // JP rounds of the last coloured solve (diagn
 constexpr int kMetaListLen = 8;   // [8, 11) work-list lengths of the JP rounds
 constexpr int kMetaTailRemaining = 11;
 constexpr int kMetaFlowPath = 12;  // 1 when the last coloured solve ran the dataflow kernel
+constexpr int kMetaSceneColored = 13;  // batched scenes: 1 when some scene took the coloured order
+constexpr uint32_t kDecisionScenes = 6u;  // decision word: the per-scene kernel solved the batch
 constexpr int kMetaTime = 144;    // [144, 154) phase timestamps (ns) of the coloured solve
 constexpr int kMetaColorCount = 16;   // [16, 80)
 constexpr int kMetaColorCursor = 80;  // [80, 144)
@@ -81,6 +84,7 @@ __device__ __forceinline__ void renorm_body(const GlobalBodies& B, uint32_t i, i
 
 #include "solver_color.cuh"
 #include "solver_flow.cuh"
+#include "solver_scene.cuh"
 
 namespace dyph {
 namespace {
@@ -280,10 +284,69 @@ void xpbd_destroy(dyph_xpbd* sv) {
     if (!sv) return;
     void* ptrs[] = {sv->lambda, sv->color, sv->order, sv->pred, sv->done, sv->bpri, sv->bmask, sv->blast, sv->meta,
                     sv->body_list, sv->slot, sv->link, sv->cmask, sv->hand, sv->tail, sv->sweep_tag,
-                    sv->csr_off, sv->csr_cur, sv->csr, sv->partial};
+                    sv->csr_off, sv->csr_cur, sv->csr, sv->partial, sv->scene_range, sv->scene_order,
+                    sv->scene_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sv;
+}
+
+dyph_status xpbd_set_scenes(dyph_xpbd* sv, uint32_t n_scenes, const uint32_t* h_body_offset,
+                            const uint32_t* d_body_offset, const uint32_t* d_scene_of) {
+    if (!sv || !h_body_offset || !d_body_offset || !d_scene_of || n_scenes == 0) return DYPH_ERR_INVALID;
+    sv->scene_n = 0;
+    // Largest scenes first: blocks are dispatched in index order, so the long
+    // scenes start early and the short ones fill in behind them.
+    std::vector<uint32_t> order(n_scenes);
+    uint32_t max_nb = 0;
+    for (uint32_t i = 0; i < n_scenes; ++i) {
+        order[i] = i;
+        max_nb = std::max(max_nb, h_body_offset[i + 1] - h_body_offset[i]);
+    }
+    std::stable_sort(order.begin(), order.end(), [h_body_offset](uint32_t x, uint32_t y) {
+        return h_body_offset[x + 1] - h_body_offset[x] > h_body_offset[y + 1] - h_body_offset[y];
+    });
+    constexpr uint32_t kMaxSmem = 200u * 1024u;
+    const uint32_t body_bytes = scene_body_bytes(max_nb);
+    if (max_nb > kSceneMaxBodies || body_bytes + kSceneWords * 4u * 64u > kMaxSmem) return DYPH_ERR_TOO_LARGE;
+    // Room for about three contacts per body of the largest scene next to its
+    // bodies; a scene with more keeps its contact words in the global scratch.
+    const uint32_t smem = std::min(kMaxSmem, body_bytes + kSceneWords * 4u * std::max(256u, 3u * max_nb));
+    // The attribute is per device and per function: set it on the current device every time.
+    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+    if (sv->scene_range) cudaFree(sv->scene_range);
+    if (sv->scene_order) cudaFree(sv->scene_order);
+    sv->scene_range = sv->scene_order = nullptr;
+    if (cudaMalloc(&sv->scene_range, 2ull * n_scenes * 4) != cudaSuccess ||
+        cudaMalloc(&sv->scene_order, static_cast<size_t>(n_scenes) * 4) != cudaSuccess)
+        return DYPH_ERR_NOMEM;
+    DYPH_CUDA_TRY(cudaMemcpy(sv->scene_order, order.data(), static_cast<size_t>(n_scenes) * 4, cudaMemcpyHostToDevice));
+    if (sv->scene_scratch) cudaFree(sv->scene_scratch);
+    sv->scene_scratch = nullptr;
+    sv->scene_stride = sv->max_contacts + n_scenes;
+    if (cudaMalloc(&sv->scene_scratch, static_cast<size_t>(kSceneWords) * sv->scene_stride * 4) != cudaSuccess)
+        return DYPH_ERR_NOMEM;
+    sv->scene_offset = d_body_offset;
+    sv->scene_of = d_scene_of;
+    sv->scene_smem = smem;
+    sv->scene_n = n_scenes;
+    // The whole-batch kernels' buffers are not used again (a world never
+    // leaves the batched form): give them back.
+    void** unused[] = {reinterpret_cast<void**>(&sv->order), reinterpret_cast<void**>(&sv->pred),
+                       reinterpret_cast<void**>(&sv->done), reinterpret_cast<void**>(&sv->bpri),
+                       reinterpret_cast<void**>(&sv->bmask), reinterpret_cast<void**>(&sv->blast),
+                       reinterpret_cast<void**>(&sv->body_list), reinterpret_cast<void**>(&sv->slot),
+                       reinterpret_cast<void**>(&sv->link), reinterpret_cast<void**>(&sv->cmask),
+                       reinterpret_cast<void**>(&sv->hand), reinterpret_cast<void**>(&sv->tail),
+                       reinterpret_cast<void**>(&sv->csr_off), reinterpret_cast<void**>(&sv->csr_cur),
+                       reinterpret_cast<void**>(&sv->csr), reinterpret_cast<void**>(&sv->partial)};
+    DYPH_CUDA_TRY(cudaDeviceSynchronize());
+    for (void** p : unused) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    return DYPH_OK;
 }
 
 dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_bodies* bodies, float dt,
@@ -296,6 +359,23 @@ dyph_status xpbd_solve(dyph_xpbd* sv, const dyph_contacts* contacts, const dyph_
     int mode = static_cast<int>(sv->mode);
     int n_iters = sv->n_iters;
     float mu = sv->friction;
+    if (sv->scene_n > 0) {
+        // Batched scenes: one block per scene.
+        SceneBufs S{sv->scene_offset, sv->scene_of, sv->scene_order, sv->scene_range, sv->scene_scratch,
+                    sv->scene_stride, sv->scene_n, sv->scene_smem};
+        DYPH_CUDA_TRY(cudaMemsetAsync(sv->scene_range, 0, 2ull * sv->scene_n * 4, s));
+        scene_range_kernel<<<std::max(1u, std::min((cv.capacity + 255u) / 256u, 4096u)), 256, 0, s>>>(cv, S);
+        if (sv->probe_flow[0])
+            DYPH_CUDA_TRY(cudaEventRecordWithFlags(static_cast<cudaEvent_t>(sv->probe_flow[0]), s,
+                                                   cudaEventRecordExternal));
+        scene_solve_kernel<<<sv->scene_n, kSceneThreads, sv->scene_smem, s>>>(cv, *bodies, S, mode, n_iters, mu, dt,
+                                                                              sv->color, sv->meta);
+        if (sv->probe_flow[1])
+            DYPH_CUDA_TRY(cudaEventRecordWithFlags(static_cast<cudaEvent_t>(sv->probe_flow[1]), s,
+                                                   cudaEventRecordExternal));
+        DYPH_CUDA_TRY(cudaGetLastError());
+        return DYPH_OK;
+    }
     // Per-body contact counts live in `blast`, JP rounds in `order`: the
     // kernels that also use them run only after this one declined the frame.
     FlowBufs F{sv->blast, reinterpret_cast<unsigned long long*>(sv->body_list), sv->slot, sv->link,

@@ -1,0 +1,398 @@
+// Batched scenes (included by solver.cu): one thread block solves one scene,
+// the scene's bodies staged in shared memory.
+//
+// The reference solves one scene per XpbdSolver::solve (xpbd_solver.cpp:
+// 603-733). A batch is many independent scenes, so each block takes one scene
+// and runs exactly that solve on it:
+//   * the scene's contacts are a contiguous run of the contact list (pairs are
+//     sorted by body a and a scene's bodies are contiguous), local contact
+//     index k = global index - first index;
+//   * a scene without contacts is left alone (the reference returns before
+//     any renormalisation when n_con == 0);
+//   * sequential order (set_force_serial, or n_con <= 256 in the reference
+//     mode, or a colouring that needs more than 64 colours or 256 rounds):
+//     contacts are solved in waves, contact k as soon as the previous contact
+//     of each of its dynamic bodies (in contact order) is solved — the serial
+//     loop's per-body order, so the result is bit-identical to it;
+//   * coloured order: Jones–Plassmann rounds with the priorities
+//     hash(k) << 32 | k of the local index (:645-688), then colour by colour;
+//   * every iteration renormalises every body of the scene (:579-584,
+//     :726-731); a contact deferred at w_total < 1e-10 is retried by the next
+//     iteration's sweep, as in the reference.
+// Each scene therefore evolves bit for bit as it does stepped alone in the
+// same mode. Waves and rounds are separated by block barriers; a scene whose
+// chain of dependent contacts is d long takes d waves.
+#pragma once
+
+namespace dyph {
+namespace {
+
+constexpr int kSceneThreads = 128;
+constexpr uint32_t kSceneNone = 0xFFFFFFFFu;
+constexpr uint32_t kSceneWords = 13;         // per-contact words (see SceneContacts)
+constexpr uint32_t kSceneMaxBodies = 65535;  // local body indices are 16 bits
+
+// Shared-memory bytes of a scene's body part (see the layout in scene_solve_kernel).
+__host__ __device__ __forceinline__ uint32_t scene_body_bytes(uint32_t nb) {
+    const uint32_t ldb = (nb + 3u) & ~3u;
+    return 20u * 4u * ldb + 2u * 8u * ldb + 4u * (ldb + 4u) + 4u * ldb;
+}
+
+struct SceneBufs {
+    const uint32_t* body_offset;  // [n_scenes + 1] first body of each scene
+    const uint32_t* scene_of;     // [n] scene of each body
+    const uint32_t* order;        // [n_scenes] scenes by descending body count (largest first)
+    uint32_t* range;              // [2 n_scenes] first / one-past-last contact of each scene
+    uint32_t* scratch;            // [kSceneWords][scratch_stride] per-contact words of scenes too big for shared memory
+    uint32_t scratch_stride;      // max contacts + n_scenes (one extra word per scene)
+    uint32_t n_scenes;
+    uint32_t smem_bytes;          // dynamic shared memory of one block
+};
+
+// First and one-past-last contact of every scene (range cleared to 0 first).
+__global__ void scene_range_kernel(dyph_contacts cv, SceneBufs S) {
+    const uint32_t nc = contact_count(cv);
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        const uint32_t s = S.scene_of[cv.body_a[c]];
+        if (c == 0 || S.scene_of[cv.body_a[c - 1]] != s) S.range[2 * s] = c;
+        if (c + 1 == nc || S.scene_of[cv.body_a[c + 1]] != s) S.range[2 * s + 1] = c + 1;
+    }
+}
+
+// Body rows of one scene in shared memory: row r of local body i at f[r * ld + i].
+// Rows 0-12 state, 13 inverse mass, 14-19 inverse inertia.
+struct SceneBodies {
+    float* f;
+    uint32_t ld;
+    __device__ __forceinline__ float& px(uint32_t i) const { return f[0 * ld + i]; }
+    __device__ __forceinline__ float& py(uint32_t i) const { return f[1 * ld + i]; }
+    __device__ __forceinline__ float& pz(uint32_t i) const { return f[2 * ld + i]; }
+    __device__ __forceinline__ float& qw(uint32_t i) const { return f[3 * ld + i]; }
+    __device__ __forceinline__ float& qx(uint32_t i) const { return f[4 * ld + i]; }
+    __device__ __forceinline__ float& qy(uint32_t i) const { return f[5 * ld + i]; }
+    __device__ __forceinline__ float& qz(uint32_t i) const { return f[6 * ld + i]; }
+    __device__ __forceinline__ float& vx(uint32_t i) const { return f[7 * ld + i]; }
+    __device__ __forceinline__ float& vy(uint32_t i) const { return f[8 * ld + i]; }
+    __device__ __forceinline__ float& vz(uint32_t i) const { return f[9 * ld + i]; }
+    __device__ __forceinline__ float& wx(uint32_t i) const { return f[10 * ld + i]; }
+    __device__ __forceinline__ float& wy(uint32_t i) const { return f[11 * ld + i]; }
+    __device__ __forceinline__ float& wz(uint32_t i) const { return f[12 * ld + i]; }
+    __device__ __forceinline__ float im(uint32_t i) const { return f[13 * ld + i]; }
+    __device__ __forceinline__ float ixx(uint32_t i) const { return f[14 * ld + i]; }
+    __device__ __forceinline__ float iyy(uint32_t i) const { return f[15 * ld + i]; }
+    __device__ __forceinline__ float izz(uint32_t i) const { return f[16 * ld + i]; }
+    __device__ __forceinline__ float ixy(uint32_t i) const { return f[17 * ld + i]; }
+    __device__ __forceinline__ float ixz(uint32_t i) const { return f[18 * ld + i]; }
+    __device__ __forceinline__ float iyz(uint32_t i) const { return f[19 * ld + i]; }
+};
+
+// Per-contact words of one scene (shared memory, or the global scratch for
+// a scene with too many contacts): row r of local contact k at w[r * ld + k].
+//   0 a | b << 16 (local body indices)   1 predecessor on a   2 predecessor on b
+//   3 wave solved in / colour            4 b-side list entry   5 lambda
+//   6-12 position xyz, normal xyz, depth (copied from the contact list)
+struct SceneContacts {
+    uint32_t* w;
+    uint32_t ld;
+    __device__ __forceinline__ uint32_t& ab(uint32_t k) const { return w[k]; }
+    __device__ __forceinline__ uint32_t& pa(uint32_t k) const { return w[1 * ld + k]; }
+    __device__ __forceinline__ uint32_t& pb(uint32_t k) const { return w[2 * ld + k]; }
+    __device__ __forceinline__ uint32_t& done(uint32_t k) const { return w[3 * ld + k]; }
+    __device__ __forceinline__ uint32_t& ent(uint32_t k) const { return w[4 * ld + k]; }
+    __device__ __forceinline__ float& lam(uint32_t k) const { return reinterpret_cast<float*>(w)[5 * ld + k]; }
+    __device__ __forceinline__ float& g(int r, uint32_t k) const { return reinterpret_cast<float*>(w)[(6 + r) * ld + k]; }
+    __device__ __forceinline__ Contact contact(uint32_t k) const {
+        Contact ct;
+        const uint32_t ab_k = ab(k);
+        ct.a = ab_k & 0xFFFFu;
+        ct.b = ab_k >> 16;
+        ct.px = g(0, k); ct.py = g(1, k); ct.pz = g(2, k);
+        ct.nx = g(3, k); ct.ny = g(4, k); ct.nz = g(5, k);
+        ct.depth = g(6, k);
+        return ct;
+    }
+};
+
+// Levels of the sequential order on one scene: level(k) = 1 + the larger
+// level of k's predecessors on its two dynamic bodies. Contacts of one level
+// share no dynamic body, and solving the levels in ascending order gives
+// every body its contacts in contact order: the serial loop's result, bit for
+// bit. Levels go to SC.done (1-based); returns the level count, or 0 if the
+// predecessor links were inconsistent (they cannot be: every predecessor has a
+// lower index).
+__device__ uint32_t scene_levels(uint32_t m, const SceneContacts& SC, uint32_t* s_max) {
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.done(k) = 0u;
+    if (threadIdx.x == 0) *s_max = 0u;
+    __syncthreads();
+    uint32_t my_max = 0;
+    for (uint32_t pass = 0;; ++pass) {
+        int pending = 0;
+        // A level, once written, is final, so a pass may use levels written
+        // by other threads during the same pass.
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            if (SC.done(k) != 0u) continue;
+            const uint32_t pa = SC.pa(k), pb = SC.pb(k);
+            const uint32_t la = pa == kSceneNone ? 0u : SC.done(pa);
+            const uint32_t lb = pb == kSceneNone ? 0u : SC.done(pb);
+            if ((pa != kSceneNone && la == 0u) || (pb != kSceneNone && lb == 0u)) {
+                pending = 1;
+                continue;
+            }
+            const uint32_t l = max(la, lb) + 1u;
+            SC.done(k) = l;
+            my_max = max(my_max, l);
+        }
+        if (!__syncthreads_or(pending)) break;
+        if (pass > m) return 0u;
+    }
+    atomicMax(s_max, my_max);
+    __syncthreads();
+    const uint32_t levels = *s_max;
+    __syncthreads();
+    return levels;
+}
+
+// Counting sort of the scene's contacts by group done(k) - base (a level or a
+// colour) into SC.ent; group g is SC.ent[SC.pa(g), SC.pa(g + 1)). The
+// predecessor rows are free once the groups are known.
+__device__ void scene_group(uint32_t m, uint32_t groups, uint32_t base, const SceneContacts& SC, uint32_t* s_scan,
+                            uint32_t* s_carry) {
+    for (uint32_t g = threadIdx.x; g <= groups; g += blockDim.x) SC.pa(g) = 0u;
+    if (threadIdx.x == 0) *s_carry = 0u;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) atomicAdd(&SC.pa(SC.done(k) - base), 1u);
+    __syncthreads();
+    for (uint32_t g0 = 0; g0 <= groups; g0 += blockDim.x) {
+        const uint32_t g = g0 + threadIdx.x;
+        const uint32_t v = g <= groups ? SC.pa(g) : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, s_scan, tot);
+        if (g <= groups) {
+            SC.pa(g) = *s_carry + ex;
+            SC.pb(g) = *s_carry + ex;  // fill cursor
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) *s_carry += tot;
+        __syncthreads();
+    }
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.ent(atomicAdd(&SC.pb(SC.done(k) - base), 1u)) = k;
+    __syncthreads();
+}
+
+// One sweep over the groups in ascending order, one contact per thread at a
+// time inside a group (no two of a group share a dynamic body).
+__device__ void scene_sweep(uint32_t groups, const SceneBodies& SB, const SceneContacts& SC, float mu, float dt,
+                            int* s_flag) {
+    for (uint32_t g = 0; g < groups; ++g) {
+        const uint32_t end = SC.pa(g + 1);
+        for (uint32_t i = SC.pa(g) + threadIdx.x; i < end; i += blockDim.x) {
+            const uint32_t k = SC.ent(i);
+            const Contact ct = SC.contact(k);
+            float lc = SC.lam(k);
+            if (solve_contact(SB, ct, mu, lc, dt) == kSolveDeferred) *s_flag = 1;
+            SC.lam(k) = lc;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_contacts cv, dyph_bodies gb,
+                                                                       SceneBufs S, int mode, int n_iters,
+                                                                       float mu, float dt,
+                                                                       uint32_t* __restrict__ color,
+                                                                       uint32_t* __restrict__ meta) {
+    extern __shared__ __align__(16) unsigned char scene_smem[];
+    __shared__ uint32_t s_scan[kSceneThreads / 32];
+    __shared__ uint32_t s_carry, s_rem, s_over, s_maxcol;
+    __shared__ int s_flag;
+    const GlobalBodies B{gb};
+    for (uint32_t t = blockIdx.x; t < S.n_scenes; t += gridDim.x) {
+        const uint32_t s = S.order[t];
+        const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
+        const uint32_t k0 = S.range[2 * s], m = S.range[2 * s + 1] - k0;
+        if (m == 0) continue;  // no contacts: the reference's solve returns at once
+        // ── layout: bodies, then (if they fit) the contact words ──
+        const uint32_t ldb = (nb + 3u) & ~3u;
+        float* fb = reinterpret_cast<float*>(scene_smem);
+        uint64_t* pri = reinterpret_cast<uint64_t*>(fb + 20 * ldb);  // [ldb] JP priorities (8-byte aligned)
+        uint64_t* mask = pri + ldb;                                  // [ldb] JP colour masks
+        uint32_t* off = reinterpret_cast<uint32_t*>(mask + ldb);     // [ldb + 4] b-side list offsets
+        uint32_t* cnt = off + ldb + 4;                               // [ldb] counts / fill cursors / last b-side
+        const uint32_t body_bytes = scene_body_bytes(nb);
+        const uint32_t ldc = (m + 4u) & ~3u;  // >= m + 1: group offsets take m + 1 words
+        const bool in_smem = body_bytes + kSceneWords * 4u * ldc <= S.smem_bytes;
+        const SceneBodies SB{fb, ldb};
+        // (in the scratch, scene s owns words [k0 + s, k0 + s + m] of each row: m + 1 words)
+        const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(scene_smem + body_bytes) : S.scratch + k0 + s,
+                               in_smem ? ldc : S.scratch_stride};
+        // ── stage the scene's bodies and contacts ──
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+            const uint32_t g = b0 + i;
+            SB.px(i) = B.px(g); SB.py(i) = B.py(g); SB.pz(i) = B.pz(g);
+            SB.qw(i) = B.qw(g); SB.qx(i) = B.qx(g); SB.qy(i) = B.qy(g); SB.qz(i) = B.qz(g);
+            SB.vx(i) = B.vx(g); SB.vy(i) = B.vy(g); SB.vz(i) = B.vz(g);
+            SB.wx(i) = B.wx(g); SB.wy(i) = B.wy(g); SB.wz(i) = B.wz(g);
+            fb[13 * ldb + i] = B.im(g);
+            fb[14 * ldb + i] = B.ixx(g); fb[15 * ldb + i] = B.iyy(g); fb[16 * ldb + i] = B.izz(g);
+            fb[17 * ldb + i] = B.ixy(g); fb[18 * ldb + i] = B.ixz(g); fb[19 * ldb + i] = B.iyz(g);
+            cnt[i] = 0u;
+        }
+        if (threadIdx.x == 0) {
+            s_flag = 0;
+            s_carry = 0u;
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            const uint32_t a = cv.body_a[k0 + k] - b0, b = cv.body_b[k0 + k] - b0;
+            SC.ab(k) = a | (b << 16);
+            SC.lam(k) = 0.f;
+            const uint32_t c = k0 + k;
+            SC.g(0, k) = cv.pos_x[c]; SC.g(1, k) = cv.pos_y[c]; SC.g(2, k) = cv.pos_z[c];
+            SC.g(3, k) = cv.norm_x[c]; SC.g(4, k) = cv.norm_y[c]; SC.g(5, k) = cv.norm_z[c];
+            SC.g(6, k) = cv.depth[c];
+            SC.pb(k) = kSceneNone;
+            if (SB.im(b) != 0.f) atomicAdd(&cnt[b], 1u);
+        }
+        __syncthreads();
+        // ── predecessors in contact order: b-side lists (count, scan, fill, sort) ──
+        for (uint32_t base = 0; base < nb; base += blockDim.x) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t v = i < nb ? cnt[i] : 0u;
+            uint32_t tot;
+            const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, s_scan, tot);
+            if (i < nb) {
+                off[i] = s_carry + ex;
+                cnt[i] = 0u;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry += tot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) off[nb] = s_carry;
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            const uint32_t b = SC.ab(k) >> 16;
+            if (SB.im(b) != 0.f) SC.ent(off[b] + atomicAdd(&cnt[b], 1u)) = k;
+        }
+        __syncthreads();
+        for (uint32_t x = threadIdx.x; x < nb; x += blockDim.x) {
+            const uint32_t lo = off[x], hi = off[x + 1];
+            for (uint32_t i = lo + 1; i < hi; ++i) {
+                const uint32_t v = SC.ent(i);
+                uint32_t j = i;
+                while (j > lo && SC.ent(j - 1) > v) {
+                    SC.ent(j) = SC.ent(j - 1);
+                    --j;
+                }
+                SC.ent(j) = v;
+            }
+            for (uint32_t i = lo + 1; i < hi; ++i) SC.pb(SC.ent(i)) = SC.ent(i - 1);
+            cnt[x] = hi > lo ? SC.ent(hi - 1) : kSceneNone;  // last b-side contact of x
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            const uint32_t a = SC.ab(k) & 0xFFFFu;
+            uint32_t p = kSceneNone;
+            if (SB.im(a) != 0.f) p = (k > 0 && (SC.ab(k - 1) & 0xFFFFu) == a) ? k - 1 : cnt[a];
+            SC.pa(k) = p;
+        }
+        // ── colouring (reference mode above 256 contacts, coloured mode always) ──
+        bool colored = mode == DYPH_SOLVER_COLORED ||
+                       ((mode == DYPH_SOLVER_REFERENCE || mode == DYPH_SOLVER_REFERENCE_ROUNDS) && m > kSerialThreshold);
+        uint32_t n_colors = 0, rounds = 0;
+        if (colored) {
+            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.done(k) = kUncolored;
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) mask[i] = 0ull;
+            if (threadIdx.x == 0) {
+                s_rem = m;
+                s_over = 0u;
+                s_maxcol = 0u;
+            }
+            __syncthreads();
+            while (s_rem > 0u && rounds < kMaxRounds) {
+                for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) pri[i] = 0ull;
+                __syncthreads();
+                for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+                    if (SC.done(k) != kUncolored) continue;
+                    const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
+                    const unsigned long long pk = (static_cast<unsigned long long>(hash_u32(k)) << 32) | k;
+                    if (SB.im(a) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[a]), pk);
+                    if (SB.im(b) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[b]), pk);
+                }
+                __syncthreads();
+                for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+                    if (SC.done(k) != kUncolored) continue;
+                    const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
+                    const bool da = SB.im(a) != 0.f, db = SB.im(b) != 0.f;
+                    const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
+                    if ((da && pri[a] != pk) || (db && pri[b] != pk)) continue;  // not a local maximum
+                    const uint64_t used = (da ? mask[a] : 0ull) | (db ? mask[b] : 0ull);
+                    if (~used == 0ull) {  // > 64 colours: the reference falls back to the serial order
+                        s_over = 1u;
+                        continue;
+                    }
+                    const uint32_t col = static_cast<uint32_t>(__ffsll(static_cast<long long>(~used)) - 1);
+                    SC.done(k) = col;
+                    const unsigned long long bit = 1ull << col;
+                    if (da) atomicOr(reinterpret_cast<unsigned long long*>(&mask[a]), bit);
+                    if (db) atomicOr(reinterpret_cast<unsigned long long*>(&mask[b]), bit);
+                    atomicMax(&s_maxcol, col);
+                    atomicSub(&s_rem, 1u);
+                }
+                __syncthreads();
+                ++rounds;
+            }
+            colored = s_rem == 0u && s_over == 0u;
+            n_colors = s_maxcol + 1u;
+            __syncthreads();
+        }
+        // ── groups: colours, or the levels of the sequential order ──
+        uint32_t groups = n_colors, base = 0u;
+        if (!colored) {
+            groups = scene_levels(m, SC, &s_maxcol);
+            base = 1u;
+            if (groups == 0u) {
+                if (threadIdx.x == 0) raise_error(DYPH_ERR_TIMEOUT, 11u);
+                return;
+            }
+        }
+        scene_group(m, groups, base, SC, s_scan, &s_carry);
+        // ── sweeps and renormalisation ──
+        bool deferred = false;
+        for (int iter = 0; iter < n_iters; ++iter) {
+            if (iter == 0 || deferred) {
+                scene_sweep(groups, SB, SC, mu, dt, &s_flag);
+                deferred = s_flag != 0;
+            }
+            const int times = deferred ? 1 : n_iters - iter;
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+                float qw = SB.qw(i), qx = SB.qx(i), qy = SB.qy(i), qz = SB.qz(i);
+                for (int t = 0; t < times; ++t) renormalize(qw, qx, qy, qz);
+                SB.qw(i) = qw; SB.qx(i) = qx; SB.qy(i) = qy; SB.qz(i) = qz;
+            }
+            __syncthreads();
+            if (!deferred) break;
+        }
+        // ── write back, colours and statistics ──
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+            const uint32_t g = b0 + i;
+            B.px(g) = SB.px(i); B.py(g) = SB.py(i); B.pz(g) = SB.pz(i);
+            B.qw(g) = SB.qw(i); B.qx(g) = SB.qx(i); B.qy(g) = SB.qy(i); B.qz(g) = SB.qz(i);
+            B.vx(g) = SB.vx(i); B.vy(g) = SB.vy(i); B.vz(g) = SB.vz(i);
+            B.wx(g) = SB.wx(i); B.wy(g) = SB.wy(i); B.wz(g) = SB.wz(i);
+        }
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) color[k0 + k] = colored ? SC.done(k) : kUncolored;
+        if (threadIdx.x == 0) {
+            if (colored) {
+                atomicMax(&meta[kMetaMaxColor], n_colors - 1u);
+                meta[kMetaSceneColored] = 1u;
+            }
+            atomicMax(&meta[kMetaRounds], rounds);
+            meta[kMetaDecision] = kDecisionScenes;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+}  // namespace dyph

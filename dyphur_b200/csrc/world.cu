@@ -8,6 +8,7 @@
 // the frame folds the pair / contact counts into peak and overflow words.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <new>
 
 #include "internal.cuh"
@@ -366,6 +367,10 @@ extern "C" dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, c
     DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
     dyph_status st = broadphase_set_scenes(w->bp, n_scenes, body_offset, scene_bounds);
     if (st != DYPH_OK) return st;
+    // One block per scene when the largest scene fits a block; otherwise the
+    // whole-batch kernels solve the batch.
+    st = xpbd_set_scenes(w->sv, n_scenes, body_offset, w->bp->body_offset, w->bp->bvh.scene_of);
+    if (st != DYPH_OK && st != DYPH_ERR_TOO_LARGE) return st;
     // Captured frames launch the single-scene form: record them again.
     if (w->graph) cudaGraphExecDestroy(w->graph);
     if (w->episode) cudaGraphExecDestroy(w->episode);

@@ -1,0 +1,131 @@
+"""Headless stress run on the GPU, a drop-in for the reference's
+stress_test_blocks example (examples/stress_test_blocks/main.cpp).
+
+    python -m dyphur_b200.run [out_prefix] [n_frames] [--grid NX NY NZ]
+                              [--spacing S] [--jitter J] [--profile]
+                              [--workload blocks|pile|batch] [--mode M]
+                              [--start-frame F]
+
+Writes <prefix>.scene, <prefix>.trajectory (poses every other frame),
+<prefix>.metrics.json and <prefix>.golden exactly as the example does. The
+default scene is the example's own: 8 x 16 x 8 boxes of half extent 0.4 m at
+1.0 m spacing, no jitter, on a ground plate, 300 frames at 60 Hz.
+
+--profile prints the per-stage milliseconds per frame over the frames after
+30 warm-up frames (the example's --profile table), timed by CUDA events
+recorded inside the captured frames instead of host fences.
+--start-frame F steps F frames untimed and writes nothing before the run:
+with `ncu -k regex:<kernel> -s F -c 1` it captures frame F's launch of a
+kernel that runs once per frame.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+
+import numpy as np
+
+
+def parse(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m dyphur_b200.run")
+    ap.add_argument("prefix", nargs="?", default="stress_test_blocks")
+    ap.add_argument("n_frames", nargs="?", type=int, default=300)
+    ap.add_argument("--grid", nargs=3, type=int, default=(8, 16, 8), metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--spacing", type=float, default=1.0)
+    ap.add_argument("--jitter", type=float, default=0.0)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--workload", default="blocks", choices=["blocks", "pile", "batch"])
+    ap.add_argument("--bodies", type=int, default=65536, help="pile: dynamic bodies")
+    ap.add_argument("--scenes", type=int, default=4096, help="batch: scenes")
+    ap.add_argument("--mode", default="reference", choices=["reference", "sequential", "colored"])
+    ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--start-frame", type=int, default=0)
+    ap.add_argument("--no-output", action="store_true", help="write no files")
+    return ap.parse_args(argv)
+
+
+def build_scene(args):
+    from . import scenes
+    if args.workload == "pile":
+        return scenes.random_pile(args.bodies, seed=args.seed)
+    if args.workload == "batch":
+        return scenes.batch(args.scenes, 8, 256, seed=args.seed)
+    nx, ny, nz = args.grid
+    return scenes.stress_blocks(spacing=args.spacing, jitter=args.jitter, seed=args.seed, grid=(nx, ny, nz))
+
+
+def profile(world, scene, frames: int, warm: int = 30) -> None:
+    """Per-stage ms per frame (integrate, broadphase, narrowphase, solver)."""
+    import torch
+    names = ("integrate", "build_and_query", "narrowphase", "solve (XPBD)")
+    fb = world.bodies.fbuf
+    init = fb.clone()
+    world.step(warm)
+    start = fb.clone()
+    rows = []
+    for stage in range(4):
+        fb.copy_(start)
+        world.capture_episode(frames, stage)
+        world.run_episode()
+        torch.cuda.synchronize()
+        rows.append(float(world.probe_ms().mean()))
+    fb.copy_(init)
+    total = sum(rows)
+    print(f"-- Per-stage avg over {frames} warm frames ({scene.n_bodies} bodies) --")
+    for name, ms in zip(names, rows):
+        print(f"  {name:<16} {ms:8.3f} ms   {100.0 * ms / total:5.1f}%")
+    print(f"  {'TOTAL':<16} {total:8.3f} ms   ({1000.0 / total:.1f} fps, stage-summed)")
+
+
+def main(argv=None) -> int:
+    import torch
+
+    from . import capi, device, formats
+
+    args = parse(argv)
+    mode = {"reference": capi.SOLVER_REFERENCE, "sequential": capi.SOLVER_SEQUENTIAL,
+            "colored": capi.SOLVER_COLORED}[args.mode]
+    scene = build_scene(args)
+    n = scene.n_bodies
+    world = device.World(scene, mode=mode)
+    if args.start_frame:
+        world.step(args.start_frame)
+        world.step(args.n_frames)
+        torch.cuda.synchronize()
+        print(f"stepped {args.start_frame} + {args.n_frames} frames, status {world.stats()['status']}")
+        return 0
+    if args.profile:
+        profile(world, scene, args.n_frames)
+        return 0
+    if not args.no_output:
+        formats.write_scene_set(args.prefix, scene)
+    records = formats.trajectory_records(args.n_frames)
+    traj = torch.empty((max(records, 1), n, 7), dtype=torch.float32).pin_memory()
+    world.set_trajectory(traj, 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    world.step(args.n_frames)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    world.set_trajectory(None)
+    st = world.stats()
+    h = world.hash()
+    if not args.no_output:
+        formats.write_trajectory(args.prefix, args.n_frames, traj.numpy()[:records])
+        formats.write_golden(args.prefix, h)
+        formats.write_metrics(args.prefix, n, args.n_frames, scene.dt, wall, float(st["last_contacts"]))
+    over = st["peak_pairs"] > world.desc.max_pairs or st["peak_contacts"] > world.desc.max_contacts
+    print(f"Peak usage: pairs {st['peak_pairs']}/{world.desc.max_pairs}, contacts "
+          f"{st['peak_contacts']}/{world.desc.max_contacts}" + (" -- CAPACITY OVERFLOW" if over else ""))
+    fps = args.n_frames / wall if wall > 0 else 0.0
+    print(f"Completed {args.n_frames} frames in {wall:.3f}s ({fps:.1f} fps, {fps / 60.0:.2f}x realtime)")
+    print(f"Hash: {h:016x}")
+    if not args.no_output:
+        print(f"Wrote: {args.prefix}.scene  {args.prefix}.trajectory  {args.prefix}.metrics.json  "
+              f"{args.prefix}.golden")
+    return 0 if not over and st["status"] == 0 else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())

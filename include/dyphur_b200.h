@@ -296,11 +296,16 @@ void dyph_world_destroy(dyph_world* w);
 /* Queue n_frames frame steps (graph-replayed after the first call). */
 dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_stream s);
 /* Batched scenes in one world (dyph_broadphase_set_scenes; desc.scene_bounds is
- * then unused). Narrowphase and solver run over all scenes at once: contacts
- * never join two scenes, so in DYPH_SOLVER_SEQUENTIAL every scene evolves
- * bit-identically to stepping it alone. The coloured modes colour the whole
- * batch (priorities are global contact indices), so their results differ from
- * a scene stepped alone by the colouring's drift. Drops captured graphs. */
+ * then unused). No reference counterpart: the reference steps one scene per
+ * solve (core/src/xpbd_solver.cpp:603-733). The solver then runs one thread
+ * block per scene over the scene's contiguous run of contacts, with the
+ * scene's own contact indices, so in EVERY mode each scene evolves
+ * bit-identically to stepping it alone in that mode (a scene without contacts
+ * in a frame is not renormalised, as the reference's solve returns at once).
+ * The largest scene's bodies must fit one block's shared memory (about 1,900
+ * bodies); otherwise the whole batch is solved as one contact set, which is
+ * exact per scene only in DYPH_SOLVER_SEQUENTIAL. Allocates; drops captured
+ * graphs. */
 dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset,
                                   const dyph_aabb* scene_bounds);
 /* Blocking: FNV-1a-64 of every scene's pose arrays (one value for a single
