@@ -54,6 +54,7 @@ _vp = C.c_void_p
 _st = C.c_int
 _PROTOS = {
     "dyph_status_string": (C.c_char_p, [C.c_int]),
+    "dyph_last_cuda_error": (C.c_char_p, []),
     "dyph_device_check": (_st, []),
     "dyph_download_device_error": (_st, [_vp, _up]),
     "dyph_download_device_error_site": (_st, [_vp, _up, _up]),
@@ -100,6 +101,7 @@ _PROTOS = {
     "dyph_world_run_episode": (_st, [_vp, _vp]),
     "dyph_world_download_history": (_st, [_vp, _vp, _vp, _vp, C.c_uint32, _up]),
     "dyph_world_set_trajectory": (_st, [_vp, _vp, C.c_uint32, C.c_uint32]),
+    "dyph_world_sync_lists": (_st, [_vp, _vp]),
     "dyph_event_create": (_st, [C.POINTER(_vp)]),
     "dyph_event_destroy": (None, [_vp]),
     "dyph_event_record": (_st, [_vp, _vp]),
@@ -130,6 +132,8 @@ def lib():
 class DyphError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         msg = lib().dyph_status_string(status).decode()
+        if status == ERR_CUDA:
+            msg += ": " + lib().dyph_last_cuda_error().decode()
         super().__init__(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
         self.status = status
 

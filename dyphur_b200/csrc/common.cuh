@@ -176,8 +176,17 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t n_blocks) {
 
 }  // namespace dyph
 
+namespace dyph {
+// The CUDA error behind the calling thread's last DYPH_ERR_CUDA
+// (dyph_last_cuda_error).
+inline thread_local cudaError_t t_last_cuda_error = cudaSuccess;
+}  // namespace dyph
+
 #define DYPH_CUDA_TRY(expr)                                   \
     do {                                                      \
         cudaError_t _e = (expr);                              \
-        if (_e != cudaSuccess) return DYPH_ERR_CUDA;          \
+        if (_e != cudaSuccess) {                              \
+            dyph::t_last_cuda_error = _e;                     \
+            return DYPH_ERR_CUDA;                             \
+        }                                                     \
     } while (0)

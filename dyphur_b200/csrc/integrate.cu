@@ -63,6 +63,10 @@ extern "C" const char* dyph_status_string(int status) {
     }
 }
 
+extern "C" const char* dyph_last_cuda_error(void) {
+    return cudaGetErrorString(dyph::t_last_cuda_error);
+}
+
 extern "C" dyph_status dyph_device_check(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {

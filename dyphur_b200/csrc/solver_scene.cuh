@@ -196,15 +196,211 @@ __device__ void scene_sweep(uint32_t groups, const SceneBodies& SB, const SceneC
     }
 }
 
+// Block-shared scalars of one scene's solve.
+struct SceneShared {
+    uint32_t scan[kSceneThreads / 32];
+    uint32_t carry, rem, over, maxcol;
+    int flag;
+};
+
+// The solver's per-body rows after the 20 body rows (see scene_body_bytes).
+struct SceneSolverRows {
+    uint64_t* pri;   // [ldb] JP priorities
+    uint64_t* mask;  // [ldb] JP colour masks
+    uint32_t* off;   // [ldb + 4] b-side list offsets
+    uint32_t* cnt;   // [ldb] counts / fill cursors / last b-side contact
+};
+
+__device__ __forceinline__ SceneSolverRows scene_solver_rows(float* fb, uint32_t ldb) {
+    SceneSolverRows R;
+    R.pri = reinterpret_cast<uint64_t*>(fb + 20 * ldb);
+    R.mask = R.pri + ldb;
+    R.off = reinterpret_cast<uint32_t*>(R.mask + ldb);
+    R.cnt = R.off + ldb + 4;
+    return R;
+}
+
+__device__ __forceinline__ void scene_load_bodies(const GlobalBodies& B, uint32_t b0, uint32_t nb, float* fb,
+                                                  uint32_t ldb) {
+    const SceneBodies SB{fb, ldb};
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        const uint32_t g = b0 + i;
+        SB.px(i) = B.px(g); SB.py(i) = B.py(g); SB.pz(i) = B.pz(g);
+        SB.qw(i) = B.qw(g); SB.qx(i) = B.qx(g); SB.qy(i) = B.qy(g); SB.qz(i) = B.qz(g);
+        SB.vx(i) = B.vx(g); SB.vy(i) = B.vy(g); SB.vz(i) = B.vz(g);
+        SB.wx(i) = B.wx(g); SB.wy(i) = B.wy(g); SB.wz(i) = B.wz(g);
+        fb[13 * ldb + i] = B.im(g);
+        fb[14 * ldb + i] = B.ixx(g); fb[15 * ldb + i] = B.iyy(g); fb[16 * ldb + i] = B.izz(g);
+        fb[17 * ldb + i] = B.ixy(g); fb[18 * ldb + i] = B.ixz(g); fb[19 * ldb + i] = B.iyz(g);
+    }
+}
+
+__device__ __forceinline__ void scene_store_bodies(const GlobalBodies& B, uint32_t b0, uint32_t nb,
+                                                   const SceneBodies& SB) {
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        const uint32_t g = b0 + i;
+        B.px(g) = SB.px(i); B.py(g) = SB.py(i); B.pz(g) = SB.pz(i);
+        B.qw(g) = SB.qw(i); B.qx(g) = SB.qx(i); B.qy(g) = SB.qy(i); B.qz(g) = SB.qz(i);
+        B.vx(g) = SB.vx(i); B.vy(g) = SB.vy(i); B.vz(g) = SB.vz(i);
+        B.wx(g) = SB.wx(i); B.wy(g) = SB.wy(i); B.wz(g) = SB.wz(i);
+    }
+}
+
+// XpbdSolver::solve on one scene whose m >= 1 contacts sit in SC (rows ab,
+// lambda = 0, geometry; pb = none) with R.cnt[b] = the b-side contact count of
+// every dynamic body b. Leaves the bodies solved and renormalised in SB and
+// the colours (or UINT32_MAX) in SC.done. Returns false after raising an error.
+__device__ bool scene_solve(uint32_t nb, uint32_t m, const SceneBodies& SB, const SceneSolverRows& R,
+                            const SceneContacts& SC, int mode, int n_iters, float mu, float dt, SceneShared& sh,
+                            bool& colored_out, uint32_t& n_colors_out, uint32_t& rounds_out) {
+    // ── predecessors in contact order: b-side lists (scan, fill, sort) ──
+    if (threadIdx.x == 0) {
+        sh.carry = 0u;
+        sh.flag = 0;
+    }
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < nb ? R.cnt[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, sh.scan, tot);
+        if (i < nb) {
+            R.off[i] = sh.carry + ex;
+            R.cnt[i] = 0u;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sh.carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) R.off[nb] = sh.carry;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const uint32_t b = SC.ab(k) >> 16;
+        if (SB.im(b) != 0.f) SC.ent(R.off[b] + atomicAdd(&R.cnt[b], 1u)) = k;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < nb; x += blockDim.x) {
+        const uint32_t lo = R.off[x], hi = R.off[x + 1];
+        for (uint32_t i = lo + 1; i < hi; ++i) {
+            const uint32_t v = SC.ent(i);
+            uint32_t j = i;
+            while (j > lo && SC.ent(j - 1) > v) {
+                SC.ent(j) = SC.ent(j - 1);
+                --j;
+            }
+            SC.ent(j) = v;
+        }
+        for (uint32_t i = lo + 1; i < hi; ++i) SC.pb(SC.ent(i)) = SC.ent(i - 1);
+        R.cnt[x] = hi > lo ? SC.ent(hi - 1) : kSceneNone;  // last b-side contact of x
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const uint32_t a = SC.ab(k) & 0xFFFFu;
+        uint32_t p = kSceneNone;
+        if (SB.im(a) != 0.f) p = (k > 0 && (SC.ab(k - 1) & 0xFFFFu) == a) ? k - 1 : R.cnt[a];
+        SC.pa(k) = p;
+    }
+    // ── colouring (reference mode above 256 contacts, coloured mode always) ──
+    bool colored = mode == DYPH_SOLVER_COLORED ||
+                   ((mode == DYPH_SOLVER_REFERENCE || mode == DYPH_SOLVER_REFERENCE_ROUNDS) && m > kSerialThreshold);
+    uint32_t n_colors = 0, rounds = 0;
+    if (colored) {
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.done(k) = kUncolored;
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.mask[i] = 0ull;
+        if (threadIdx.x == 0) {
+            sh.rem = m;
+            sh.over = 0u;
+            sh.maxcol = 0u;
+        }
+        __syncthreads();
+        while (sh.rem > 0u && rounds < kMaxRounds) {
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.pri[i] = 0ull;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+                if (SC.done(k) != kUncolored) continue;
+                const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
+                const unsigned long long pk = (static_cast<unsigned long long>(hash_u32(k)) << 32) | k;
+                if (SB.im(a) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&R.pri[a]), pk);
+                if (SB.im(b) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&R.pri[b]), pk);
+            }
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+                if (SC.done(k) != kUncolored) continue;
+                const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
+                const bool da = SB.im(a) != 0.f, db = SB.im(b) != 0.f;
+                const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
+                if ((da && R.pri[a] != pk) || (db && R.pri[b] != pk)) continue;  // not a local maximum
+                const uint64_t used = (da ? R.mask[a] : 0ull) | (db ? R.mask[b] : 0ull);
+                if (~used == 0ull) {  // > 64 colours: the reference falls back to the serial order
+                    sh.over = 1u;
+                    continue;
+                }
+                const uint32_t col = static_cast<uint32_t>(__ffsll(static_cast<long long>(~used)) - 1);
+                SC.done(k) = col;
+                const unsigned long long bit = 1ull << col;
+                if (da) atomicOr(reinterpret_cast<unsigned long long*>(&R.mask[a]), bit);
+                if (db) atomicOr(reinterpret_cast<unsigned long long*>(&R.mask[b]), bit);
+                atomicMax(&sh.maxcol, col);
+                atomicSub(&sh.rem, 1u);
+            }
+            __syncthreads();
+            ++rounds;
+        }
+        colored = sh.rem == 0u && sh.over == 0u;
+        n_colors = sh.maxcol + 1u;
+        __syncthreads();
+    }
+    // ── groups: colours, or the levels of the sequential order ──
+    uint32_t groups = n_colors, base = 0u;
+    if (!colored) {
+        groups = scene_levels(m, SC, &sh.maxcol);
+        base = 1u;
+        if (groups == 0u) {
+            if (threadIdx.x == 0) raise_error(DYPH_ERR_TIMEOUT, 11u);
+            return false;
+        }
+    }
+    scene_group(m, groups, base, SC, sh.scan, &sh.carry);
+    // ── sweeps and renormalisation ──
+    bool deferred = false;
+    for (int iter = 0; iter < n_iters; ++iter) {
+        if (iter == 0 || deferred) {
+            scene_sweep(groups, SB, SC, mu, dt, &sh.flag);
+            deferred = sh.flag != 0;
+        }
+        const int times = deferred ? 1 : n_iters - iter;
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+            float qw = SB.qw(i), qx = SB.qx(i), qy = SB.qy(i), qz = SB.qz(i);
+            for (int t = 0; t < times; ++t) renormalize(qw, qx, qy, qz);
+            SB.qw(i) = qw; SB.qx(i) = qx; SB.qy(i) = qy; SB.qz(i) = qz;
+        }
+        __syncthreads();
+        if (!deferred) break;
+    }
+    colored_out = colored;
+    n_colors_out = n_colors;
+    rounds_out = rounds;
+    return true;
+}
+
+__device__ __forceinline__ void scene_stats(uint32_t* meta, bool colored, uint32_t n_colors, uint32_t rounds) {
+    if (threadIdx.x == 0) {
+        if (colored) {
+            atomicMax(&meta[kMetaMaxColor], n_colors - 1u);
+            meta[kMetaSceneColored] = 1u;
+        }
+        atomicMax(&meta[kMetaRounds], rounds);
+        meta[kMetaDecision] = kDecisionScenes;
+    }
+}
+
 __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_contacts cv, dyph_bodies gb,
                                                                        SceneBufs S, int mode, int n_iters,
                                                                        float mu, float dt,
                                                                        uint32_t* __restrict__ color,
                                                                        uint32_t* __restrict__ meta) {
     extern __shared__ __align__(16) unsigned char scene_smem[];
-    __shared__ uint32_t s_scan[kSceneThreads / 32];
-    __shared__ uint32_t s_carry, s_rem, s_over, s_maxcol;
-    __shared__ int s_flag;
+    __shared__ SceneShared sh;
     const GlobalBodies B{gb};
     for (uint32_t t = blockIdx.x; t < S.n_scenes; t += gridDim.x) {
         const uint32_t s = S.order[t];
@@ -214,10 +410,7 @@ __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_cont
         // ── layout: bodies, then (if they fit) the contact words ──
         const uint32_t ldb = (nb + 3u) & ~3u;
         float* fb = reinterpret_cast<float*>(scene_smem);
-        uint64_t* pri = reinterpret_cast<uint64_t*>(fb + 20 * ldb);  // [ldb] JP priorities (8-byte aligned)
-        uint64_t* mask = pri + ldb;                                  // [ldb] JP colour masks
-        uint32_t* off = reinterpret_cast<uint32_t*>(mask + ldb);     // [ldb + 4] b-side list offsets
-        uint32_t* cnt = off + ldb + 4;                               // [ldb] counts / fill cursors / last b-side
+        const SceneSolverRows R = scene_solver_rows(fb, ldb);
         const uint32_t body_bytes = scene_body_bytes(nb);
         const uint32_t ldc = (m + 4u) & ~3u;  // >= m + 1: group offsets take m + 1 words
         const bool in_smem = body_bytes + kSceneWords * 4u * ldc <= S.smem_bytes;
@@ -226,21 +419,8 @@ __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_cont
         const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(scene_smem + body_bytes) : S.scratch + k0 + s,
                                in_smem ? ldc : S.scratch_stride};
         // ── stage the scene's bodies and contacts ──
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-            const uint32_t g = b0 + i;
-            SB.px(i) = B.px(g); SB.py(i) = B.py(g); SB.pz(i) = B.pz(g);
-            SB.qw(i) = B.qw(g); SB.qx(i) = B.qx(g); SB.qy(i) = B.qy(g); SB.qz(i) = B.qz(g);
-            SB.vx(i) = B.vx(g); SB.vy(i) = B.vy(g); SB.vz(i) = B.vz(g);
-            SB.wx(i) = B.wx(g); SB.wy(i) = B.wy(g); SB.wz(i) = B.wz(g);
-            fb[13 * ldb + i] = B.im(g);
-            fb[14 * ldb + i] = B.ixx(g); fb[15 * ldb + i] = B.iyy(g); fb[16 * ldb + i] = B.izz(g);
-            fb[17 * ldb + i] = B.ixy(g); fb[18 * ldb + i] = B.ixz(g); fb[19 * ldb + i] = B.iyz(g);
-            cnt[i] = 0u;
-        }
-        if (threadIdx.x == 0) {
-            s_flag = 0;
-            s_carry = 0u;
-        }
+        scene_load_bodies(B, b0, nb, fb, ldb);
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.cnt[i] = 0u;
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
             const uint32_t a = cv.body_a[k0 + k] - b0, b = cv.body_b[k0 + k] - b0;
@@ -251,145 +431,16 @@ __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_cont
             SC.g(3, k) = cv.norm_x[c]; SC.g(4, k) = cv.norm_y[c]; SC.g(5, k) = cv.norm_z[c];
             SC.g(6, k) = cv.depth[c];
             SC.pb(k) = kSceneNone;
-            if (SB.im(b) != 0.f) atomicAdd(&cnt[b], 1u);
+            if (SB.im(b) != 0.f) atomicAdd(&R.cnt[b], 1u);
         }
         __syncthreads();
-        // ── predecessors in contact order: b-side lists (count, scan, fill, sort) ──
-        for (uint32_t base = 0; base < nb; base += blockDim.x) {
-            const uint32_t i = base + threadIdx.x;
-            const uint32_t v = i < nb ? cnt[i] : 0u;
-            uint32_t tot;
-            const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, s_scan, tot);
-            if (i < nb) {
-                off[i] = s_carry + ex;
-                cnt[i] = 0u;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) s_carry += tot;
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) off[nb] = s_carry;
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
-            const uint32_t b = SC.ab(k) >> 16;
-            if (SB.im(b) != 0.f) SC.ent(off[b] + atomicAdd(&cnt[b], 1u)) = k;
-        }
-        __syncthreads();
-        for (uint32_t x = threadIdx.x; x < nb; x += blockDim.x) {
-            const uint32_t lo = off[x], hi = off[x + 1];
-            for (uint32_t i = lo + 1; i < hi; ++i) {
-                const uint32_t v = SC.ent(i);
-                uint32_t j = i;
-                while (j > lo && SC.ent(j - 1) > v) {
-                    SC.ent(j) = SC.ent(j - 1);
-                    --j;
-                }
-                SC.ent(j) = v;
-            }
-            for (uint32_t i = lo + 1; i < hi; ++i) SC.pb(SC.ent(i)) = SC.ent(i - 1);
-            cnt[x] = hi > lo ? SC.ent(hi - 1) : kSceneNone;  // last b-side contact of x
-        }
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
-            const uint32_t a = SC.ab(k) & 0xFFFFu;
-            uint32_t p = kSceneNone;
-            if (SB.im(a) != 0.f) p = (k > 0 && (SC.ab(k - 1) & 0xFFFFu) == a) ? k - 1 : cnt[a];
-            SC.pa(k) = p;
-        }
-        // ── colouring (reference mode above 256 contacts, coloured mode always) ──
-        bool colored = mode == DYPH_SOLVER_COLORED ||
-                       ((mode == DYPH_SOLVER_REFERENCE || mode == DYPH_SOLVER_REFERENCE_ROUNDS) && m > kSerialThreshold);
+        bool colored = false;
         uint32_t n_colors = 0, rounds = 0;
-        if (colored) {
-            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.done(k) = kUncolored;
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) mask[i] = 0ull;
-            if (threadIdx.x == 0) {
-                s_rem = m;
-                s_over = 0u;
-                s_maxcol = 0u;
-            }
-            __syncthreads();
-            while (s_rem > 0u && rounds < kMaxRounds) {
-                for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) pri[i] = 0ull;
-                __syncthreads();
-                for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
-                    if (SC.done(k) != kUncolored) continue;
-                    const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
-                    const unsigned long long pk = (static_cast<unsigned long long>(hash_u32(k)) << 32) | k;
-                    if (SB.im(a) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[a]), pk);
-                    if (SB.im(b) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&pri[b]), pk);
-                }
-                __syncthreads();
-                for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
-                    if (SC.done(k) != kUncolored) continue;
-                    const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
-                    const bool da = SB.im(a) != 0.f, db = SB.im(b) != 0.f;
-                    const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
-                    if ((da && pri[a] != pk) || (db && pri[b] != pk)) continue;  // not a local maximum
-                    const uint64_t used = (da ? mask[a] : 0ull) | (db ? mask[b] : 0ull);
-                    if (~used == 0ull) {  // > 64 colours: the reference falls back to the serial order
-                        s_over = 1u;
-                        continue;
-                    }
-                    const uint32_t col = static_cast<uint32_t>(__ffsll(static_cast<long long>(~used)) - 1);
-                    SC.done(k) = col;
-                    const unsigned long long bit = 1ull << col;
-                    if (da) atomicOr(reinterpret_cast<unsigned long long*>(&mask[a]), bit);
-                    if (db) atomicOr(reinterpret_cast<unsigned long long*>(&mask[b]), bit);
-                    atomicMax(&s_maxcol, col);
-                    atomicSub(&s_rem, 1u);
-                }
-                __syncthreads();
-                ++rounds;
-            }
-            colored = s_rem == 0u && s_over == 0u;
-            n_colors = s_maxcol + 1u;
-            __syncthreads();
-        }
-        // ── groups: colours, or the levels of the sequential order ──
-        uint32_t groups = n_colors, base = 0u;
-        if (!colored) {
-            groups = scene_levels(m, SC, &s_maxcol);
-            base = 1u;
-            if (groups == 0u) {
-                if (threadIdx.x == 0) raise_error(DYPH_ERR_TIMEOUT, 11u);
-                return;
-            }
-        }
-        scene_group(m, groups, base, SC, s_scan, &s_carry);
-        // ── sweeps and renormalisation ──
-        bool deferred = false;
-        for (int iter = 0; iter < n_iters; ++iter) {
-            if (iter == 0 || deferred) {
-                scene_sweep(groups, SB, SC, mu, dt, &s_flag);
-                deferred = s_flag != 0;
-            }
-            const int times = deferred ? 1 : n_iters - iter;
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-                float qw = SB.qw(i), qx = SB.qx(i), qy = SB.qy(i), qz = SB.qz(i);
-                for (int t = 0; t < times; ++t) renormalize(qw, qx, qy, qz);
-                SB.qw(i) = qw; SB.qx(i) = qx; SB.qy(i) = qy; SB.qz(i) = qz;
-            }
-            __syncthreads();
-            if (!deferred) break;
-        }
+        if (!scene_solve(nb, m, SB, R, SC, mode, n_iters, mu, dt, sh, colored, n_colors, rounds)) return;
         // ── write back, colours and statistics ──
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-            const uint32_t g = b0 + i;
-            B.px(g) = SB.px(i); B.py(g) = SB.py(i); B.pz(g) = SB.pz(i);
-            B.qw(g) = SB.qw(i); B.qx(g) = SB.qx(i); B.qy(g) = SB.qy(i); B.qz(g) = SB.qz(i);
-            B.vx(g) = SB.vx(i); B.vy(g) = SB.vy(i); B.vz(g) = SB.vz(i);
-            B.wx(g) = SB.wx(i); B.wy(g) = SB.wy(i); B.wz(g) = SB.wz(i);
-        }
+        scene_store_bodies(B, b0, nb, SB);
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) color[k0 + k] = colored ? SC.done(k) : kUncolored;
-        if (threadIdx.x == 0) {
-            if (colored) {
-                atomicMax(&meta[kMetaMaxColor], n_colors - 1u);
-                meta[kMetaSceneColored] = 1u;
-            }
-            atomicMax(&meta[kMetaRounds], rounds);
-            meta[kMetaDecision] = kDecisionScenes;
-        }
+        scene_stats(meta, colored, n_colors, rounds);
         __syncthreads();
     }
 }

@@ -10,8 +10,10 @@
 
 #include <algorithm>
 #include <new>
+#include <vector>
 
 #include "internal.cuh"
+#include "scene_frame.cuh"
 
 struct dyph_world {
     dyph_world_desc desc{};
@@ -37,6 +39,18 @@ struct dyph_world {
     cudaEvent_t traj_copied[2] = {nullptr, nullptr};
     bool traj_pending = false;            // a copy on the side stream not yet joined
     bool traj_live[2] = {false, false};   // traj_copied[k] was last recorded outside a capture
+    // Batched scenes with the whole frame fused into one kernel (one block per scene).
+    bool fused = false;
+    uint32_t frame_smem = 0;
+    uint32_t* f_pair_base = nullptr;     // [n_scenes + 1]
+    uint32_t* f_contact_base = nullptr;  // [n_scenes + 1]
+    uint32_t* f_pair_raw = nullptr;
+    uint32_t* f_contact_raw = nullptr;
+    uint32_t* f_color_raw = nullptr;
+    uint32_t* f_counts = nullptr;        // [4 n_scenes]
+    uint32_t* f_words = nullptr;
+    uint32_t* f_pos = nullptr;           // [2 n_scenes] gather positions
+    uint32_t f_words_stride = 0, f_contact_slots = 0;
 };
 
 namespace dyph {
@@ -115,6 +129,29 @@ dyph_status enqueue_frame(dyph_world* w, cudaStream_t s, int probe_stage = -1, v
                           void* ev1 = nullptr) {
     const dyph_world_desc& d = w->desc;
     dyph_status st;
+    if (w->fused) {
+        // One launch per frame: every scene's integrate, pairs, narrowphase and solve.
+        DYPH_CUDA_TRY(cudaMemsetAsync(w->bp->counts, 0, 4 * sizeof(uint32_t), s));
+        DYPH_CUDA_TRY(cudaMemsetAsync(w->np->counts, 0, 4 * sizeof(uint32_t), s));
+        DYPH_CUDA_TRY(cudaMemsetAsync(w->sv->meta, 0, 16 * sizeof(uint32_t), s));
+        if (probe_stage >= 0 && (st = probe_record(ev0, s)) != DYPH_OK) return st;
+        const dyph_integrator_params& ip = d.integrator;
+        const float sub_dt = ip.dt / static_cast<float>(ip.n_substeps);
+        SceneBufs S{w->bp->body_offset, w->bp->bvh.scene_of, w->sv->scene_order, nullptr, nullptr, 0,
+                    w->bp->n_scenes, w->frame_smem};
+        FrameBufs F{w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw,
+                    w->f_counts, w->f_words, w->f_words_stride, w->f_contact_slots};
+        scene_frame_kernel<<<w->bp->n_scenes, kSceneThreads, w->frame_smem, s>>>(
+            d.bodies, d.shapes, S, F, ip.gravity[0], ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt,
+            ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->friction, ip.dt, w->sv->meta,
+            w->bp->counts, w->np->counts, w->stats + 4);
+        DYPH_CUDA_TRY(cudaGetLastError());
+        if (probe_stage >= 0 && (st = probe_record(ev1, s)) != DYPH_OK) return st;
+        frame_stats_kernel<<<1, 1, 0, s>>>(w->bp->counts, w->np->counts, w->bp->max_pairs, w->np->max_contacts,
+                                           w->stats);
+        DYPH_CUDA_TRY(cudaGetLastError());
+        return DYPH_OK;
+    }
     w->sv->probe_flow[0] = probe_stage == 4 ? ev0 : nullptr;
     w->sv->probe_flow[1] = probe_stage == 4 ? ev1 : nullptr;
     for (int stage = 0; stage < 4; ++stage) {
@@ -159,6 +196,10 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
         if (w->traj_copied[k]) cudaEventDestroy(w->traj_copied[k]);
     }
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
+    void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
+                  w->f_words, w->f_pos};
+    for (void* p : fb)
+        if (p) cudaFree(p);
     broadphase_destroy(w->bp);
     narrowphase_destroy(w->np);
     xpbd_destroy(w->sv);
@@ -361,6 +402,69 @@ extern "C" dyph_status dyph_world_solver(dyph_world* w, dyph_xpbd** out) {
     return DYPH_OK;
 }
 
+namespace {
+
+// Fused frames for batched scenes: per-scene pair / contact slots sized as the
+// scene's own capacities when stepped alone (48 n + 64 pairs, 16 n + 64
+// contacts), and one block's shared memory for the largest scene's bodies
+// plus about two contacts per body.
+dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset) {
+    w->fused = false;
+    uint32_t max_nb = 0;
+    std::vector<uint32_t> pb(n_scenes + 1, 0u), cb(n_scenes + 1, 0u);
+    for (uint32_t i = 0; i < n_scenes; ++i) {
+        const uint32_t nb = body_offset[i + 1] - body_offset[i];
+        max_nb = std::max(max_nb, nb);
+        pb[i + 1] = pb[i] + std::max(64u, 48u * nb + 64u);
+        cb[i + 1] = cb[i] + std::max(64u, 16u * nb + 64u);
+    }
+    constexpr uint32_t kMaxSmem = 200u * 1024u;
+    const uint32_t body_bytes = frame_body_bytes(max_nb);
+    if (body_bytes + 56u * 64u > kMaxSmem) return DYPH_ERR_TOO_LARGE;
+    const uint32_t smem = std::min(kMaxSmem, body_bytes + (4u + kSceneWords * 4u) * 2u * std::max(64u, max_nb));
+    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+    uint32_t** bufs[] = {&w->f_pair_base, &w->f_contact_base, &w->f_pair_raw, &w->f_contact_raw, &w->f_color_raw,
+                         &w->f_counts, &w->f_words, &w->f_pos};
+    for (uint32_t** b : bufs) {
+        if (*b) cudaFree(*b);
+        *b = nullptr;
+    }
+    const size_t pslots = pb[n_scenes], cslots = cb[n_scenes];
+    w->f_contact_slots = static_cast<uint32_t>(cslots);
+    w->f_words_stride = static_cast<uint32_t>(cslots + n_scenes);
+    const size_t sizes[] = {n_scenes + 1ull, n_scenes + 1ull, pslots, 9 * cslots, cslots, 4ull * n_scenes,
+                            static_cast<size_t>(kSceneWords) * w->f_words_stride, 2ull * n_scenes};
+    for (int k = 0; k < 8; ++k)
+        if (cudaMalloc(bufs[k], sizes[k] * sizeof(uint32_t)) != cudaSuccess) return DYPH_ERR_NOMEM;
+    DYPH_CUDA_TRY(cudaMemcpy(w->f_pair_base, pb.data(), pb.size() * 4, cudaMemcpyHostToDevice));
+    DYPH_CUDA_TRY(cudaMemcpy(w->f_contact_base, cb.data(), cb.size() * 4, cudaMemcpyHostToDevice));
+    DYPH_CUDA_TRY(cudaMemset(w->f_counts, 0, 4ull * n_scenes * sizeof(uint32_t)));
+    w->frame_smem = smem;
+    w->fused = true;
+    return DYPH_OK;
+}
+
+}  // namespace
+
+extern "C" dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s) {
+    if (!w) return DYPH_ERR_INVALID;
+    if (!w->fused) return DYPH_OK;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaEventRecord(w->ev_in, cs));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(w->stream, w->ev_in, 0));
+    const uint32_t n = w->bp->n_scenes;
+    scene_gather_scan_kernel<<<1, 1024, 0, w->stream>>>(w->f_counts, n, w->f_pos, w->bp->counts, w->np->counts);
+    SceneBufs S{w->bp->body_offset, w->bp->bvh.scene_of, w->sv->scene_order, nullptr, nullptr, 0, n, 0};
+    FrameBufs F{w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
+                w->f_words, w->f_words_stride, w->f_contact_slots};
+    scene_gather_copy_kernel<<<n, 256, 0, w->stream>>>(S, F, w->f_pos, w->bp->pairs, w->np->view, w->sv->color);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    DYPH_CUDA_TRY(cudaEventRecord(w->ev_out, w->stream));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->ev_out, 0));
+    return DYPH_OK;
+}
+
 extern "C" dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset,
                                              const dyph_aabb* scene_bounds) {
     if (!w || !body_offset || n_scenes == 0 || body_offset[n_scenes] != w->desc.bodies.n) return DYPH_ERR_INVALID;
@@ -371,6 +475,10 @@ extern "C" dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, c
     // whole-batch kernels solve the batch.
     st = xpbd_set_scenes(w->sv, n_scenes, body_offset, w->bp->body_offset, w->bp->bvh.scene_of);
     if (st != DYPH_OK && st != DYPH_ERR_TOO_LARGE) return st;
+    if (st == DYPH_OK) {
+        st = setup_fused(w, n_scenes, body_offset);
+        if (st != DYPH_OK && st != DYPH_ERR_TOO_LARGE) return st;
+    }
     // Captured frames launch the single-scene form: record them again.
     if (w->graph) cudaGraphExecDestroy(w->graph);
     if (w->episode) cudaGraphExecDestroy(w->episode);

@@ -416,8 +416,13 @@ class World:
         check(capi.lib().dyph_world_scene_hashes(self.h, _stream_ptr(stream), out.ctypes.data, n))
         return out
 
+    def sync_lists(self) -> None:
+        """Compact the last frame's per-scene pair / contact lists (fused batched frames)."""
+        check(capi.lib().dyph_world_sync_lists(self.h, None), "dyph_world_sync_lists")
+
     def pairs(self) -> np.ndarray:
         L = capi.lib()
+        self.sync_lists()
         n = C.c_uint32()
         check(L.dyph_broadphase_download_count(self._bp, None, C.byref(n)))
         m = min(int(n.value), int(L.dyph_broadphase_max_pairs(self._bp)))
@@ -426,6 +431,7 @@ class World:
         return host.numpy().view(np.uint32).copy()
 
     def contacts(self):
+        self.sync_lists()
         v = capi.Contacts()
         check(capi.lib().dyph_narrowphase_contacts(self._np, C.byref(v)))
         a, b = C.c_uint32(), C.c_uint32()
@@ -442,6 +448,7 @@ class World:
 
     def colors(self, n: int):
         """JP colours of the last frame's solve (UINT32_MAX on the sequential path) and the colour count."""
+        self.sync_lists()
         out = np.empty(max(n, 1), np.uint32)
         nc = C.c_uint32()
         check(capi.lib().dyph_xpbd_download_colors(self._sv, None, out.ctypes.data_as(capi._up), n, C.byref(nc)))

@@ -136,6 +136,9 @@ typedef enum dyph_solver_mode {
 /* ── library ──────────────────────────────────────────────────────────────── */
 
 const char* dyph_status_string(int status);
+/* Text of the CUDA runtime error behind the calling thread's last
+ * DYPH_ERR_CUDA ("no error" if there was none). */
+const char* dyph_last_cuda_error(void);
 /* Returns DYPH_OK when a CUDA device of compute capability 10.x is current. */
 dyph_status dyph_device_check(void);
 /* Sticky device-side error word of the library (DYPH_ERR_TIMEOUT etc.), read
@@ -302,12 +305,28 @@ dyph_status dyph_world_step(dyph_world* w, int32_t n_frames, dyph_stream s);
  * scene's own contact indices, so in EVERY mode each scene evolves
  * bit-identically to stepping it alone in that mode (a scene without contacts
  * in a frame is not renormalised, as the reference's solve returns at once).
+ * When the largest scene also fits the fused frame (about 1,400 bodies), each
+ * frame is one kernel launch: every block integrates its scene, finds its
+ * candidate pairs by testing every body pair's fp16 leaf boxes (the same set
+ * the LBVH traversal returns), runs the narrowphase and the solve, all in
+ * shared memory; the BVH is then not built (dyph_broadphase_bvh_view is
+ * empty) and the pair / contact lists are compacted on request
+ * (dyph_world_sync_lists). Each scene keeps at most 48 n + 64 pairs and
+ * 16 n + 64 contacts (n its body count), its capacities when stepped alone.
  * The largest scene's bodies must fit one block's shared memory (about 1,900
  * bodies); otherwise the whole batch is solved as one contact set, which is
  * exact per scene only in DYPH_SOLVER_SEQUENTIAL. Allocates; drops captured
  * graphs. */
 dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset,
                                   const dyph_aabb* scene_bounds);
+/* Batched worlds whose frame runs fused (one kernel launch per frame, one
+ * thread block per scene: integrate, pair search, narrowphase and solve in
+ * shared memory, see dyph_world_set_scenes) keep each scene's pairs and
+ * contacts in per-scene slots. This call compacts the last frame's lists, in
+ * the order the per-frame stages produce them, into the broadphase's pair
+ * list, the narrowphase's ContactView and the solver's colours (queued on s;
+ * no-op for other worlds). Call it before reading those lists. */
+dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
 /* Blocking: FNV-1a-64 of every scene's pose arrays (one value for a single
  * scene); cap >= number of scenes. */
 dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uint64_t* host_out, uint32_t cap);

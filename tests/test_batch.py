@@ -135,3 +135,33 @@ def test_batched_dense_scene_spills_contact_words(dev, oracle_mod):
             o = oracle_mod.World(s.scene(i))
             assert o.step(10, mode) == 0
             assert o.hash() == int(hb[i]), (mode, i)
+
+
+def test_batched_lists_match_oracle_per_scene(dev, oracle_mod):
+    """The fused frame's compacted lists (dyph_world_sync_lists): pairs,
+    contact rows and JP colours of every scene equal the oracle's for the
+    scene stepped alone, in scene order."""
+    s = scenes.batch(24, 8, 200, seed=13)
+    w = dev.World(s, mode=0)
+    w.step(60)
+    pairs = w.pairs()
+    ab, p7 = w.contacts()
+    cols, _ = w.colors(len(ab))
+    po = pc = 0
+    n_colored = 0
+    for i in range(s.n_scenes):
+        o = oracle_mod.World(s.scene(i))
+        assert o.step(60, 0) == 0
+        off = np.uint32(s.body_offset[i])
+        op, _ = o.pairs()
+        assert np.array_equal(pairs[po:po + len(op)], op + off), i
+        po += len(op)
+        oab, op7 = o.contacts()
+        assert np.array_equal(ab[pc:pc + len(oab)], oab + off), i
+        assert np.array_equal(p7[pc:pc + len(oab)].view(np.uint32), op7.view(np.uint32)), i
+        oc = o.colors()
+        assert np.array_equal(cols[pc:pc + len(oab)], oc), i
+        n_colored += int(not np.all(oc == 0xFFFFFFFF))
+        pc += len(oab)
+    assert po == len(pairs) and pc == len(ab)
+    assert n_colored > 0, "no scene took the coloured order"
