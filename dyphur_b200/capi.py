@@ -102,6 +102,8 @@ _PROTOS = {
     "dyph_world_download_history": (_st, [_vp, _vp, _vp, _vp, C.c_uint32, _up]),
     "dyph_world_set_trajectory": (_st, [_vp, _vp, C.c_uint32, C.c_uint32]),
     "dyph_world_sync_lists": (_st, [_vp, _vp]),
+    "dyph_world_set_phase_timing": (_st, [_vp, C.c_int]),
+    "dyph_world_download_phase_ns": (_st, [_vp, _vp, _vp, C.c_uint32]),
     "dyph_event_create": (_st, [C.POINTER(_vp)]),
     "dyph_event_destroy": (None, [_vp]),
     "dyph_event_record": (_st, [_vp, _vp]),

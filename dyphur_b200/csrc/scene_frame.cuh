@@ -61,175 +61,238 @@ struct SceneBodiesShaped : SceneBodies {
     __device__ __forceinline__ uint32_t shape(uint32_t i) const { return i; }
 };
 
-__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_kernel(
-    dyph_bodies gb, dyph_shapes gs, SceneBufs S, FrameBufs F, float gx, float gy, float gz, float sub_dt,
-    float half_dt, int n_substeps, int mode, int n_iters, float mu, float dt, uint32_t* __restrict__ meta,
-    uint32_t* __restrict__ bp_counts, uint32_t* __restrict__ np_counts, uint32_t* __restrict__ status) {
+// Per-frame parameters of the fused kernel.
+struct FrameParams {
+    dyph_bodies gb;
+    dyph_shapes gs;
+    float gx, gy, gz, sub_dt, half_dt, mu, dt;
+    int n_substeps, mode, n_iters;
+    uint32_t* meta;
+    uint32_t* bp_counts;
+    uint32_t* np_counts;
+    uint32_t* status;
+    unsigned long long* phase_ns;  // null, or [kFramePhases] device-clock ns summed over scenes
+};
+
+// Phases of a scene's fused frame, timed per scene by its team leader when
+// phase_ns is set: 0 staging + integrate + leaf boxes, 1 pair search,
+// 2 narrowphase, 3 contact solve, 4 write-back.
+constexpr int kFramePhases = 5;
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <class Team>
+__device__ __forceinline__ void phase_mark(const Team& T, const FrameParams& P_, int k, uint64_t& t0) {
+    if (P_.phase_ns && T.leader()) {
+        const uint64_t t = global_ns();
+        atomicAdd(&P_.phase_ns[k], static_cast<unsigned long long>(t - t0));
+        t0 = t;
+    }
+}
+
+// One frame of scene s by team T with `smem_bytes` of shared memory at smem.
+// Returns false after raising an error.
+template <class Team>
+__device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
+                            const SceneBufs& S, const FrameBufs& F, const FrameParams& P_) {
+    const GlobalBodies B{P_.gb};
+    const uint32_t lane = threadIdx.x & 31u;
+    uint64_t t0 = P_.phase_ns ? global_ns() : 0u;
+    const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
+    const uint32_t ldb = (nb + 3u) & ~3u;
+    float* fb = reinterpret_cast<float*>(smem);
+    const SceneSolverRows R = scene_solver_rows(fb, ldb);
+    uint32_t* info = R.cnt + ldb;
+    float* half = reinterpret_cast<float*>(info + ldb);
+    float* box = half + 3 * ldb;  // rows mnx, mny, mnz, mxx, mxy, mxz
+    const SceneBodiesShaped SB{{fb, ldb}};
+    const SceneShapes SS{info, half, ldb};
+    const uint32_t pcap = F.pair_base[s + 1] - F.pair_base[s];
+    const uint32_t ccap = F.contact_base[s + 1] - F.contact_base[s];
+    // ── stage and integrate ──
+    scene_load_bodies(T, B, b0, nb, fb, ldb);
+    for (uint32_t i = T.rank(); i < nb; i += T.size()) {
+        const uint32_t g = b0 + i, sh_i = P_.gb.shape[g];
+        info[i] = P_.gs.type[sh_i] | (P_.gb.flags[g] << 8);
+        half[i] = P_.gs.half_x[sh_i];
+        half[ldb + i] = P_.gs.half_y[sh_i];
+        half[2 * ldb + i] = P_.gs.half_z[sh_i];
+        if (SB.im(i) != 0.f && !((info[i] >> 8) & kFlagSleeping)) {
+            Pose p{SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i), SB.qy(i), SB.qz(i),
+                   SB.vx(i), SB.vy(i), SB.vz(i)};
+            const float ox = SB.wx(i), oy = SB.wy(i), oz = SB.wz(i);
+            for (int k = 0; k < P_.n_substeps; ++k)
+                integrate_body(p, ox, oy, oz, P_.gx, P_.gy, P_.gz, P_.sub_dt, P_.half_dt);
+            SB.px(i) = p.px; SB.py(i) = p.py; SB.pz(i) = p.pz;
+            SB.qw(i) = p.qw; SB.qx(i) = p.qx; SB.qy(i) = p.qy; SB.qz(i) = p.qz;
+            SB.vx(i) = p.vx; SB.vy(i) = p.vy; SB.vz(i) = p.vz;
+        }
+        // leaf box from the integrated pose, kept as the exact floats of its fp16 bounds
+        const BoxF bx = unpack_box(leaf_box(SS.type(i), SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i),
+                                            SB.qy(i), SB.qz(i), SS.hx(i), SS.hy(i), SS.hz(i)));
+        box[i] = bx.mnx; box[ldb + i] = bx.mny; box[2 * ldb + i] = bx.mnz;
+        box[3 * ldb + i] = bx.mxx; box[4 * ldb + i] = bx.mxy; box[5 * ldb + i] = bx.mxz;
+    }
+    T.sync();
+    phase_mark(T, P_, 0, t0);
+    // ── candidate pairs: per body a, the partners b > a in ascending order ──
+    for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
+        const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
+        uint32_t c = 0;
+        for (uint32_t j0 = a + 1; j0 < nb; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            bool ov = false;
+            if (j < nb) {
+                const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
+                             box[5 * ldb + j]};
+                ov = box_overlap(n, q);
+            }
+            c += __popc(__ballot_sync(0xffffffffu, ov));
+        }
+        if (lane == 0) R.cnt[a] = c;
+    }
+    if (T.leader()) sh.carry = 0u;
+    T.sync();
+    for (uint32_t base = 0; base < nb; base += T.size()) {
+        const uint32_t i = base + T.rank();
+        const uint32_t v = i < nb ? R.cnt[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = T.exclusive_scan(v, sh.scan, tot);
+        if (i < nb) R.off[i] = sh.carry + ex;
+        T.sync();
+        if (T.leader()) sh.carry += tot;
+        T.sync();
+    }
+    const uint32_t p_true = sh.carry;
+    const uint32_t P = min(p_true, pcap);
+    // ── layout of the pairs and the contact words: shared memory if they fit ──
+    const uint32_t cc = min(P, ccap);
+    const uint32_t ldc = (cc + 4u) & ~3u;  // >= cc + 1: group offsets take m + 1 words
+    const uint32_t pwords = (P + 3u) & ~3u;
+    const uint32_t body_bytes = frame_body_bytes(nb);
+    const bool in_smem = body_bytes + 4u * pwords + kSceneWords * 4u * ldc <= smem_bytes;
+    uint32_t* pairs = in_smem ? reinterpret_cast<uint32_t*>(smem + body_bytes) : F.pair_raw + F.pair_base[s];
+    const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(smem + body_bytes) + pwords
+                                   : F.words + F.contact_base[s] + s,
+                           in_smem ? ldc : F.words_stride};
+    for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
+        const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
+        uint32_t pos = R.off[a];
+        for (uint32_t j0 = a + 1; j0 < nb && pos < P; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            bool ov = false;
+            if (j < nb) {
+                const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
+                             box[5 * ldb + j]};
+                ov = box_overlap(n, q);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, ov);
+            const uint32_t at = pos + __popc(bal & ((1u << lane) - 1u));
+            if (ov && at < P) pairs[at] = a | (j << 16);
+            pos += __popc(bal);
+        }
+    }
+    T.sync();
+    if (in_smem)
+        for (uint32_t p = T.rank(); p < P; p += T.size()) F.pair_raw[F.pair_base[s] + p] = pairs[p];
+    phase_mark(T, P_, 1, t0);
+    // ── narrowphase: contacts in pair order ──
+    for (uint32_t i = T.rank(); i < nb; i += T.size()) R.cnt[i] = 0u;
+    if (T.leader()) sh.carry = 0u;
+    T.sync();
+    const uint32_t cbase = F.contact_base[s];
+    for (uint32_t base = 0; base < P; base += T.size()) {
+        const uint32_t p = base + T.rank();
+        Contact c{};
+        bool hit = false;
+        if (p < P) {
+            const uint32_t ab = pairs[p];
+            hit = process_pair(SB, SS, ab & 0xFFFFu, ab >> 16, c);
+        }
+        uint32_t tot;
+        const uint32_t ex = T.exclusive_scan(hit ? 1u : 0u, sh.scan, tot);
+        const uint32_t k = sh.carry + ex;
+        if (hit && k < cc) {
+            SC.ab(k) = c.a | (c.b << 16);
+            SC.lam(k) = 0.f;
+            SC.pb(k) = kSceneNone;
+            SC.g(0, k) = c.px; SC.g(1, k) = c.py; SC.g(2, k) = c.pz;
+            SC.g(3, k) = c.nx; SC.g(4, k) = c.ny; SC.g(5, k) = c.nz;
+            SC.g(6, k) = c.depth;
+            if (SB.im(c.b) != 0.f) atomicAdd(&R.cnt[c.b], 1u);
+            const uint32_t slot = cbase + k, st = F.contact_slots;
+            F.contact_raw[slot] = b0 + c.a;
+            F.contact_raw[st + slot] = b0 + c.b;
+            F.contact_raw[2 * st + slot] = __float_as_uint(c.px);
+            F.contact_raw[3 * st + slot] = __float_as_uint(c.py);
+            F.contact_raw[4 * st + slot] = __float_as_uint(c.pz);
+            F.contact_raw[5 * st + slot] = __float_as_uint(c.nx);
+            F.contact_raw[6 * st + slot] = __float_as_uint(c.ny);
+            F.contact_raw[7 * st + slot] = __float_as_uint(c.nz);
+            F.contact_raw[8 * st + slot] = __float_as_uint(c.depth);
+        }
+        T.sync();
+        if (T.leader()) sh.carry += tot;
+        T.sync();
+    }
+    const uint32_t m_true = sh.carry, m = min(m_true, cc);
+    T.sync();  // every thread has read the count before scene_solve reuses sh.carry
+    if (T.leader()) {
+        F.counts[4 * s + 0] = P;
+        F.counts[4 * s + 1] = p_true;
+        F.counts[4 * s + 2] = m;
+        F.counts[4 * s + 3] = m_true;
+        atomicAdd(&P_.bp_counts[0], P);
+        atomicAdd(&P_.bp_counts[1], p_true);
+        atomicAdd(&P_.np_counts[0], m);
+        atomicAdd(&P_.np_counts[1], m_true);
+        // a scene past its own capacity keeps its ordered prefix, as it does alone
+        if (p_true > pcap) atomicCAS(P_.status, 0u, static_cast<uint32_t>(DYPH_ERR_PAIR_OVERFLOW));
+        if (m_true > ccap) atomicCAS(P_.status, 0u, static_cast<uint32_t>(DYPH_ERR_CONTACT_OVERFLOW));
+    }
+    phase_mark(T, P_, 2, t0);
+    // ── contact solve (none without contacts, as the reference's solve returns) ──
+    bool colored = false;
+    uint32_t n_colors = 0, rounds = 0;
+    if (m > 0) {
+        if (!scene_solve(T, nb, m, SB, R, SC, P_.mode, P_.n_iters, P_.mu, P_.dt, sh, colored, n_colors, rounds))
+            return false;
+        for (uint32_t k = T.rank(); k < m; k += T.size())
+            F.color_raw[cbase + k] = colored ? SC.done(k) : kUncolored;
+        scene_stats(T, P_.meta, colored, n_colors, rounds);
+    }
+    phase_mark(T, P_, 3, t0);
+    scene_store_bodies(T, B, b0, nb, SB);
+    T.sync();
+    phase_mark(T, P_, 4, t0);
+    return true;
+}
+
+// Work item i: items[4 i] a large scene solved by the whole block when
+// items[4 i + 1] == kItemBlock; otherwise up to four small scenes, one per
+// warp (kItemEmpty marks an unused warp), each with a quarter of the block's
+// shared memory.
+constexpr uint32_t kItemEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kItemBlock = 0xFFFFFFFEu;
+
+__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_kernel(SceneBufs S, FrameBufs F, FrameParams P_,
+                                                                       const uint32_t* __restrict__ items,
+                                                                       uint32_t n_items) {
     extern __shared__ __align__(16) unsigned char scene_smem[];
-    __shared__ SceneShared sh;
-    const GlobalBodies B{gb};
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
-    for (uint32_t t = blockIdx.x; t < S.n_scenes; t += gridDim.x) {
-        const uint32_t s = S.order[t];
-        const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
-        const uint32_t ldb = (nb + 3u) & ~3u;
-        float* fb = reinterpret_cast<float*>(scene_smem);
-        const SceneSolverRows R = scene_solver_rows(fb, ldb);
-        uint32_t* info = R.cnt + ldb;
-        float* half = reinterpret_cast<float*>(info + ldb);
-        float* box = half + 3 * ldb;  // rows mnx, mny, mnz, mxx, mxy, mxz
-        const SceneBodiesShaped SB{{fb, ldb}};
-        const SceneShapes SS{info, half, ldb};
-        const uint32_t pcap = F.pair_base[s + 1] - F.pair_base[s];
-        const uint32_t ccap = F.contact_base[s + 1] - F.contact_base[s];
-        // ── stage and integrate ──
-        scene_load_bodies(B, b0, nb, fb, ldb);
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-            const uint32_t g = b0 + i, sh_i = gb.shape[g];
-            info[i] = gs.type[sh_i] | (gb.flags[g] << 8);
-            half[i] = gs.half_x[sh_i];
-            half[ldb + i] = gs.half_y[sh_i];
-            half[2 * ldb + i] = gs.half_z[sh_i];
-            if (SB.im(i) != 0.f && !((info[i] >> 8) & kFlagSleeping)) {
-                Pose p{SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i), SB.qy(i), SB.qz(i),
-                       SB.vx(i), SB.vy(i), SB.vz(i)};
-                const float ox = SB.wx(i), oy = SB.wy(i), oz = SB.wz(i);
-                for (int k = 0; k < n_substeps; ++k) integrate_body(p, ox, oy, oz, gx, gy, gz, sub_dt, half_dt);
-                SB.px(i) = p.px; SB.py(i) = p.py; SB.pz(i) = p.pz;
-                SB.qw(i) = p.qw; SB.qx(i) = p.qx; SB.qy(i) = p.qy; SB.qz(i) = p.qz;
-                SB.vx(i) = p.vx; SB.vy(i) = p.vy; SB.vz(i) = p.vz;
-            }
-            // leaf box from the integrated pose, kept as the exact floats of its fp16 bounds
-            const BoxF bx = unpack_box(leaf_box(SS.type(i), SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i),
-                                                SB.qy(i), SB.qz(i), SS.hx(i), SS.hy(i), SS.hz(i)));
-            box[i] = bx.mnx; box[ldb + i] = bx.mny; box[2 * ldb + i] = bx.mnz;
-            box[3 * ldb + i] = bx.mxx; box[4 * ldb + i] = bx.mxy; box[5 * ldb + i] = bx.mxz;
+    __shared__ SceneShared sh[kSceneThreads / 32];
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t share = (S.smem_bytes / 4u) & ~15u;
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+        if (items[4 * it + 1] == kItemBlock) {
+            frame_scene(BlockTeam{}, items[4 * it], scene_smem, S.smem_bytes, sh[0], S, F, P_);
+        } else {
+            const uint32_t s = items[4 * it + warp];
+            if (s != kItemEmpty) frame_scene(WarpTeam{}, s, scene_smem + warp * share, share, sh[warp], S, F, P_);
         }
-        __syncthreads();
-        // ── candidate pairs: per body a, the partners b > a in ascending order ──
-        for (uint32_t a = warp; a < nb; a += n_warps) {
-            const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
-            uint32_t c = 0;
-            for (uint32_t j0 = a + 1; j0 < nb; j0 += 32u) {
-                const uint32_t j = j0 + lane;
-                bool ov = false;
-                if (j < nb) {
-                    const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
-                                 box[5 * ldb + j]};
-                    ov = box_overlap(n, q);
-                }
-                c += __popc(__ballot_sync(0xffffffffu, ov));
-            }
-            if (lane == 0) R.cnt[a] = c;
-        }
-        if (threadIdx.x == 0) sh.carry = 0u;
-        __syncthreads();
-        for (uint32_t base = 0; base < nb; base += blockDim.x) {
-            const uint32_t i = base + threadIdx.x;
-            const uint32_t v = i < nb ? R.cnt[i] : 0u;
-            uint32_t tot;
-            const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, sh.scan, tot);
-            if (i < nb) R.off[i] = sh.carry + ex;
-            __syncthreads();
-            if (threadIdx.x == 0) sh.carry += tot;
-            __syncthreads();
-        }
-        const uint32_t p_true = sh.carry;
-        const uint32_t P = min(p_true, pcap);
-        // ── layout of the pairs and the contact words: shared memory if they fit ──
-        const uint32_t cc = min(P, ccap);
-        const uint32_t ldc = (cc + 4u) & ~3u;  // >= cc + 1: group offsets take m + 1 words
-        const uint32_t pwords = (P + 3u) & ~3u;
-        const uint32_t body_bytes = frame_body_bytes(nb);
-        const bool in_smem = body_bytes + 4u * pwords + kSceneWords * 4u * ldc <= S.smem_bytes;
-        uint32_t* pairs = in_smem ? reinterpret_cast<uint32_t*>(scene_smem + body_bytes) : F.pair_raw + F.pair_base[s];
-        const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(scene_smem + body_bytes) + pwords
-                                       : F.words + F.contact_base[s] + s,
-                               in_smem ? ldc : F.words_stride};
-        for (uint32_t a = warp; a < nb; a += n_warps) {
-            const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
-            uint32_t pos = R.off[a];
-            for (uint32_t j0 = a + 1; j0 < nb && pos < P; j0 += 32u) {
-                const uint32_t j = j0 + lane;
-                bool ov = false;
-                if (j < nb) {
-                    const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
-                                 box[5 * ldb + j]};
-                    ov = box_overlap(n, q);
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, ov);
-                const uint32_t at = pos + __popc(bal & ((1u << lane) - 1u));
-                if (ov && at < P) pairs[at] = a | (j << 16);
-                pos += __popc(bal);
-            }
-        }
-        __syncthreads();
-        if (in_smem)
-            for (uint32_t p = threadIdx.x; p < P; p += blockDim.x) F.pair_raw[F.pair_base[s] + p] = pairs[p];
-        // ── narrowphase: contacts in pair order ──
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.cnt[i] = 0u;
-        if (threadIdx.x == 0) sh.carry = 0u;
-        __syncthreads();
-        const uint32_t cbase = F.contact_base[s];
-        for (uint32_t base = 0; base < P; base += blockDim.x) {
-            const uint32_t p = base + threadIdx.x;
-            Contact c{};
-            bool hit = false;
-            if (p < P) {
-                const uint32_t ab = pairs[p];
-                hit = process_pair(SB, SS, ab & 0xFFFFu, ab >> 16, c);
-            }
-            uint32_t tot;
-            const uint32_t ex = block_exclusive_scan<kSceneThreads>(hit ? 1u : 0u, sh.scan, tot);
-            const uint32_t k = sh.carry + ex;
-            if (hit && k < cc) {
-                SC.ab(k) = c.a | (c.b << 16);
-                SC.lam(k) = 0.f;
-                SC.pb(k) = kSceneNone;
-                SC.g(0, k) = c.px; SC.g(1, k) = c.py; SC.g(2, k) = c.pz;
-                SC.g(3, k) = c.nx; SC.g(4, k) = c.ny; SC.g(5, k) = c.nz;
-                SC.g(6, k) = c.depth;
-                if (SB.im(c.b) != 0.f) atomicAdd(&R.cnt[c.b], 1u);
-                const uint32_t slot = cbase + k, st = F.contact_slots;
-                F.contact_raw[slot] = b0 + c.a;
-                F.contact_raw[st + slot] = b0 + c.b;
-                F.contact_raw[2 * st + slot] = __float_as_uint(c.px);
-                F.contact_raw[3 * st + slot] = __float_as_uint(c.py);
-                F.contact_raw[4 * st + slot] = __float_as_uint(c.pz);
-                F.contact_raw[5 * st + slot] = __float_as_uint(c.nx);
-                F.contact_raw[6 * st + slot] = __float_as_uint(c.ny);
-                F.contact_raw[7 * st + slot] = __float_as_uint(c.nz);
-                F.contact_raw[8 * st + slot] = __float_as_uint(c.depth);
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) sh.carry += tot;
-            __syncthreads();
-        }
-        const uint32_t m_true = sh.carry, m = min(m_true, cc);
-        __syncthreads();  // every thread has read the count before scene_solve reuses sh.carry
-        if (threadIdx.x == 0) {
-            F.counts[4 * s + 0] = P;
-            F.counts[4 * s + 1] = p_true;
-            F.counts[4 * s + 2] = m;
-            F.counts[4 * s + 3] = m_true;
-            atomicAdd(&bp_counts[0], P);
-            atomicAdd(&bp_counts[1], p_true);
-            atomicAdd(&np_counts[0], m);
-            atomicAdd(&np_counts[1], m_true);
-            // a scene past its own capacity keeps its ordered prefix, as it does alone
-            if (p_true > pcap) atomicCAS(status, 0u, static_cast<uint32_t>(DYPH_ERR_PAIR_OVERFLOW));
-            if (m_true > ccap) atomicCAS(status, 0u, static_cast<uint32_t>(DYPH_ERR_CONTACT_OVERFLOW));
-        }
-        // ── contact solve (none without contacts, as the reference's solve returns) ──
-        bool colored = false;
-        uint32_t n_colors = 0, rounds = 0;
-        if (m > 0) {
-            if (!scene_solve(nb, m, SB, R, SC, mode, n_iters, mu, dt, sh, colored, n_colors, rounds)) return;
-            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x)
-                F.color_raw[cbase + k] = colored ? SC.done(k) : kUncolored;
-            scene_stats(meta, colored, n_colors, rounds);
-        }
-        scene_store_bodies(B, b0, nb, SB);
         __syncthreads();
     }
 }

@@ -113,6 +113,42 @@ struct SceneContacts {
     }
 };
 
+// A team of threads that runs one scene: the whole block (big scenes) or one
+// warp (small scenes, several to a block).
+struct BlockTeam {
+    __device__ __forceinline__ uint32_t rank() const { return threadIdx.x; }
+    __device__ __forceinline__ uint32_t size() const { return kSceneThreads; }
+    __device__ __forceinline__ uint32_t warp() const { return threadIdx.x >> 5; }
+    __device__ __forceinline__ uint32_t warps() const { return kSceneThreads / 32; }
+    __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ bool any(bool p) const { return __syncthreads_or(p) != 0; }
+    __device__ __forceinline__ uint32_t exclusive_scan(uint32_t v, uint32_t* scratch, uint32_t& total) const {
+        return block_exclusive_scan<kSceneThreads>(v, scratch, total);
+    }
+};
+
+struct WarpTeam {
+    __device__ __forceinline__ uint32_t rank() const { return threadIdx.x & 31u; }
+    __device__ __forceinline__ uint32_t size() const { return 32u; }
+    __device__ __forceinline__ uint32_t warp() const { return 0u; }
+    __device__ __forceinline__ uint32_t warps() const { return 1u; }
+    __device__ __forceinline__ bool leader() const { return (threadIdx.x & 31u) == 0u; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ bool any(bool p) const { return __any_sync(0xffffffffu, p) != 0; }
+    __device__ __forceinline__ uint32_t exclusive_scan(uint32_t v, uint32_t*, uint32_t& total) const {
+        const uint32_t lane = threadIdx.x & 31u;
+        uint32_t x = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= static_cast<uint32_t>(d)) x += y;
+        }
+        total = __shfl_sync(0xffffffffu, x, 31);
+        return x - v;
+    }
+};
+
 // Levels of the sequential order on one scene: level(k) = 1 + the larger
 // level of k's predecessors on its two dynamic bodies. Contacts of one level
 // share no dynamic body, and solving the levels in ascending order gives
@@ -120,16 +156,17 @@ struct SceneContacts {
 // bit. Levels go to SC.done (1-based); returns the level count, or 0 if the
 // predecessor links were inconsistent (they cannot be: every predecessor has a
 // lower index).
-__device__ uint32_t scene_levels(uint32_t m, const SceneContacts& SC, uint32_t* s_max) {
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.done(k) = 0u;
-    if (threadIdx.x == 0) *s_max = 0u;
-    __syncthreads();
+template <class Team>
+__device__ uint32_t scene_levels(const Team& T, uint32_t m, const SceneContacts& SC, uint32_t* s_max) {
+    for (uint32_t k = T.rank(); k < m; k += T.size()) SC.done(k) = 0u;
+    if (T.leader()) *s_max = 0u;
+    T.sync();
     uint32_t my_max = 0;
     for (uint32_t pass = 0;; ++pass) {
         int pending = 0;
         // A level, once written, is final, so a pass may use levels written
         // by other threads during the same pass.
-        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
             if (SC.done(k) != 0u) continue;
             const uint32_t pa = SC.pa(k), pb = SC.pb(k);
             const uint32_t la = pa == kSceneNone ? 0u : SC.done(pa);
@@ -142,57 +179,59 @@ __device__ uint32_t scene_levels(uint32_t m, const SceneContacts& SC, uint32_t* 
             SC.done(k) = l;
             my_max = max(my_max, l);
         }
-        if (!__syncthreads_or(pending)) break;
+        if (!T.any(pending)) break;
         if (pass > m) return 0u;
     }
     atomicMax(s_max, my_max);
-    __syncthreads();
+    T.sync();
     const uint32_t levels = *s_max;
-    __syncthreads();
+    T.sync();
     return levels;
 }
 
 // Counting sort of the scene's contacts by group done(k) - base (a level or a
 // colour) into SC.ent; group g is SC.ent[SC.pa(g), SC.pa(g + 1)). The
 // predecessor rows are free once the groups are known.
-__device__ void scene_group(uint32_t m, uint32_t groups, uint32_t base, const SceneContacts& SC, uint32_t* s_scan,
-                            uint32_t* s_carry) {
-    for (uint32_t g = threadIdx.x; g <= groups; g += blockDim.x) SC.pa(g) = 0u;
-    if (threadIdx.x == 0) *s_carry = 0u;
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) atomicAdd(&SC.pa(SC.done(k) - base), 1u);
-    __syncthreads();
-    for (uint32_t g0 = 0; g0 <= groups; g0 += blockDim.x) {
-        const uint32_t g = g0 + threadIdx.x;
+template <class Team>
+__device__ void scene_group(const Team& T, uint32_t m, uint32_t groups, uint32_t base, const SceneContacts& SC,
+                            uint32_t* s_scan, uint32_t* s_carry) {
+    for (uint32_t g = T.rank(); g <= groups; g += T.size()) SC.pa(g) = 0u;
+    if (T.leader()) *s_carry = 0u;
+    T.sync();
+    for (uint32_t k = T.rank(); k < m; k += T.size()) atomicAdd(&SC.pa(SC.done(k) - base), 1u);
+    T.sync();
+    for (uint32_t g0 = 0; g0 <= groups; g0 += T.size()) {
+        const uint32_t g = g0 + T.rank();
         const uint32_t v = g <= groups ? SC.pa(g) : 0u;
         uint32_t tot;
-        const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, s_scan, tot);
+        const uint32_t ex = T.exclusive_scan(v, s_scan, tot);
         if (g <= groups) {
             SC.pa(g) = *s_carry + ex;
             SC.pb(g) = *s_carry + ex;  // fill cursor
         }
-        __syncthreads();
-        if (threadIdx.x == 0) *s_carry += tot;
-        __syncthreads();
+        T.sync();
+        if (T.leader()) *s_carry += tot;
+        T.sync();
     }
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.ent(atomicAdd(&SC.pb(SC.done(k) - base), 1u)) = k;
-    __syncthreads();
+    for (uint32_t k = T.rank(); k < m; k += T.size()) SC.ent(atomicAdd(&SC.pb(SC.done(k) - base), 1u)) = k;
+    T.sync();
 }
 
 // One sweep over the groups in ascending order, one contact per thread at a
 // time inside a group (no two of a group share a dynamic body).
-__device__ void scene_sweep(uint32_t groups, const SceneBodies& SB, const SceneContacts& SC, float mu, float dt,
-                            int* s_flag) {
+template <class Team>
+__device__ void scene_sweep(const Team& T, uint32_t groups, const SceneBodies& SB, const SceneContacts& SC, float mu,
+                            float dt, int* s_flag) {
     for (uint32_t g = 0; g < groups; ++g) {
         const uint32_t end = SC.pa(g + 1);
-        for (uint32_t i = SC.pa(g) + threadIdx.x; i < end; i += blockDim.x) {
+        for (uint32_t i = SC.pa(g) + T.rank(); i < end; i += T.size()) {
             const uint32_t k = SC.ent(i);
             const Contact ct = SC.contact(k);
             float lc = SC.lam(k);
             if (solve_contact(SB, ct, mu, lc, dt) == kSolveDeferred) *s_flag = 1;
             SC.lam(k) = lc;
         }
-        __syncthreads();
+        T.sync();
     }
 }
 
@@ -220,10 +259,11 @@ __device__ __forceinline__ SceneSolverRows scene_solver_rows(float* fb, uint32_t
     return R;
 }
 
-__device__ __forceinline__ void scene_load_bodies(const GlobalBodies& B, uint32_t b0, uint32_t nb, float* fb,
-                                                  uint32_t ldb) {
+template <class Team>
+__device__ __forceinline__ void scene_load_bodies(const Team& T, const GlobalBodies& B, uint32_t b0, uint32_t nb,
+                                                  float* fb, uint32_t ldb) {
     const SceneBodies SB{fb, ldb};
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+    for (uint32_t i = T.rank(); i < nb; i += T.size()) {
         const uint32_t g = b0 + i;
         SB.px(i) = B.px(g); SB.py(i) = B.py(g); SB.pz(i) = B.pz(g);
         SB.qw(i) = B.qw(g); SB.qx(i) = B.qx(g); SB.qy(i) = B.qy(g); SB.qz(i) = B.qz(g);
@@ -235,9 +275,10 @@ __device__ __forceinline__ void scene_load_bodies(const GlobalBodies& B, uint32_
     }
 }
 
-__device__ __forceinline__ void scene_store_bodies(const GlobalBodies& B, uint32_t b0, uint32_t nb,
+template <class Team>
+__device__ __forceinline__ void scene_store_bodies(const Team& T, const GlobalBodies& B, uint32_t b0, uint32_t nb,
                                                    const SceneBodies& SB) {
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+    for (uint32_t i = T.rank(); i < nb; i += T.size()) {
         const uint32_t g = b0 + i;
         B.px(g) = SB.px(i); B.py(g) = SB.py(i); B.pz(g) = SB.pz(i);
         B.qw(g) = SB.qw(i); B.qx(g) = SB.qx(i); B.qy(g) = SB.qy(i); B.qz(g) = SB.qz(i);
@@ -250,36 +291,37 @@ __device__ __forceinline__ void scene_store_bodies(const GlobalBodies& B, uint32
 // lambda = 0, geometry; pb = none) with R.cnt[b] = the b-side contact count of
 // every dynamic body b. Leaves the bodies solved and renormalised in SB and
 // the colours (or UINT32_MAX) in SC.done. Returns false after raising an error.
-__device__ bool scene_solve(uint32_t nb, uint32_t m, const SceneBodies& SB, const SceneSolverRows& R,
+template <class Team>
+__device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneBodies& SB, const SceneSolverRows& R,
                             const SceneContacts& SC, int mode, int n_iters, float mu, float dt, SceneShared& sh,
                             bool& colored_out, uint32_t& n_colors_out, uint32_t& rounds_out) {
     // ── predecessors in contact order: b-side lists (scan, fill, sort) ──
-    if (threadIdx.x == 0) {
+    if (T.leader()) {
         sh.carry = 0u;
         sh.flag = 0;
     }
-    __syncthreads();
-    for (uint32_t base = 0; base < nb; base += blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
+    T.sync();
+    for (uint32_t base = 0; base < nb; base += T.size()) {
+        const uint32_t i = base + T.rank();
         const uint32_t v = i < nb ? R.cnt[i] : 0u;
         uint32_t tot;
-        const uint32_t ex = block_exclusive_scan<kSceneThreads>(v, sh.scan, tot);
+        const uint32_t ex = T.exclusive_scan(v, sh.scan, tot);
         if (i < nb) {
             R.off[i] = sh.carry + ex;
             R.cnt[i] = 0u;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) sh.carry += tot;
-        __syncthreads();
+        T.sync();
+        if (T.leader()) sh.carry += tot;
+        T.sync();
     }
-    if (threadIdx.x == 0) R.off[nb] = sh.carry;
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+    if (T.leader()) R.off[nb] = sh.carry;
+    T.sync();
+    for (uint32_t k = T.rank(); k < m; k += T.size()) {
         const uint32_t b = SC.ab(k) >> 16;
         if (SB.im(b) != 0.f) SC.ent(R.off[b] + atomicAdd(&R.cnt[b], 1u)) = k;
     }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < nb; x += blockDim.x) {
+    T.sync();
+    for (uint32_t x = T.rank(); x < nb; x += T.size()) {
         const uint32_t lo = R.off[x], hi = R.off[x + 1];
         for (uint32_t i = lo + 1; i < hi; ++i) {
             const uint32_t v = SC.ent(i);
@@ -293,8 +335,8 @@ __device__ bool scene_solve(uint32_t nb, uint32_t m, const SceneBodies& SB, cons
         for (uint32_t i = lo + 1; i < hi; ++i) SC.pb(SC.ent(i)) = SC.ent(i - 1);
         R.cnt[x] = hi > lo ? SC.ent(hi - 1) : kSceneNone;  // last b-side contact of x
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+    T.sync();
+    for (uint32_t k = T.rank(); k < m; k += T.size()) {
         const uint32_t a = SC.ab(k) & 0xFFFFu;
         uint32_t p = kSceneNone;
         if (SB.im(a) != 0.f) p = (k > 0 && (SC.ab(k - 1) & 0xFFFFu) == a) ? k - 1 : R.cnt[a];
@@ -305,26 +347,26 @@ __device__ bool scene_solve(uint32_t nb, uint32_t m, const SceneBodies& SB, cons
                    ((mode == DYPH_SOLVER_REFERENCE || mode == DYPH_SOLVER_REFERENCE_ROUNDS) && m > kSerialThreshold);
     uint32_t n_colors = 0, rounds = 0;
     if (colored) {
-        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) SC.done(k) = kUncolored;
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.mask[i] = 0ull;
-        if (threadIdx.x == 0) {
+        for (uint32_t k = T.rank(); k < m; k += T.size()) SC.done(k) = kUncolored;
+        for (uint32_t i = T.rank(); i < nb; i += T.size()) R.mask[i] = 0ull;
+        if (T.leader()) {
             sh.rem = m;
             sh.over = 0u;
             sh.maxcol = 0u;
         }
-        __syncthreads();
+        T.sync();
         while (sh.rem > 0u && rounds < kMaxRounds) {
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.pri[i] = 0ull;
-            __syncthreads();
-            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            for (uint32_t i = T.rank(); i < nb; i += T.size()) R.pri[i] = 0ull;
+            T.sync();
+            for (uint32_t k = T.rank(); k < m; k += T.size()) {
                 if (SC.done(k) != kUncolored) continue;
                 const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
                 const unsigned long long pk = (static_cast<unsigned long long>(hash_u32(k)) << 32) | k;
                 if (SB.im(a) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&R.pri[a]), pk);
                 if (SB.im(b) != 0.f) atomicMax(reinterpret_cast<unsigned long long*>(&R.pri[b]), pk);
             }
-            __syncthreads();
-            for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            T.sync();
+            for (uint32_t k = T.rank(); k < m; k += T.size()) {
                 if (SC.done(k) != kUncolored) continue;
                 const uint32_t a = SC.ab(k) & 0xFFFFu, b = SC.ab(k) >> 16;
                 const bool da = SB.im(a) != 0.f, db = SB.im(b) != 0.f;
@@ -343,38 +385,38 @@ __device__ bool scene_solve(uint32_t nb, uint32_t m, const SceneBodies& SB, cons
                 atomicMax(&sh.maxcol, col);
                 atomicSub(&sh.rem, 1u);
             }
-            __syncthreads();
+            T.sync();
             ++rounds;
         }
         colored = sh.rem == 0u && sh.over == 0u;
         n_colors = sh.maxcol + 1u;
-        __syncthreads();
+        T.sync();
     }
     // ── groups: colours, or the levels of the sequential order ──
     uint32_t groups = n_colors, base = 0u;
     if (!colored) {
-        groups = scene_levels(m, SC, &sh.maxcol);
+        groups = scene_levels(T, m, SC, &sh.maxcol);
         base = 1u;
         if (groups == 0u) {
-            if (threadIdx.x == 0) raise_error(DYPH_ERR_TIMEOUT, 11u);
+            if (T.leader()) raise_error(DYPH_ERR_TIMEOUT, 11u);
             return false;
         }
     }
-    scene_group(m, groups, base, SC, sh.scan, &sh.carry);
+    scene_group(T, m, groups, base, SC, sh.scan, &sh.carry);
     // ── sweeps and renormalisation ──
     bool deferred = false;
     for (int iter = 0; iter < n_iters; ++iter) {
         if (iter == 0 || deferred) {
-            scene_sweep(groups, SB, SC, mu, dt, &sh.flag);
+            scene_sweep(T, groups, SB, SC, mu, dt, &sh.flag);
             deferred = sh.flag != 0;
         }
         const int times = deferred ? 1 : n_iters - iter;
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        for (uint32_t i = T.rank(); i < nb; i += T.size()) {
             float qw = SB.qw(i), qx = SB.qx(i), qy = SB.qy(i), qz = SB.qz(i);
             for (int t = 0; t < times; ++t) renormalize(qw, qx, qy, qz);
             SB.qw(i) = qw; SB.qx(i) = qx; SB.qy(i) = qy; SB.qz(i) = qz;
         }
-        __syncthreads();
+        T.sync();
         if (!deferred) break;
     }
     colored_out = colored;
@@ -383,8 +425,10 @@ __device__ bool scene_solve(uint32_t nb, uint32_t m, const SceneBodies& SB, cons
     return true;
 }
 
-__device__ __forceinline__ void scene_stats(uint32_t* meta, bool colored, uint32_t n_colors, uint32_t rounds) {
-    if (threadIdx.x == 0) {
+template <class Team>
+__device__ __forceinline__ void scene_stats(const Team& T, uint32_t* meta, bool colored, uint32_t n_colors,
+                                            uint32_t rounds) {
+    if (T.leader()) {
         if (colored) {
             atomicMax(&meta[kMetaMaxColor], n_colors - 1u);
             meta[kMetaSceneColored] = 1u;
@@ -402,6 +446,7 @@ __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_cont
     extern __shared__ __align__(16) unsigned char scene_smem[];
     __shared__ SceneShared sh;
     const GlobalBodies B{gb};
+    const BlockTeam T;
     for (uint32_t t = blockIdx.x; t < S.n_scenes; t += gridDim.x) {
         const uint32_t s = S.order[t];
         const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
@@ -419,7 +464,7 @@ __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_cont
         const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(scene_smem + body_bytes) : S.scratch + k0 + s,
                                in_smem ? ldc : S.scratch_stride};
         // ── stage the scene's bodies and contacts ──
-        scene_load_bodies(B, b0, nb, fb, ldb);
+        scene_load_bodies(T, B, b0, nb, fb, ldb);
         for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) R.cnt[i] = 0u;
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
@@ -436,11 +481,11 @@ __global__ void __launch_bounds__(kSceneThreads, 4) scene_solve_kernel(dyph_cont
         __syncthreads();
         bool colored = false;
         uint32_t n_colors = 0, rounds = 0;
-        if (!scene_solve(nb, m, SB, R, SC, mode, n_iters, mu, dt, sh, colored, n_colors, rounds)) return;
+        if (!scene_solve(T, nb, m, SB, R, SC, mode, n_iters, mu, dt, sh, colored, n_colors, rounds)) return;
         // ── write back, colours and statistics ──
-        scene_store_bodies(B, b0, nb, SB);
+        scene_store_bodies(T, B, b0, nb, SB);
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) color[k0 + k] = colored ? SC.done(k) : kUncolored;
-        scene_stats(meta, colored, n_colors, rounds);
+        scene_stats(T, meta, colored, n_colors, rounds);
         __syncthreads();
     }
 }

@@ -50,6 +50,9 @@ struct dyph_world {
     uint32_t* f_counts = nullptr;        // [4 n_scenes]
     uint32_t* f_words = nullptr;
     uint32_t* f_pos = nullptr;           // [2 n_scenes] gather positions
+    uint32_t* f_items = nullptr;         // [4 f_n_items] work items of the fused kernel
+    uint32_t f_n_items = 0;
+    unsigned long long* f_phase = nullptr;  // [kFramePhases] phase timing of fused frames (null = off)
     uint32_t f_words_stride = 0, f_contact_slots = 0;
 };
 
@@ -141,10 +144,10 @@ dyph_status enqueue_frame(dyph_world* w, cudaStream_t s, int probe_stage = -1, v
                     w->bp->n_scenes, w->frame_smem};
         FrameBufs F{w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw,
                     w->f_counts, w->f_words, w->f_words_stride, w->f_contact_slots};
-        scene_frame_kernel<<<w->bp->n_scenes, kSceneThreads, w->frame_smem, s>>>(
-            d.bodies, d.shapes, S, F, ip.gravity[0], ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt,
-            ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->friction, ip.dt, w->sv->meta,
-            w->bp->counts, w->np->counts, w->stats + 4);
+        FrameParams P{d.bodies, d.shapes, ip.gravity[0], ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt,
+                      w->sv->friction, ip.dt, ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters,
+                      w->sv->meta, w->bp->counts, w->np->counts, w->stats + 4, w->f_phase};
+        scene_frame_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, s>>>(S, F, P, w->f_items, w->f_n_items);
         DYPH_CUDA_TRY(cudaGetLastError());
         if (probe_stage >= 0 && (st = probe_record(ev1, s)) != DYPH_OK) return st;
         frame_stats_kernel<<<1, 1, 0, s>>>(w->bp->counts, w->np->counts, w->bp->max_pairs, w->np->max_contacts,
@@ -197,7 +200,7 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     }
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                  w->f_words, w->f_pos};
+                  w->f_words, w->f_pos, w->f_items, w->f_phase};
     for (void* p : fb)
         if (p) cudaFree(p);
     broadphase_destroy(w->bp);
@@ -430,6 +433,8 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
         if (*b) cudaFree(*b);
         *b = nullptr;
     }
+    if (w->f_items) cudaFree(w->f_items);
+    w->f_items = nullptr;
     const size_t pslots = pb[n_scenes], cslots = cb[n_scenes];
     w->f_contact_slots = static_cast<uint32_t>(cslots);
     w->f_words_stride = static_cast<uint32_t>(cslots + n_scenes);
@@ -437,6 +442,31 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
                             static_cast<size_t>(kSceneWords) * w->f_words_stride, 2ull * n_scenes};
     for (int k = 0; k < 8; ++k)
         if (cudaMalloc(bufs[k], sizes[k] * sizeof(uint32_t)) != cudaSuccess) return DYPH_ERR_NOMEM;
+    // Work items, largest scenes first: a scene whose frame is expected to fit
+    // a quarter of the block's shared memory (about 4 pairs and 2.5 contacts
+    // per body) runs on one warp, four such scenes to a block; larger scenes
+    // take the whole block.
+    std::vector<uint32_t> order(n_scenes);
+    for (uint32_t i = 0; i < n_scenes; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [body_offset](uint32_t x, uint32_t y) {
+        return body_offset[x + 1] - body_offset[x] > body_offset[y + 1] - body_offset[y];
+    });
+    const uint32_t share = (smem / 4u) & ~15u;
+    std::vector<uint32_t> items;
+    std::vector<uint32_t> small;
+    for (uint32_t s : order) {
+        const uint32_t nb = body_offset[s + 1] - body_offset[s];
+        if (frame_body_bytes(nb) + 146u * nb <= share) {
+            small.push_back(s);
+        } else {
+            items.insert(items.end(), {s, kItemBlock, kItemEmpty, kItemEmpty});
+        }
+    }
+    for (size_t i = 0; i < small.size(); i += 4)
+        for (size_t j = 0; j < 4; ++j) items.push_back(i + j < small.size() ? small[i + j] : kItemEmpty);
+    w->f_n_items = static_cast<uint32_t>(items.size() / 4);
+    if (cudaMalloc(&w->f_items, items.size() * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
+    DYPH_CUDA_TRY(cudaMemcpy(w->f_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice));
     DYPH_CUDA_TRY(cudaMemcpy(w->f_pair_base, pb.data(), pb.size() * 4, cudaMemcpyHostToDevice));
     DYPH_CUDA_TRY(cudaMemcpy(w->f_contact_base, cb.data(), cb.size() * 4, cudaMemcpyHostToDevice));
     DYPH_CUDA_TRY(cudaMemset(w->f_counts, 0, 4ull * n_scenes * sizeof(uint32_t)));
@@ -535,5 +565,34 @@ extern "C" dyph_status dyph_world_set_trajectory(dyph_world* w, float* host_dst,
         if (!w->traj_copied[k]) DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->traj_copied[k], cudaEventDisableTiming));
     }
     if (!w->traj_stream) DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->traj_stream, cudaStreamNonBlocking));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_set_phase_timing(dyph_world* w, int on) {
+    if (!w) return DYPH_ERR_INVALID;
+    if (!w->fused) return on ? DYPH_ERR_INVALID : DYPH_OK;
+    DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    // captured frames hold the old setting
+    if (w->graph) cudaGraphExecDestroy(w->graph);
+    if (w->episode) cudaGraphExecDestroy(w->episode);
+    w->graph = w->episode = nullptr;
+    w->episode_frames = 0;
+    if (!on) {
+        if (w->f_phase) cudaFree(w->f_phase);
+        w->f_phase = nullptr;
+        return DYPH_OK;
+    }
+    if (!w->f_phase && cudaMalloc(&w->f_phase, kFramePhases * sizeof(unsigned long long)) != cudaSuccess)
+        return DYPH_ERR_NOMEM;
+    DYPH_CUDA_TRY(cudaMemset(w->f_phase, 0, kFramePhases * sizeof(unsigned long long)));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s, uint64_t* out, uint32_t cap) {
+    if (!w || !out || cap < static_cast<uint32_t>(kFramePhases) || !w->f_phase) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaMemcpyAsync(out, w->f_phase, kFramePhases * sizeof(uint64_t), cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaMemsetAsync(w->f_phase, 0, kFramePhases * sizeof(uint64_t), cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
     return DYPH_OK;
 }

@@ -416,6 +416,17 @@ class World:
         check(capi.lib().dyph_world_scene_hashes(self.h, _stream_ptr(stream), out.ctypes.data, n))
         return out
 
+    def phase_timing(self, on: bool = True) -> None:
+        """Time the phases of fused batched frames (dyph_world_set_phase_timing)."""
+        check(capi.lib().dyph_world_set_phase_timing(self.h, int(on)), "dyph_world_set_phase_timing")
+
+    def phase_ns(self) -> np.ndarray:
+        """Summed ns of the fused frames' phases since the last read: staging + integrate + boxes,
+        pair search, narrowphase, contact solve, write-back."""
+        out = np.zeros(5, np.uint64)
+        check(capi.lib().dyph_world_download_phase_ns(self.h, None, out.ctypes.data, 5), "phase_ns")
+        return out
+
     def sync_lists(self) -> None:
         """Compact the last frame's per-scene pair / contact lists (fused batched frames)."""
         check(capi.lib().dyph_world_sync_lists(self.h, None), "dyph_world_sync_lists")

@@ -56,13 +56,34 @@ def build_scene(args):
 
 
 def profile(world, scene, frames: int, warm: int = 30) -> None:
-    """Per-stage ms per frame (integrate, broadphase, narrowphase, solver)."""
+    """Per-stage ms per frame (integrate, broadphase, narrowphase, solver);
+    for a fused batched world, the frame's wall time and its phases' share
+    of the scenes' summed work time."""
     import torch
+    from . import capi
     names = ("integrate", "build_and_query", "narrowphase", "solve (XPBD)")
     fb = world.bodies.fbuf
     init = fb.clone()
     world.step(warm)
     start = fb.clone()
+    try:
+        world.phase_timing(True)
+    except capi.DyphError:
+        pass
+    else:
+        world.capture_episode(frames, 4)
+        world.run_episode()
+        torch.cuda.synchronize()
+        ms = float(world.probe_ms().mean())
+        ph = world.phase_ns().astype(np.float64)
+        world.phase_timing(False)
+        fb.copy_(init)
+        labels = ("stage+integrate+boxes", "pair search", "narrowphase", "contact solve", "write-back")
+        print(f"-- Fused frame: {ms:.3f} ms per frame over {frames} warm frames ({scene.n_scenes} scenes, "
+              f"{scene.n_bodies} bodies); phases, share of the scenes' summed work time --")
+        for name, v in zip(labels, ph):
+            print(f"  {name:<22} {100.0 * v / ph.sum():5.1f}%   ({v / frames / 1e3:10.1f} us summed per frame)")
+        return
     rows = []
     for stage in range(4):
         fb.copy_(start)

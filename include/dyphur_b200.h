@@ -327,6 +327,16 @@ dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32
  * list, the narrowphase's ContactView and the solver's colours (queued on s;
  * no-op for other worlds). Call it before reading those lists. */
 dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
+/* Phase timing of fused batched frames, the per-stage table of the
+ * reference's --profile mode (examples/stress_test_blocks/main.cpp:199-254)
+ * for a frame that is one kernel: with it on, every scene's team leader adds
+ * the device-clock ns of its phases — 0 staging, integrate and leaf boxes,
+ * 1 pair search, 2 narrowphase, 3 contact solve, 4 write-back — summed over
+ * scenes (work time, not wall time). Drops captured graphs; invalid for
+ * worlds that are not fused. dyph_world_download_phase_ns reads (cap >= 5)
+ * and clears the sums (blocking). */
+dyph_status dyph_world_set_phase_timing(dyph_world* w, int on);
+dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s, uint64_t* out, uint32_t cap);
 /* Blocking: FNV-1a-64 of every scene's pose arrays (one value for a single
  * scene); cap >= number of scenes. */
 dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uint64_t* host_out, uint32_t cap);
