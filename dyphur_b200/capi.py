@@ -6,7 +6,7 @@ import ctypes as C
 from ._lib import load_library
 
 OK, ERR_INVALID, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_CONTACT_OVERFLOW, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_NOMEM, \
-    ERR_NOT_FINITE, ERR_TOO_LARGE = range(10)
+    ERR_NOT_FINITE, ERR_TOO_LARGE, ERR_UNSUPPORTED = range(11)
 SORT_NOALLOC_MAX_KEYS = 262144
 SOLVER_REFERENCE, SOLVER_SEQUENTIAL, SOLVER_COLORED, SOLVER_REFERENCE_ROUNDS = 0, 1, 2, 3
 
@@ -102,6 +102,8 @@ _PROTOS = {
     "dyph_world_download_history": (_st, [_vp, _vp, _vp, _vp, C.c_uint32, _up]),
     "dyph_world_set_trajectory": (_st, [_vp, _vp, C.c_uint32, C.c_uint32]),
     "dyph_world_sync_lists": (_st, [_vp, _vp]),
+    "dyph_world_rollout": (_st, [_vp, C.c_int32, C.c_int32, _vp, _vp]),
+    "dyph_world_rollout_backward": (_st, [_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp]),
     "dyph_world_set_phase_timing": (_st, [_vp, C.c_int]),
     "dyph_world_download_phase_ns": (_st, [_vp, _vp, _vp, C.c_uint32]),
     "dyph_event_create": (_st, [C.POINTER(_vp)]),

@@ -5,11 +5,23 @@
 
 namespace dyph {
 
+// Branch word of a box-box contact (filled when box_box_centroid gets `br`):
+//   bits 0-1  SAT axis type (0 face of A, 1 face of B, 2 edge pair)
+//   bits 2-3  axis i, bits 4-5 axis j (edge pair)
+//   bit  7    reference face on B (face case; after the larger-face switch)
+//   bits 8-9  reference face axis
+//   bits 10-17 incident vertices kept (face case)
+//   bits 18-21 edge-point signs s0A, s1A, s0B, s1B negative (edge case)
+//   bit  22   edge case with |1 - b12^2| > 1e-6 (closest-point parameters solved)
+constexpr uint32_t kBrRefB = 1u << 7;
+constexpr uint32_t kBrDenom = 1u << 22;
+
 // box_box (core/src/narrowphase.cpp:130-306) followed by the centroid
 // reduction of process_pair (:991-998). Returns false for no contact.
 __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz, const float Ae[3][3],
                                                  const float Ah[3], float bcx, float bcy, float bcz,
-                                                 const float Be[3][3], const float Bh[3], Contact& out) {
+                                                 const float Be[3][3], const float Bh[3], Contact& out,
+                                                 uint32_t* br = nullptr) {
     const float eps_par = 1e-5f;
     float C[3][3];
     float dx = bcx - acx, dy = bcy - acy, dz = bcz - acz;
@@ -42,6 +54,8 @@ __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz
     float sx_acc = 0.f, sy_acc = 0.f, sz_acc = 0.f, sd_acc = 0.f;
     int n_out = 0;
     int best_type = best.type, best_i = best.i;
+    uint32_t word = static_cast<uint32_t>(best.type) | (static_cast<uint32_t>(best.i) << 2) |
+                    (static_cast<uint32_t>(best.j) << 4);
     if (best_type == 0 || best_type == 1) {
         if (best_type == 0) {
             int t0A = (best_i + 1) % 3, t1A = (best_i + 2) % 3;
@@ -53,6 +67,7 @@ __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz
         }
         const bool a_is_ref = (best_type == 0);
         const int ref_ax = best_i;
+        word |= (a_is_ref ? 0u : kBrRefB) | (static_cast<uint32_t>(ref_ax) << 8);
         const float rcx = a_is_ref ? acx : bcx, rcy = a_is_ref ? acy : bcy, rcz = a_is_ref ? acz : bcz;
         float Re[3][3], Ie[3][3], Rh[3], Ih[3];
 #pragma unroll
@@ -93,6 +108,7 @@ __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz
             if (fabsf(qt0) > Rh_t0 + 1e-3f) continue;
             if (fabsf(qt1) > Rh_t1 + 1e-3f) continue;
             if (n_out < 4) {
+                word |= 1u << (10 + k);
                 // centroid accumulation in the reference's order (cx += opx[k] ...)
                 sx_acc += vx - sign_depth * dv * bnx;
                 sy_acc += vy - sign_depth * dv * bny;
@@ -123,6 +139,8 @@ __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz
         float d1 = wx * uAx + wy * uAy + wz * uAz;
         float d2 = wx * uBx + wy * uBy + wz * uBz;
         float s_t = 0.f, t_t = 0.f;
+        word |= (s0A < 0.f ? 1u << 18 : 0u) | (s1A < 0.f ? 1u << 19 : 0u) | (s0B < 0.f ? 1u << 20 : 0u) |
+                (s1B < 0.f ? 1u << 21 : 0u) | (fabsf(denom) > 1e-6f ? kBrDenom : 0u);
         if (fabsf(denom) > 1e-6f) {
             s_t = __fdiv_rn(b12 * d2 - d1, denom);
             t_t = __fdiv_rn(d2 - b12 * d1, denom);
@@ -136,6 +154,7 @@ __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz
         n_out = 1;
     }
     if (n_out == 0) return false;
+    if (br) *br = word;
     float inv = __fdiv_rn(1.f, static_cast<float>(n_out));
     out.px = sx_acc * inv; out.py = sy_acc * inv; out.pz = sz_acc * inv;
     out.nx = bnx; out.ny = bny; out.nz = bnz;
@@ -146,17 +165,18 @@ __device__ __forceinline__ bool box_box_centroid(float acx, float acy, float acz
 // process_pair for box / sphere shapes (narrowphase.cpp:920-1001).
 // Returns true and fills `c` when the pair is in contact.
 template <class Bodies, class Shapes>
-__device__ __forceinline__ bool process_pair(const Bodies& B, const Shapes& S, uint32_t ia, uint32_t ib, Contact& c) {
+__device__ __forceinline__ bool process_pair(const Bodies& B, const Shapes& S, uint32_t ia, uint32_t ib, Contact& c,
+                                             uint32_t* br = nullptr) {
     const uint32_t sha = B.shape(ia), shb = B.shape(ib);
     const uint32_t ta = S.type(sha), tb = S.type(shb);
     c.a = ia; c.b = ib;
     if (ta == kShapeSphere && tb == kShapeSphere)
-        return sphere_sphere(B.px(ia), B.py(ia), B.pz(ia), S.hx(sha), B.px(ib), B.py(ib), B.pz(ib), S.hx(shb), c);
+        return sphere_sphere(B.px(ia), B.py(ia), B.pz(ia), S.hx(sha), B.px(ib), B.py(ib), B.pz(ib), S.hx(shb), c, br);
     if (ta == kShapeSphere && tb == kShapeBox) {
         float Be[3][3];
         make_axes(B.qw(ib), B.qx(ib), B.qy(ib), B.qz(ib), Be);
         if (!sphere_box(B.px(ia), B.py(ia), B.pz(ia), S.hx(sha), B.px(ib), B.py(ib), B.pz(ib), Be, S.hx(shb),
-                        S.hy(shb), S.hz(shb), c))
+                        S.hy(shb), S.hz(shb), c, br))
             return false;
         c.nx = -c.nx; c.ny = -c.ny; c.nz = -c.nz;
         return true;
@@ -165,7 +185,7 @@ __device__ __forceinline__ bool process_pair(const Bodies& B, const Shapes& S, u
         float Ae[3][3];
         make_axes(B.qw(ia), B.qx(ia), B.qy(ia), B.qz(ia), Ae);
         return sphere_box(B.px(ib), B.py(ib), B.pz(ib), S.hx(shb), B.px(ia), B.py(ia), B.pz(ia), Ae, S.hx(sha),
-                          S.hy(sha), S.hz(sha), c);
+                          S.hy(sha), S.hz(sha), c, br);
     }
     if (ta == kShapeBox && tb == kShapeBox) {
         float Ae[3][3], Be[3][3];
@@ -173,7 +193,7 @@ __device__ __forceinline__ bool process_pair(const Bodies& B, const Shapes& S, u
         const float Bh[3] = {S.hx(shb), S.hy(shb), S.hz(shb)};
         make_axes(B.qw(ia), B.qx(ia), B.qy(ia), B.qz(ia), Ae);
         make_axes(B.qw(ib), B.qx(ib), B.qy(ib), B.qz(ib), Be);
-        return box_box_centroid(B.px(ia), B.py(ia), B.pz(ia), Ae, Ah, B.px(ib), B.py(ib), B.pz(ib), Be, Bh, c);
+        return box_box_centroid(B.px(ia), B.py(ia), B.pz(ia), Ae, Ah, B.px(ib), B.py(ib), B.pz(ib), Be, Bh, c, br);
     }
     return false;  // convex hulls / meshes are not on this path
 }
@@ -215,8 +235,15 @@ constexpr int kSolveSkipped = 0;   // depth <= 0 or already resolved
 constexpr int kSolveDone = 1;      // correction applied
 constexpr int kSolveDeferred = 2;  // w_total < 1e-10: lambda untouched, retried next iteration
 
+// Branch flags of one contact solve (solve_contact's optional `flags`).
+constexpr uint32_t kSfActive = 1u;     // position correction applied
+constexpr uint32_t kSfNormal = 2u;     // normal velocity impulse (vrel_n < 0)
+constexpr uint32_t kSfFriction = 4u;   // friction impulse applied
+constexpr uint32_t kSfClamped = 8u;    // friction impulse clamped to mu * j_n_static
+
 template <class Bodies>
-__device__ __forceinline__ int solve_contact(const Bodies& B, const Contact& ct, float mu, float& lc, float dt) {
+__device__ __forceinline__ int solve_contact(const Bodies& B, const Contact& ct, float mu, float& lc, float dt,
+                                             uint32_t* flags = nullptr) {
     const uint32_t ia = ct.a, ib = ct.b;
     const float depth = ct.depth;
     if (depth <= 0.f) return kSolveSkipped;
@@ -238,6 +265,7 @@ __device__ __forceinline__ int solve_contact(const Bodies& B, const Contact& ct,
     if (w_total < 1e-10f) return kSolveDeferred;
     const float dl = __fdiv_rn(remaining, w_total);
     lc += remaining;
+    if (flags) *flags = kSfActive;
     if (wa != 0.f) { B.px(ia) += wa * dl * nx; B.py(ia) += wa * dl * ny; B.pz(ia) += wa * dl * nz; }
     if (wb != 0.f) { B.px(ib) -= wb * dl * nx; B.py(ib) -= wb * dl * ny; B.pz(ib) -= wb * dl * nz; }
     apply_ang_delta(B, ia, dl * iIa_x, dl * iIa_y, dl * iIa_z);
@@ -254,6 +282,7 @@ __device__ __forceinline__ int solve_contact(const Bodies& B, const Contact& ct,
         const float vrel_x = vcax - vcbx, vrel_y = vcay - vcby, vrel_z = vcaz - vcbz;
         const float vrel_n = vrel_x * nx + vrel_y * ny + vrel_z * nz;
         if (vrel_n < 0.f) {
+            if (flags) *flags |= kSfNormal;
             const float j_n = __fdiv_rn(-vrel_n, w_total);
             float doa_x, doa_y, doa_z, dob_x, dob_y, dob_z;
             world_inv_inertia(B, ia, raxnx, raxny, raxnz, doa_x, doa_y, doa_z);
@@ -294,6 +323,7 @@ __device__ __forceinline__ int solve_contact(const Bodies& B, const Contact& ct,
             if (wt > 1e-10f) {
                 const float j_n_static = __fdiv_rn(lc, dt * w_total);
                 float j_t = __fdiv_rn(vt_len, wt);
+                if (flags) *flags |= kSfFriction | (mu * j_n_static < j_t ? kSfClamped : 0u);
                 j_t = fminf(j_t, mu * j_n_static);
                 if (wa != 0.f) {
                     B.vx(ia) -= wa * j_t * tx; B.vy(ia) -= wa * j_t * ty; B.vz(ia) -= wa * j_t * tz;

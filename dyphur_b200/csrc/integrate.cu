@@ -59,6 +59,7 @@ extern "C" const char* dyph_status_string(int status) {
         case DYPH_ERR_NOMEM: return "device allocation failed";
         case DYPH_ERR_NOT_FINITE: return "non-finite body state";
         case DYPH_ERR_TOO_LARGE: return "size exceeds the fixed scratch of a no-allocation entry point";
+        case DYPH_ERR_UNSUPPORTED: return "a frame took a path the adjoint does not differentiate";
         default: return "unknown status";
     }
 }

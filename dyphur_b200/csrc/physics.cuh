@@ -181,13 +181,16 @@ __device__ __forceinline__ void make_axes(float qw, float qx, float qy, float qz
 }
 
 // sphere_sphere (narrowphase.cpp:46-68).
+// `br` (optional) receives the branch taken: bit 0 set when the centres
+// coincide (dist < 1e-8, fixed normal).
 __device__ __forceinline__ bool sphere_sphere(float acx, float acy, float acz, float ra, float bcx, float bcy,
-                                              float bcz, float rb, Contact& c) {
+                                              float bcz, float rb, Contact& c, uint32_t* br = nullptr) {
     float dx = acx - bcx, dy = acy - bcy, dz = acz - bcz;
     float dist2 = dx * dx + dy * dy + dz * dz;
     float sum_r = ra + rb;
     if (dist2 >= sum_r * sum_r) return false;
     float dist = __fsqrt_rn(dist2);
+    if (br) *br = dist < 1e-8f ? 1u : 0u;
     if (dist < 1e-8f) { c.nx = 0.f; c.ny = 1.f; c.nz = 0.f; }
     else { float inv = __fdiv_rn(1.f, dist); c.nx = dx * inv; c.ny = dy * inv; c.nz = dz * inv; }
     c.depth = sum_r - dist;
@@ -198,10 +201,13 @@ __device__ __forceinline__ bool sphere_sphere(float acx, float acy, float acz, f
     return true;
 }
 
-// sphere_box (narrowphase.cpp:71-127); E rows are the box axes.
+// sphere_box (narrowphase.cpp:71-127); E rows are the box axes. `br`
+// (optional) receives the branch taken: bit 0 centre inside the box, then
+// bits 1-2 the face axis and bit 3 its sign (s < 0); outside, bits 4 + 2k /
+// 5 + 2k mark local coordinate k clamped to -h_k / +h_k.
 __device__ __forceinline__ bool sphere_box(float scx, float scy, float scz, float sr, float bcx, float bcy,
                                            float bcz, const float E[3][3], float bh0, float bh1, float bh2,
-                                           Contact& c) {
+                                           Contact& c, uint32_t* br = nullptr) {
     const float e0x = E[0][0], e0y = E[0][1], e0z = E[0][2];
     const float e1x = E[1][0], e1y = E[1][1], e1z = E[1][2];
     const float e2x = E[2][0], e2y = E[2][1], e2z = E[2][2];
@@ -220,19 +226,25 @@ __device__ __forceinline__ bool sphere_box(float scx, float scy, float scz, floa
             float s = q0 >= 0.f ? 1.f : -1.f;
             c.nx = -(s * e0x); c.ny = -(s * e0y); c.nz = -(s * e0z);
             c.depth = sr + pen0;
+            if (br) *br = 1u | (0u << 1) | (s < 0.f ? 8u : 0u);
         } else if (pen1 <= pen2) {
             float s = q1 >= 0.f ? 1.f : -1.f;
             c.nx = -(s * e1x); c.ny = -(s * e1y); c.nz = -(s * e1z);
             c.depth = sr + pen1;
+            if (br) *br = 1u | (1u << 1) | (s < 0.f ? 8u : 0u);
         } else {
             float s = q2 >= 0.f ? 1.f : -1.f;
             c.nx = -(s * e2x); c.ny = -(s * e2y); c.nz = -(s * e2z);
             c.depth = sr + pen2;
+            if (br) *br = 1u | (2u << 1) | (s < 0.f ? 8u : 0u);
         }
         c.px = scx - c.nx * sr; c.py = scy - c.ny * sr; c.pz = scz - c.nz * sr;
         return true;
     }
     if (dist2 >= sr * sr) return false;
+    if (br)
+        *br = (q0 < -bh0 ? 16u : 0u) | (q0 > bh0 ? 32u : 0u) | (q1 < -bh1 ? 64u : 0u) | (q1 > bh1 ? 128u : 0u) |
+              (q2 < -bh2 ? 256u : 0u) | (q2 > bh2 ? 512u : 0u);
     float dist = __fsqrt_rn(dist2);
     float inv_d = __fdiv_rn(1.f, dist);
     float wx = lx * e0x + ly * e1x + lz * e2x;

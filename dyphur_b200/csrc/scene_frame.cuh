@@ -94,11 +94,30 @@ __device__ __forceinline__ void phase_mark(const Team& T, const FrameParams& P_,
     }
 }
 
+// Recording for the adjoint pass (frame_scene with `adj`): the frame is
+// recomputed from the given state, its branches and intermediates recorded,
+// and nothing is written back or reported.
+struct AdjRun {
+    float* rec;          // [kRecWords][rec_stride] per-contact records, slot = contact slot of the scene
+    uint32_t rec_stride;
+    float* pose1;        // [7][n_stride] pose after integrate (x, q)
+    float* qs;           // [4][n_stride] quaternions after the sweeps, before the renormalisations
+    uint32_t n_stride;
+    uint32_t* flag;      // unsupported paths
+};
+
+// What the adjoint pass needs of a recomputed frame.
+struct FrameOut {
+    SceneContacts SC;
+    uint32_t m, groups;
+};
+
 // One frame of scene s by team T with `smem_bytes` of shared memory at smem.
 // Returns false after raising an error.
 template <class Team>
 __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
-                            const SceneBufs& S, const FrameBufs& F, const FrameParams& P_) {
+                            const SceneBufs& S, const FrameBufs& F, const FrameParams& P_,
+                            const AdjRun* adj = nullptr, FrameOut* out = nullptr) {
     const GlobalBodies B{P_.gb};
     const uint32_t lane = threadIdx.x & 31u;
     uint64_t t0 = P_.phase_ns ? global_ns() : 0u;
@@ -130,6 +149,11 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
             SB.px(i) = p.px; SB.py(i) = p.py; SB.pz(i) = p.pz;
             SB.qw(i) = p.qw; SB.qx(i) = p.qx; SB.qy(i) = p.qy; SB.qz(i) = p.qz;
             SB.vx(i) = p.vx; SB.vy(i) = p.vy; SB.vz(i) = p.vz;
+        }
+        if (adj) {
+            float* r = adj->pose1 + b0 + i;
+            const float v[7] = {SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i), SB.qy(i), SB.qz(i)};
+            for (int j = 0; j < 7; ++j) r[static_cast<size_t>(j) * adj->n_stride] = v[j];
         }
         // leaf box from the integrated pose, kept as the exact floats of its fp16 bounds
         const BoxF bx = unpack_box(leaf_box(SS.type(i), SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i),
@@ -197,7 +221,7 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
         }
     }
     T.sync();
-    if (in_smem)
+    if (in_smem && !adj)
         for (uint32_t p = T.rank(); p < P; p += T.size()) F.pair_raw[F.pair_base[s] + p] = pairs[p];
     phase_mark(T, P_, 1, t0);
     // ── narrowphase: contacts in pair order ──
@@ -209,9 +233,10 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
         const uint32_t p = base + T.rank();
         Contact c{};
         bool hit = false;
+        uint32_t br = 0u;
         if (p < P) {
             const uint32_t ab = pairs[p];
-            hit = process_pair(SB, SS, ab & 0xFFFFu, ab >> 16, c);
+            hit = process_pair(SB, SS, ab & 0xFFFFu, ab >> 16, c, adj ? &br : nullptr);
         }
         uint32_t tot;
         const uint32_t ex = T.exclusive_scan(hit ? 1u : 0u, sh.scan, tot);
@@ -225,15 +250,19 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
             SC.g(6, k) = c.depth;
             if (SB.im(c.b) != 0.f) atomicAdd(&R.cnt[c.b], 1u);
             const uint32_t slot = cbase + k, st = F.contact_slots;
-            F.contact_raw[slot] = b0 + c.a;
-            F.contact_raw[st + slot] = b0 + c.b;
-            F.contact_raw[2 * st + slot] = __float_as_uint(c.px);
-            F.contact_raw[3 * st + slot] = __float_as_uint(c.py);
-            F.contact_raw[4 * st + slot] = __float_as_uint(c.pz);
-            F.contact_raw[5 * st + slot] = __float_as_uint(c.nx);
-            F.contact_raw[6 * st + slot] = __float_as_uint(c.ny);
-            F.contact_raw[7 * st + slot] = __float_as_uint(c.nz);
-            F.contact_raw[8 * st + slot] = __float_as_uint(c.depth);
+            if (adj) {
+                adj->rec[27ull * adj->rec_stride + slot] = __uint_as_float(br);
+            } else {
+                F.contact_raw[slot] = b0 + c.a;
+                F.contact_raw[st + slot] = b0 + c.b;
+                F.contact_raw[2 * st + slot] = __float_as_uint(c.px);
+                F.contact_raw[3 * st + slot] = __float_as_uint(c.py);
+                F.contact_raw[4 * st + slot] = __float_as_uint(c.pz);
+                F.contact_raw[5 * st + slot] = __float_as_uint(c.nx);
+                F.contact_raw[6 * st + slot] = __float_as_uint(c.ny);
+                F.contact_raw[7 * st + slot] = __float_as_uint(c.nz);
+                F.contact_raw[8 * st + slot] = __float_as_uint(c.depth);
+            }
         }
         T.sync();
         if (T.leader()) sh.carry += tot;
@@ -241,7 +270,7 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     }
     const uint32_t m_true = sh.carry, m = min(m_true, cc);
     T.sync();  // every thread has read the count before scene_solve reuses sh.carry
-    if (T.leader()) {
+    if (T.leader() && !adj) {
         F.counts[4 * s + 0] = P;
         F.counts[4 * s + 1] = p_true;
         F.counts[4 * s + 2] = m;
@@ -257,16 +286,22 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     phase_mark(T, P_, 2, t0);
     // ── contact solve (none without contacts, as the reference's solve returns) ──
     bool colored = false;
-    uint32_t n_colors = 0, rounds = 0;
+    uint32_t n_colors = 0, rounds = 0, groups = 0;
     if (m > 0) {
-        if (!scene_solve(T, nb, m, SB, R, SC, P_.mode, P_.n_iters, P_.mu, P_.dt, sh, colored, n_colors, rounds))
+        SolveRecord rec{};
+        if (adj) rec = SolveRecord{adj->rec, adj->rec_stride, cbase, adj->qs, adj->n_stride, b0, adj->flag};
+        if (!scene_solve(T, nb, m, SB, R, SC, P_.mode, P_.n_iters, P_.mu, P_.dt, sh, colored, n_colors, rounds,
+                         adj ? &rec : nullptr, &groups))
             return false;
-        for (uint32_t k = T.rank(); k < m; k += T.size())
-            F.color_raw[cbase + k] = colored ? SC.done(k) : kUncolored;
-        scene_stats(T, P_.meta, colored, n_colors, rounds);
+        if (!adj) {
+            for (uint32_t k = T.rank(); k < m; k += T.size())
+                F.color_raw[cbase + k] = colored ? SC.done(k) : kUncolored;
+            scene_stats(T, P_.meta, colored, n_colors, rounds);
+        }
     }
+    if (out) *out = FrameOut{SC, m, groups};
     phase_mark(T, P_, 3, t0);
-    scene_store_bodies(T, B, b0, nb, SB);
+    if (!adj) scene_store_bodies(T, B, b0, nb, SB);
     T.sync();
     phase_mark(T, P_, 4, t0);
     return true;

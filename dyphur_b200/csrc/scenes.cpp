@@ -242,7 +242,7 @@ extern "C" dyph_scene_set* dyph_scene_make(int kind, uint64_t seed, int32_t a0, 
                         }
                 const float Ip = 5.f / 3.f * (0.3f * 0.3f + 0.3f * 0.3f);
                 const float Ipv[3] = {Ip, Ip, Ip};
-                const float pp[3] = {-2.5f, gy + 0.3f + 0.01f, 0.f};
+                const float pp[3] = {-1.2f, gy + 0.3f + 0.01f, 0.f};
                 const float pv[3] = {N(rng), 0.f, 0.f};
                 B.add_body(pp, q, pv, 5.f, Ipv, ps, 0u);
                 B.add_ground(gs);

@@ -32,8 +32,9 @@ typedef enum dyph_scene_kind {
      * the box's density) over its own ground box. */
     DYPH_SCENE_BATCH = 3,
     /* a0 scenes of 64 boxes (h 0.2 m, 1 kg) in a 4x4x4 block resting on the
-     * ground plus a pusher box (h 0.3 m, 5 kg) moving toward the block with
-     * speed N(2, 0.3) m/s. */
+     * ground plus a pusher box (h 0.3 m, 5 kg) starting 0.285 m from the
+     * block's face and moving toward it with speed N(2, 0.3) m/s; loss
+     * targets for the 64 boxes (zero rows for the pusher and the ground). */
     DYPH_SCENE_PUSH = 4,
     /* a0 independent scenes, counts log-uniform in [a1, a2], bodies drawn as in
      * DYPH_SCENE_RANDOM_PILE inside a footprint scaled to the count. */

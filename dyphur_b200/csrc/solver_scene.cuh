@@ -217,18 +217,58 @@ __device__ void scene_group(const Team& T, uint32_t m, uint32_t groups, uint32_t
     T.sync();
 }
 
+// What the adjoint pass records of a scene's solve (solve_record): for every
+// contact that acts, both bodies' state before its solve and lambda; the
+// quaternions before the renormalisations.
+constexpr int kRecWords = 36;  // per-contact record rows (see SolveRecord)
+struct SolveRecord {
+    // rows r of contact k at rec[r * stride + base + k]: 0-12 body a state,
+    // 13-25 body b state, 26 lambda before, 27 narrowphase branch word,
+    // 28-34 contact geometry adjoint (point, normal, depth), 35 acted
+    float* rec;
+    uint32_t stride, base;
+    float* qs;           // [4][qs_stride] quaternions after the sweeps, at body b0 + i
+    uint32_t qs_stride, b0;
+    uint32_t* flag;      // set when the solve took a path the adjoint does not cover
+};
+
+__device__ __forceinline__ void record_state(float* r, uint32_t stride, const SceneBodies& SB, uint32_t i,
+                                             int row0) {
+    const float v[13] = {SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i), SB.qy(i), SB.qz(i),
+                         SB.vx(i), SB.vy(i), SB.vz(i), SB.wx(i), SB.wy(i), SB.wz(i)};
+#pragma unroll
+    for (int j = 0; j < 13; ++j) r[static_cast<size_t>(row0 + j) * stride] = v[j];
+}
+
 // One sweep over the groups in ascending order, one contact per thread at a
 // time inside a group (no two of a group share a dynamic body).
 template <class Team>
 __device__ void scene_sweep(const Team& T, uint32_t groups, const SceneBodies& SB, const SceneContacts& SC, float mu,
-                            float dt, int* s_flag) {
+                            float dt, int* s_flag, const SolveRecord* rec = nullptr, int iter = 0) {
     for (uint32_t g = 0; g < groups; ++g) {
         const uint32_t end = SC.pa(g + 1);
         for (uint32_t i = SC.pa(g) + T.rank(); i < end; i += T.size()) {
             const uint32_t k = SC.ent(i);
             const Contact ct = SC.contact(k);
             float lc = SC.lam(k);
-            if (solve_contact(SB, ct, mu, lc, dt) == kSolveDeferred) *s_flag = 1;
+            if (rec) {
+                // the pre-solve state is written first and marked as acted only if it did
+                float* r = rec->rec + rec->base + k;
+                const float lc0 = lc;
+                record_state(r, rec->stride, SB, ct.a, 0);
+                record_state(r, rec->stride, SB, ct.b, 13);
+                uint32_t fl = 0u;
+                if (solve_contact(SB, ct, mu, lc, dt, &fl) == kSolveDeferred) *s_flag = 1;
+                if (fl & kSfActive) {
+                    r[26ull * rec->stride] = lc0;
+                    r[35ull * rec->stride] = 1.f;
+                    if (iter > 0) atomicOr(rec->flag, 1u);  // acted after a renormalisation
+                } else if (iter == 0) {
+                    r[35ull * rec->stride] = 0.f;
+                }
+            } else if (solve_contact(SB, ct, mu, lc, dt) == kSolveDeferred) {
+                *s_flag = 1;
+            }
             SC.lam(k) = lc;
         }
         T.sync();
@@ -294,7 +334,8 @@ __device__ __forceinline__ void scene_store_bodies(const Team& T, const GlobalBo
 template <class Team>
 __device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneBodies& SB, const SceneSolverRows& R,
                             const SceneContacts& SC, int mode, int n_iters, float mu, float dt, SceneShared& sh,
-                            bool& colored_out, uint32_t& n_colors_out, uint32_t& rounds_out) {
+                            bool& colored_out, uint32_t& n_colors_out, uint32_t& rounds_out,
+                            const SolveRecord* rec = nullptr, uint32_t* groups_out = nullptr) {
     // ── predecessors in contact order: b-side lists (scan, fill, sort) ──
     if (T.leader()) {
         sh.carry = 0u;
@@ -405,11 +446,20 @@ __device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneB
     scene_group(T, m, groups, base, SC, sh.scan, &sh.carry);
     // ── sweeps and renormalisation ──
     bool deferred = false;
+    if (groups_out) *groups_out = groups;
     for (int iter = 0; iter < n_iters; ++iter) {
         if (iter == 0 || deferred) {
-            scene_sweep(T, groups, SB, SC, mu, dt, &sh.flag);
+            scene_sweep(T, groups, SB, SC, mu, dt, &sh.flag, rec, iter);
             deferred = sh.flag != 0;
         }
+        if (rec && iter == 0)
+            for (uint32_t i = T.rank(); i < nb; i += T.size()) {
+                float* q = rec->qs + rec->b0 + i;
+                q[0] = SB.qw(i);
+                q[rec->qs_stride] = SB.qx(i);
+                q[2ull * rec->qs_stride] = SB.qy(i);
+                q[3ull * rec->qs_stride] = SB.qz(i);
+            }
         const int times = deferred ? 1 : n_iters - iter;
         for (uint32_t i = T.rank(); i < nb; i += T.size()) {
             float qw = SB.qw(i), qx = SB.qx(i), qy = SB.qy(i), qz = SB.qz(i);

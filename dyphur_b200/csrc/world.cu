@@ -14,6 +14,7 @@
 
 #include "internal.cuh"
 #include "scene_frame.cuh"
+#include "scene_adjoint.cuh"
 
 struct dyph_world {
     dyph_world_desc desc{};
@@ -53,6 +54,14 @@ struct dyph_world {
     uint32_t* f_items = nullptr;         // [4 f_n_items] work items of the fused kernel
     uint32_t f_n_items = 0;
     unsigned long long* f_phase = nullptr;  // [kFramePhases] phase timing of fused frames (null = off)
+    // Adjoint of fused frames (dyph_world_rollout_backward), allocated on first use.
+    float* a_rec = nullptr;              // [kRecWords][f_contact_slots]
+    float* a_pose1 = nullptr;            // [7][n]
+    float* a_qs = nullptr;               // [4][n]
+    float* a_g[2] = {nullptr, nullptr};  // [13][n] adjoint ping-pong
+    float* a_seg = nullptr;              // [a_seg_frames][13][n] states of one checkpoint segment
+    uint32_t a_seg_frames = 0;
+    uint32_t* a_flag = nullptr;
     uint32_t f_words_stride = 0, f_contact_slots = 0;
 };
 
@@ -200,7 +209,8 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     }
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                  w->f_words, w->f_pos, w->f_items, w->f_phase};
+                  w->f_words, w->f_pos, w->f_items, w->f_phase, w->a_rec, w->a_pose1, w->a_qs, w->a_g[0],
+                  w->a_g[1], w->a_seg, w->a_flag};
     for (void* p : fb)
         if (p) cudaFree(p);
     broadphase_destroy(w->bp);
@@ -595,4 +605,142 @@ extern "C" dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s
     DYPH_CUDA_TRY(cudaMemsetAsync(w->f_phase, 0, kFramePhases * sizeof(uint64_t), cs));
     DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
     return DYPH_OK;
+}
+
+namespace dyph {
+namespace {
+
+// State rows (pos xyz, rot wxyz, vel xyz, ang xyz) of every body to / from a
+// [13][n] buffer.
+__global__ void pack_state_kernel(GlobalBodies B, float* __restrict__ out) {
+    const uint32_t n = B.v.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float v[13] = {B.px(i), B.py(i), B.pz(i), B.qw(i), B.qx(i), B.qy(i), B.qz(i),
+                             B.vx(i), B.vy(i), B.vz(i), B.wx(i), B.wy(i), B.wz(i)};
+        for (int r = 0; r < 13; ++r) out[static_cast<size_t>(r) * n + i] = v[r];
+    }
+}
+
+__global__ void unpack_state_kernel(const float* __restrict__ in, GlobalBodies B) {
+    const uint32_t n = B.v.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = in + i;
+        B.px(i) = r[0]; B.py(i) = r[n]; B.pz(i) = r[2ull * n];
+        B.qw(i) = r[3ull * n]; B.qx(i) = r[4ull * n]; B.qy(i) = r[5ull * n]; B.qz(i) = r[6ull * n];
+        B.vx(i) = r[7ull * n]; B.vy(i) = r[8ull * n]; B.vz(i) = r[9ull * n];
+        B.wx(i) = r[10ull * n]; B.wy(i) = r[11ull * n]; B.wz(i) = r[12ull * n];
+    }
+}
+
+dyph_status pack_state(const dyph_world* w, float* out, cudaStream_t s) {
+    const uint32_t n = w->desc.bodies.n;
+    pack_state_kernel<<<(n + 255) / 256, 256, 0, s>>>(GlobalBodies{w->desc.bodies}, out);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    return DYPH_OK;
+}
+
+dyph_status unpack_state(const dyph_world* w, const float* in, cudaStream_t s) {
+    const uint32_t n = w->desc.bodies.n;
+    unpack_state_kernel<<<(n + 255) / 256, 256, 0, s>>>(in, GlobalBodies{w->desc.bodies});
+    DYPH_CUDA_TRY(cudaGetLastError());
+    return DYPH_OK;
+}
+
+// A BodyView over a [13][n] state buffer, with the world's constant rows.
+dyph_bodies state_view(const dyph_world* w, float* st) {
+    dyph_bodies v = w->desc.bodies;
+    const size_t n = v.n;
+    float** rows[13] = {&v.pos_x, &v.pos_y, &v.pos_z, &v.rot_w, &v.rot_x, &v.rot_y, &v.rot_z,
+                        &v.vel_x, &v.vel_y, &v.vel_z, &v.ang_x, &v.ang_y, &v.ang_z};
+    for (int r = 0; r < 13; ++r) *rows[r] = st + r * n;
+    return v;
+}
+
+dyph_status adjoint_buffers(dyph_world* w, uint32_t seg_frames) {
+    const size_t n = w->desc.bodies.n;
+    if (!w->a_rec) {
+        if (cudaMalloc(&w->a_rec, static_cast<size_t>(kRecWords) * w->f_contact_slots * 4) != cudaSuccess ||
+            cudaMalloc(&w->a_pose1, 7 * n * 4) != cudaSuccess || cudaMalloc(&w->a_qs, 4 * n * 4) != cudaSuccess ||
+            cudaMalloc(&w->a_g[0], 13 * n * 4) != cudaSuccess || cudaMalloc(&w->a_g[1], 13 * n * 4) != cudaSuccess ||
+            cudaMalloc(&w->a_flag, 4) != cudaSuccess)
+            return DYPH_ERR_NOMEM;
+        DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(w->frame_smem)));
+    }
+    if (seg_frames > w->a_seg_frames) {
+        if (w->a_seg) cudaFree(w->a_seg);
+        w->a_seg = nullptr;
+        w->a_seg_frames = 0;
+        if (cudaMalloc(&w->a_seg, static_cast<size_t>(seg_frames) * 13 * n * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
+        w->a_seg_frames = seg_frames;
+    }
+    return DYPH_OK;
+}
+
+}  // namespace
+}  // namespace dyph
+
+extern "C" dyph_status dyph_world_rollout(dyph_world* w, int32_t n_frames, int32_t every, float* d_ckpt,
+                                          dyph_stream s) {
+    if (!w || !w->fused || n_frames <= 0 || every <= 0 || !d_ckpt) return DYPH_ERR_INVALID;
+    const size_t n = w->desc.bodies.n;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    for (int32_t f = 0; f < n_frames; ++f) {
+        if (f % every == 0) {
+            dyph_status st = pack_state(w, d_ckpt + static_cast<size_t>(f / every) * 13 * n, cs);
+            if (st != DYPH_OK) return st;
+        }
+        dyph_status st = dyph_world_step(w, 1, s);
+        if (st != DYPH_OK) return st;
+    }
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_frames, int32_t every,
+                                                   const float* d_ckpt, const float* d_grad_final,
+                                                   float* d_grad_init, float* d_grad_inv_mass, dyph_stream s) {
+    if (!w || !w->fused || n_frames <= 0 || every <= 0 || !d_ckpt || !d_grad_final || !d_grad_init ||
+        !d_grad_inv_mass)
+        return DYPH_ERR_INVALID;
+    dyph_status st = adjoint_buffers(w, static_cast<uint32_t>(every));
+    if (st != DYPH_OK) return st;
+    const size_t n = w->desc.bodies.n;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaMemsetAsync(w->a_flag, 0, 4, cs));
+    DYPH_CUDA_TRY(cudaMemsetAsync(d_grad_inv_mass, 0, n * 4, cs));
+    DYPH_CUDA_TRY(cudaMemcpyAsync(w->a_g[0], d_grad_final, 13 * n * 4, cudaMemcpyDeviceToDevice, cs));
+    const dyph_world_desc& d = w->desc;
+    const dyph_integrator_params& ip = d.integrator;
+    const float sub_dt = ip.dt / static_cast<float>(ip.n_substeps);
+    SceneBufs S{w->bp->body_offset, w->bp->bvh.scene_of, w->sv->scene_order, nullptr, nullptr, 0, w->bp->n_scenes,
+                w->frame_smem};
+    FrameBufs F{w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
+                w->f_words, w->f_words_stride, w->f_contact_slots};
+    AdjRun A{w->a_rec, w->f_contact_slots, w->a_pose1, w->a_qs, static_cast<uint32_t>(n), w->a_flag};
+    int cur = 0;
+    const int32_t n_seg = (n_frames + every - 1) / every;
+    for (int32_t seg = n_seg - 1; seg >= 0; --seg) {
+        const int32_t f0 = seg * every, len = std::min(every, n_frames - f0);
+        // states at frames f0 .. f0 + len - 1, recomputed from the checkpoint
+        if ((st = unpack_state(w, d_ckpt + static_cast<size_t>(seg) * 13 * n, cs)) != DYPH_OK) return st;
+        for (int32_t j = 0; j < len; ++j) {
+            if ((st = pack_state(w, w->a_seg + static_cast<size_t>(j) * 13 * n, cs)) != DYPH_OK) return st;
+            if (j + 1 < len && (st = dyph_world_step(w, 1, s)) != DYPH_OK) return st;
+        }
+        for (int32_t j = len - 1; j >= 0; --j) {
+            FrameParams P{state_view(w, w->a_seg + static_cast<size_t>(j) * 13 * n), d.shapes, ip.gravity[0],
+                          ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt, w->sv->friction, ip.dt,
+                          ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->meta,
+                          w->bp->counts, w->np->counts, w->stats + 4, nullptr};
+            AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
+            scene_frame_adjoint_kernel<<<w->bp->n_scenes, kSceneThreads, w->frame_smem, cs>>>(S, F, P, A, G);
+            DYPH_CUDA_TRY(cudaGetLastError());
+            cur ^= 1;
+        }
+    }
+    DYPH_CUDA_TRY(cudaMemcpyAsync(d_grad_init, w->a_g[cur], 13 * n * 4, cudaMemcpyDeviceToDevice, cs));
+    uint32_t flag = 0;
+    DYPH_CUDA_TRY(cudaMemcpyAsync(&flag, w->a_flag, 4, cudaMemcpyDeviceToHost, cs));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    return flag ? DYPH_ERR_UNSUPPORTED : DYPH_OK;
 }

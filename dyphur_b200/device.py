@@ -316,6 +316,8 @@ class World:
             self._scene_offset = off
             check(capi.lib().dyph_world_set_scenes(h, scene.n_scenes, off.ctypes.data, bnds),
                   "dyph_world_set_scenes")
+        # the state at creation (rows pos, rot, vel, ang), the start of differentiable rollouts
+        self.initial = self.bodies.fbuf[:13].clone()
         bp, np_, sv = C.c_void_p(), C.c_void_p(), C.c_void_p()
         check(capi.lib().dyph_world_broadphase(h, C.byref(bp)))
         check(capi.lib().dyph_world_narrowphase(h, C.byref(np_)))

@@ -38,7 +38,8 @@ typedef enum dyph_status {
     DYPH_ERR_NO_DEVICE = 6,        /* no CUDA device / not an sm_100 device */
     DYPH_ERR_NOMEM = 7,            /* device allocation failed */
     DYPH_ERR_NOT_FINITE = 8,       /* NaN / Inf found in body state */
-    DYPH_ERR_TOO_LARGE = 9         /* size above a fixed-scratch entry point's maximum */
+    DYPH_ERR_TOO_LARGE = 9,        /* size above a fixed-scratch entry point's maximum */
+    DYPH_ERR_UNSUPPORTED = 10      /* a path the adjoint does not differentiate (see dyph_world_rollout_backward) */
 } dyph_status;
 
 /* Mirrors BodyView (core/include/core/body.hpp:30-46). */
@@ -337,6 +338,33 @@ dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
  * and clears the sums (blocking). */
 dyph_status dyph_world_set_phase_timing(dyph_world* w, int on);
 dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s, uint64_t* out, uint32_t cap);
+/* ── adjoint: gradients through fused batched frames. No reference
+ *    counterpart: the reference has no differentiation (its docs defer it). ─
+ *
+ * dyph_world_rollout steps n_frames frames from the world's current state and
+ * stores the state at frames 0, every, 2 every, ... into d_ckpt (device,
+ * [ceil(n_frames / every)][13][n] floats, rows pos xyz, rot wxyz, vel xyz,
+ * ang xyz, as the BodyView arrays).
+ *
+ * dyph_world_rollout_backward takes d_grad_final, the adjoint of the state
+ * after the rollout ([13][n]), and returns d_grad_init, the adjoint of the
+ * state at frame 0 ([13][n]), and d_grad_inv_mass, the adjoint of every
+ * body's inverse mass ([n], overwritten; the inverse inertia is held fixed).
+ * Each checkpoint segment is recomputed forward, then every frame is reversed
+ * by one kernel launch (one thread block per scene) that recomputes the
+ * frame, records its contact set, narrowphase branches and pre-solve states,
+ * and applies the hand-written adjoints of the renormalisations, the contact
+ * solves (in reverse colour / level order), the narrowphase and the
+ * integration. The contact set and every branch are those of the forward
+ * frames. Static bodies get zero adjoints. Returns DYPH_ERR_UNSUPPORTED (the
+ * gradients are then incomplete) when a frame took a path the adjoint does
+ * not differentiate: a contact that first acted after a renormalisation
+ * (deferred at w_total < 1e-10), more than 8 substeps or 10 iterations.
+ * Fused batched worlds only; the world's body state is scratch afterwards. */
+dyph_status dyph_world_rollout(dyph_world* w, int32_t n_frames, int32_t every, float* d_ckpt, dyph_stream s);
+dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_frames, int32_t every, const float* d_ckpt,
+                                        const float* d_grad_final, float* d_grad_init, float* d_grad_inv_mass,
+                                        dyph_stream s);
 /* Blocking: FNV-1a-64 of every scene's pose arrays (one value for a single
  * scene); cap >= number of scenes. */
 dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uint64_t* host_out, uint32_t cap);

@@ -17,6 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libdyphur_oracle.so")
+DUAL_SO = os.path.join(HERE, "_build", "libdyphur_dual.so")
 REF_SO = os.path.join(HERE, "_ref", "libdyphur_ref.so")
 
 STAGE_INTEGRATE, STAGE_BROADPHASE, STAGE_NARROWPHASE, STAGE_SOLVE = 1, 2, 3, 4
@@ -37,10 +38,55 @@ class _Scene(ctypes.Structure):
 
 def build_oracle() -> str:
     """Compile the C restatement if needed (gcc only; works on any host)."""
-    src = os.path.join(HERE, "dyphur_oracle.c")
-    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("dyphur_oracle.c", "dual_oracle.cpp")]
+    stale = any(not os.path.exists(so) for so in (ORACLE_SO, DUAL_SO)) or \
+        os.path.getmtime(ORACLE_SO) < os.path.getmtime(srcs[0]) or os.path.getmtime(DUAL_SO) < os.path.getmtime(srcs[1])
+    if stale:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return ORACLE_SO
+
+
+PARAM_VEL, PARAM_ANG, PARAM_INV_MASS = 0, 3, 6
+
+
+def dual_rollout(state13, inv_mass, iI6, shape_type, half3, flags, n_frames, dt, gravity, n_substeps, n_iters, mu,
+                 params, targets, mask, at_float=False, shift_param=-1, shift=0.0):
+    """FP64 forward-mode gradient of L = Σ_{mask} |x_final - target|^2 over one
+    scene stepped n_frames frames in the sequential order (oracle/dual_oracle.cpp),
+    along the float run's contact set and branches; at_float takes the chain
+    rule's coefficients at the float values (the FP64 derivative of the float map);
+    shift_param / shift move one parameter's FP64 value only (for central differences
+    of the FP64 re-run along the same branches).
+    params: list of (kind, body), kind 0-2 velocity x/y/z, 3-5 spin x/y/z, 6 inverse mass.
+    Returns (loss, grad [len(params)], final float state [13, n], final FP64 state [13, n])."""
+    build_oracle()
+    L = ctypes.CDLL(DUAL_SO)
+    f = L.dyd_rollout
+    f.restype = ctypes.c_int
+    n = int(np.asarray(inv_mass).shape[0])
+    arrs = [np.ascontiguousarray(state13, np.float32), np.ascontiguousarray(inv_mass, np.float32),
+            np.ascontiguousarray(iI6, np.float32), np.ascontiguousarray(shape_type, np.uint32),
+            np.ascontiguousarray(half3, np.float32), np.ascontiguousarray(flags, np.uint32),
+            np.ascontiguousarray(gravity, np.float32)]
+    kind = np.ascontiguousarray([k for k, _ in params], np.int32)
+    body = np.ascontiguousarray([b for _, b in params], np.uint32)
+    tgt = np.ascontiguousarray(targets, np.float32).reshape(-1)
+    msk = np.ascontiguousarray(mask, np.uint8)
+    loss = ctypes.c_double()
+    grad = np.zeros(len(params), np.float64)
+    fin_f = np.zeros((13, n), np.float32)
+    fin_v = np.zeros((13, n), np.float64)
+    vp = ctypes.c_void_p
+    f.argtypes = [ctypes.c_uint32] + [vp] * 6 + [ctypes.c_int, ctypes.c_float, vp, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_float, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_double, vp, vp, vp, vp]
+    rc = f(n, *[a.ctypes.data for a in arrs[:6]], int(n_frames), float(dt), arrs[6].ctypes.data, int(n_substeps),
+           int(n_iters), float(mu), len(params), kind.ctypes.data, body.ctypes.data, tgt.ctypes.data,
+           msk.ctypes.data, int(bool(at_float)), int(shift_param), float(shift), ctypes.byref(loss),
+           grad.ctypes.data, fin_f.ctypes.data, fin_v.ctypes.data)
+    if rc != 0:
+        raise ValueError("too many gradient parameters for the dual-number oracle")
+    return loss.value, grad, fin_f, fin_v
 
 
 def ref_available() -> bool:
