@@ -72,6 +72,7 @@ def parse():
                     help="solver order (default: sequential for the batch, reference for the single scene)")
     ap.add_argument("--frames", type=int, default=None)
     ap.add_argument("--no-single", action="store_true", help="batch line without the single-scene object")
+    ap.add_argument("--no-adjoint", action="store_true", help="batch line without the fwd+bwd objects")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-single-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
@@ -522,6 +523,96 @@ def drift_report(scene, frames, torch) -> dict:
             "within_1e-3_m": out[frames][0] <= 1e-3}
 
 
+def _dual_error(w, scene, i, frames, g_vel, g_ang, g_im, at_float, loss_mask, scale, max_params=90):
+    """Relative error of the adjoint's gradient for scene i of a batch against
+    the FP64 dual-number oracle (oracle/dual_oracle.cpp) over the same frames;
+    the batch loss is `scale` times the sum of the scenes' masked losses."""
+    from oracle import oracle
+    b0, b1 = int(scene.body_offset[i]), int(scene.body_offset[i + 1])
+    fb = w.bodies.fbuf.cpu().numpy()
+    n = b1 - b0
+    im = fb[13, b0:b1].copy()
+    dyn = [j for j in range(n) if im[j] != 0]
+    params = [(k, dyn[-1]) for k in range(6)] + [(6, j) for j in dyn][:max_params - 6]
+    mask = loss_mask[b0:b1].astype(np.uint8)
+    tg = scene.targets[b0:b1]
+    _, g_d, _, _ = oracle.dual_rollout(np.ascontiguousarray(w.initial[:, b0:b1].cpu().numpy()), im,
+                                       np.ascontiguousarray(fb[14:20, b0:b1]), scene.shape_type[scene.shape[b0:b1]],
+                                       np.ascontiguousarray(scene.shape_half[scene.shape[b0:b1]].T),
+                                       scene.flags[b0:b1], frames, scene.dt, scene.gravity, scene.n_substeps,
+                                       scene.n_iters, scene.friction, params, tg, mask, at_float=at_float)
+    g = []
+    for k, j in params:
+        g.append(g_vel[b0 + j, k] if k < 3 else (g_ang[b0 + j, k - 3] if k < 6 else g_im[b0 + j]))
+    g = np.array(g, np.float64) / scale
+    return float(np.linalg.norm(g - g_d) / max(np.linalg.norm(g_d), 1e-30))
+
+
+def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask, reps: int = 3) -> dict:
+    """Forward rollout and forward + adjoint of a differentiable batch
+    (sequential order), loss = mean over the masked bodies of |x_final -
+    target|^2: body-steps/s of each, their ratio, the device memory the
+    adjoint keeps, and the gradient error against the FP64 oracle."""
+    from dyphur_b200 import device
+    from dyphur_b200.autograd import rollout
+    w = device.World(scene, mode=1)
+    n = scene.n_bodies
+    stream = torch.cuda.current_stream()
+    dyn = torch.from_numpy(loss_mask.astype(np.float32)).cuda()
+    scale = 1.0 / float(loss_mask.sum())
+    tgt = torch.from_numpy(scene.targets).cuda()
+
+    def once(fr):
+        vel = w.initial[7:10, :n].T.clone().requires_grad_(True)
+        ang = w.initial[10:13, :n].T.clone().requires_grad_(True)
+        im = w.bodies.fbuf[13, :n].clone().requires_grad_(True)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        fin = rollout(w, vel, ang, im, fr, every=min(every, fr))
+        e[1].record(stream)
+        pos = fin[:3].T
+        loss = (((pos - tgt) ** 2).sum(1) * dyn).sum() * scale
+        loss.backward()
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), vel.grad, ang.grad, im.grad
+
+    once(frames)  # warm-up
+    tf, tb = [], []
+    for _ in range(reps):
+        a, b, gv, ga, gm = once(frames)
+        tf.append(a)
+        tb.append(b)
+    fwd_ms, bwd_ms = statistics.median(tf), statistics.median(tb)
+    gv, ga, gm = gv.cpu().numpy(), ga.cpu().numpy(), gm.cpu().numpy()
+    per_frame = None
+    if every > 1:  # the same with a checkpoint at every frame (no segment recompute)
+        every_cfg = every
+        every = 1
+        a, b, _, _, _ = once(frames)
+        a, b, _, _, _ = once(frames)
+        per_frame = (a + b) / a
+        every = every_cfg
+    err_full = _dual_error(w, scene, 0, frames, gv, ga, gm, True, loss_mask, scale)
+    _, _, gv10, ga10, gm10 = once(10)
+    err_10 = _dual_error(w, scene, 0, 10, gv10.cpu().numpy(), ga10.cpu().numpy(), gm10.cpu().numpy(), False,
+                         loss_mask, scale)
+    n_ckpt = (frames + every - 1) // every
+    slots = int(sum(max(64, 16 * int(b) + 64) for b in np.diff(scene.body_offset)))
+    act = 4 * (n_ckpt * 13 * n + every * 13 * n + 36 * slots + (7 + 4 + 26) * n)
+    w.close()
+    return {"workload": label, "scenes": scene.n_scenes, "bodies": n, "frames": frames,
+            "checkpoint_every": every, "solver_mode": "sequential",
+            "fwd": {"value": n * frames / (fwd_ms / 1e3), "unit": METRIC, "ms": fwd_ms},
+            "fwd_bwd": {"value": n * frames / ((fwd_ms + bwd_ms) / 1e3), "unit": METRIC, "ms": fwd_ms + bwd_ms},
+            "fwd_bwd_over_fwd": (fwd_ms + bwd_ms) / fwd_ms,
+            "fwd_bwd_over_fwd_checkpoint_every_frame": per_frame,
+            "adjoint_device_bytes": act,
+            "grad_rel_err_vs_fp64": {"scene": 0, "frames_10_fp64_values": err_10,
+                                     f"frames_{frames}_fp64_at_float_values": err_full},
+            "grads": "initial velocities and spins, inverse masses (inverse inertia held fixed)"}
+
+
 def per_scene_baseline(scene, frames: int, mode: int, torch, sample: int = 32) -> dict:
     """The plain per-scene GPU path on a sample of the batch: each scene its own
     world, its frames replayed as one captured episode, scenes one after another."""
@@ -690,6 +781,20 @@ def run_b200(args) -> None:
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = batch_cpu_baseline(dict(BATCH, frames=frames))
             note("batch cpu baseline")
+        if not args.no_adjoint and world == 1:
+            push = scenes.push(256, seed=4)
+            boxes = np.zeros(push.n_bodies, bool)
+            for i in range(push.n_scenes):
+                boxes[push.body_offset[i]:push.body_offset[i] + 64] = True
+            mixed = scenes.batch_mixed(1024, 16, 512, seed=5)
+            line["adjoint"] = [
+                adjoint_report(torch, push, 120, 10,
+                               "differentiable push: 256 scenes of 64 boxes + a 5 kg pusher, loss = mean squared "
+                               "distance of the boxes' final centroids to seeded targets, 120 frames", boxes),
+                adjoint_report(torch, mixed, 60, 1,
+                               "batched fwd+bwd: 1024 scenes of 16-512 mixed boxes / spheres, loss = mean squared "
+                               "final position of every dynamic body, 60 frames", mixed.mass > 0)]
+            note("adjoint")
         if not args.no_single and world == 1:
             line["single_scene"] = single_line(args, torch, barrier, 1, 0, local, SINGLE["seed"], SINGLE["frames"],
                                                "reference", nested=True)

@@ -380,20 +380,13 @@ struct BodyBar {
 };
 
 // solve_contact on the pair (L body 0 = a, body 1 = b) from its pre-solve
-// state. G0 / G1 hold the adjoint of the post-solve state on entry and of the
-// pre-solve state on return (im accumulates); pb, nb, db receive the contact
-// geometry's adjoint. lc_in is lambda before the solve.
+// state, with the branch flags `fl` the forward solve recorded. G0 / G1 hold
+// the adjoint of the post-solve state on entry and of the pre-solve state on
+// return (im accumulates); pb, nb, db receive the contact geometry's adjoint.
+// lc_in is lambda before the solve.
 __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Contact& ct, float mu, float dt,
-                                                  float lc_in, BodyBar& G0, BodyBar& G1, F3& pb, F3& nb,
-                                                  float& db) {
-    // the forward's branches, from the same arithmetic
-    LocalPair Lf = L;
-    Contact lct = ct;
-    lct.a = 0u;
-    lct.b = 1u;
-    float lcf = lc_in;
-    uint32_t fl = 0u;
-    solve_contact(LocalPairRef{&Lf}, lct, mu, lcf, dt, &fl);
+                                                  float lc_in, uint32_t fl, BodyBar& G0, BodyBar& G1, F3& pb,
+                                                  F3& nb, float& db) {
     if (!(fl & kSfActive)) return;
     const float wa = L.m[0], wb = L.m[1];
     const bool da = wa != 0.f, dbn = wb != 0.f;

@@ -46,169 +46,189 @@ __device__ __forceinline__ float& grow(float* g, uint32_t stride, int r, uint32_
     return g[static_cast<size_t>(r) * stride + i];
 }
 
-__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_adjoint_kernel(SceneBufs S, FrameBufs F,
-                                                                               FrameParams P_, AdjRun A,
-                                                                               AdjFrame G) {
-    extern __shared__ __align__(16) unsigned char scene_smem[];
-    __shared__ SceneShared sh;
-    const BlockTeam T;
+// The adjoint of scene s's frame by team T (`smem_bytes` of shared memory at smem).
+template <class Team>
+__device__ void adjoint_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
+                              const SceneBufs& S, const FrameBufs& F, const FrameParams& P_, const AdjRun& A,
+                              const AdjFrame& G) {
     const uint32_t ns = A.n_stride, rs = A.rec_stride;
-    for (uint32_t t = blockIdx.x; t < S.n_scenes; t += gridDim.x) {
-        const uint32_t s = S.order[t];
-        const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
-        FrameOut fo{};
-        if (!frame_scene(T, s, scene_smem, S.smem_bytes, sh, S, F, P_, &A, &fo)) continue;
-        const uint32_t ldb = (nb + 3u) & ~3u;
-        float* fb = reinterpret_cast<float*>(scene_smem);
-        const SceneBodies SB{fb, ldb};
-        const SceneSolverRows R = scene_solver_rows(fb, ldb);
-        const uint32_t* info = R.cnt + ldb;
-        const float* half = reinterpret_cast<const float*>(info + ldb);
-        const SceneContacts& SC = fo.SC;
-        const uint32_t m = fo.m, cbase = F.contact_base[s];
-        // ── adjoint of the frame's end state ──
-        for (uint32_t i = T.rank(); i < nb; i += T.size())
-            for (int r = 0; r < 13; ++r) grow(G.gout, ns, r, b0 + i) = G.gin[static_cast<size_t>(r) * ns + b0 + i];
+    const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
+    FrameOut fo{};
+    if (!frame_scene(T, s, smem, smem_bytes, sh, S, F, P_, &A, &fo)) return;
+    const uint32_t ldb = (nb + 3u) & ~3u;
+    float* fb = reinterpret_cast<float*>(smem);
+    const SceneBodies SB{fb, ldb};
+    const SceneSolverRows R = scene_solver_rows(fb, ldb);
+    const uint32_t* info = R.cnt + ldb;
+    const float* half = reinterpret_cast<const float*>(info + ldb);
+    const SceneContacts& SC = fo.SC;
+    const uint32_t m = fo.m, cbase = F.contact_base[s];
+    // ── adjoint of the frame's end state ──
+    for (uint32_t i = T.rank(); i < nb; i += T.size())
+        for (int r = 0; r < 13; ++r) grow(G.gout, ns, r, b0 + i) = G.gin[static_cast<size_t>(r) * ns + b0 + i];
+    T.sync();
+    if (m > 0) {
+        // ── renormalisations: q_end = renorm^n_iters(q_sweeps) ──
+        for (uint32_t i = T.rank(); i < nb; i += T.size()) {
+            float q[4] = {A.qs[b0 + i], A.qs[ns + b0 + i], A.qs[2ull * ns + b0 + i], A.qs[3ull * ns + b0 + i]};
+            float chain[10][4];
+            const int n_it = P_.n_iters;
+            int kept = 0;
+            for (int it = 0; it < n_it && it < 10; ++it) {
+                for (int c = 0; c < 4; ++c) chain[it][c] = q[c];
+                renormalize(q[0], q[1], q[2], q[3]);
+                ++kept;
+            }
+            if (n_it > 10) atomicOr(A.flag, 2u);
+            float g[4] = {grow(G.gout, ns, 3, b0 + i), grow(G.gout, ns, 4, b0 + i), grow(G.gout, ns, 5, b0 + i),
+                          grow(G.gout, ns, 6, b0 + i)};
+            for (int it = kept - 1; it >= 0; --it) {
+                float gi[4];
+                normalize_adj(chain[it], g, gi);
+                for (int c = 0; c < 4; ++c) g[c] = gi[c];
+            }
+            for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, b0 + i) = g[c];
+        }
         T.sync();
-        if (m > 0) {
-            // ── renormalisations: q_end = renorm^n_iters(q_sweeps) ──
-            for (uint32_t i = T.rank(); i < nb; i += T.size()) {
-                float q[4] = {A.qs[b0 + i], A.qs[ns + b0 + i], A.qs[2ull * ns + b0 + i], A.qs[3ull * ns + b0 + i]};
-                float chain[10][4];
-                const int n_it = P_.n_iters;
-                int kept = 0;
-                for (int it = 0; it < n_it && it < 10; ++it) {
-                    for (int c = 0; c < 4; ++c) chain[it][c] = q[c];
-                    renormalize(q[0], q[1], q[2], q[3]);
-                    ++kept;
-                }
-                if (n_it > 10) atomicOr(A.flag, 2u);
-                float g[4] = {grow(G.gout, ns, 3, b0 + i), grow(G.gout, ns, 4, b0 + i), grow(G.gout, ns, 5, b0 + i),
-                              grow(G.gout, ns, 6, b0 + i)};
-                for (int it = kept - 1; it >= 0; --it) {
-                    float gi[4];
-                    normalize_adj(chain[it], g, gi);
-                    for (int c = 0; c < 4; ++c) g[c] = gi[c];
-                }
-                for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, b0 + i) = g[c];
-            }
-            T.sync();
-            // ── contact solves, last group first ──
-            for (int g = static_cast<int>(fo.groups) - 1; g >= 0; --g) {
-                const uint32_t end = SC.pa(g + 1);
-                for (uint32_t idx = SC.pa(g) + T.rank(); idx < end; idx += T.size()) {
-                    const uint32_t k = SC.ent(idx);
-                    const float* r = A.rec + cbase + k;
-                    if (r[35ull * rs] == 0.f) continue;  // did not act
-                    const Contact ct = SC.contact(k);
-                    const uint32_t ia = ct.a, ib = ct.b;
-                    LocalPair L;
-                    for (int j = 0; j < 2; ++j) {
-                        const uint32_t bi = j ? ib : ia;
-                        const int o = j ? 13 : 0;
-                        for (int c = 0; c < 3; ++c) L.p[j][c] = r[static_cast<size_t>(o + c) * rs];
-                        for (int c = 0; c < 4; ++c) L.q[j][c] = r[static_cast<size_t>(o + 3 + c) * rs];
-                        for (int c = 0; c < 3; ++c) L.v[j][c] = r[static_cast<size_t>(o + 7 + c) * rs];
-                        for (int c = 0; c < 3; ++c) L.w[j][c] = r[static_cast<size_t>(o + 10 + c) * rs];
-                        L.m[j] = SB.im(bi);
-                        L.I[j][0] = SB.ixx(bi); L.I[j][1] = SB.iyy(bi); L.I[j][2] = SB.izz(bi);
-                        L.I[j][3] = SB.ixy(bi); L.I[j][4] = SB.ixz(bi); L.I[j][5] = SB.iyz(bi);
-                    }
-                    BodyBar G0, G1;
-                    BodyBar* Gs[2] = {&G0, &G1};
-                    for (int j = 0; j < 2; ++j) {
-                        const uint32_t gi = b0 + (j ? ib : ia);
-                        BodyBar& Gj = *Gs[j];
-                        Gj.x = f3(grow(G.gout, ns, 0, gi), grow(G.gout, ns, 1, gi), grow(G.gout, ns, 2, gi));
-                        for (int c = 0; c < 4; ++c) Gj.q[c] = grow(G.gout, ns, 3 + c, gi);
-                        Gj.v = f3(grow(G.gout, ns, 7, gi), grow(G.gout, ns, 8, gi), grow(G.gout, ns, 9, gi));
-                        Gj.w = f3(grow(G.gout, ns, 10, gi), grow(G.gout, ns, 11, gi), grow(G.gout, ns, 12, gi));
-                        Gj.im = 0.f;
-                    }
-                    F3 pb = f3(0.f, 0.f, 0.f), nb3 = pb;
-                    float db = 0.f;
-                    solve_contact_adj(L, ct, P_.mu, P_.dt, r[26ull * rs], G0, G1, pb, nb3, db);
-                    for (int j = 0; j < 2; ++j) {
-                        if (L.m[j] == 0.f) continue;  // a static body's state is not a variable
-                        const uint32_t gi = b0 + (j ? ib : ia);
-                        const BodyBar& Gj = *Gs[j];
-                        grow(G.gout, ns, 0, gi) = Gj.x.x; grow(G.gout, ns, 1, gi) = Gj.x.y;
-                        grow(G.gout, ns, 2, gi) = Gj.x.z;
-                        for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, gi) = Gj.q[c];
-                        grow(G.gout, ns, 7, gi) = Gj.v.x; grow(G.gout, ns, 8, gi) = Gj.v.y;
-                        grow(G.gout, ns, 9, gi) = Gj.v.z;
-                        grow(G.gout, ns, 10, gi) = Gj.w.x; grow(G.gout, ns, 11, gi) = Gj.w.y;
-                        grow(G.gout, ns, 12, gi) = Gj.w.z;
-                        G.gim[gi] += Gj.im;
-                    }
-                    float* w = A.rec + cbase + k;
-                    w[28ull * rs] = pb.x; w[29ull * rs] = pb.y; w[30ull * rs] = pb.z;
-                    w[31ull * rs] = nb3.x; w[32ull * rs] = nb3.y; w[33ull * rs] = nb3.z;
-                    w[34ull * rs] = db;
-                }
-                T.sync();
-            }
-            // ── narrowphase: geometry adjoints -> poses after integrate ──
-            for (uint32_t k = T.rank(); k < m; k += T.size()) {
+        // ── contact solves, last group first ──
+        for (int g = static_cast<int>(fo.groups) - 1; g >= 0; --g) {
+            const uint32_t end = SC.pa(g + 1);
+            for (uint32_t idx = SC.pa(g) + T.rank(); idx < end; idx += T.size()) {
+                const uint32_t k = SC.ent(idx);
                 const float* r = A.rec + cbase + k;
-                if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
+                if (r[35ull * rs] == 0.f) continue;  // did not act
                 const Contact ct = SC.contact(k);
                 const uint32_t ia = ct.a, ib = ct.b;
-                const uint32_t ga = b0 + ia, gbi = b0 + ib;
-                const F3 xa = f3(A.pose1[ga], A.pose1[ns + ga], A.pose1[2ull * ns + ga]);
-                const F3 xb = f3(A.pose1[gbi], A.pose1[ns + gbi], A.pose1[2ull * ns + gbi]);
-                const float qa[4] = {A.pose1[3ull * ns + ga], A.pose1[4ull * ns + ga], A.pose1[5ull * ns + ga],
-                                     A.pose1[6ull * ns + ga]};
-                const float qb[4] = {A.pose1[3ull * ns + gbi], A.pose1[4ull * ns + gbi], A.pose1[5ull * ns + gbi],
-                                     A.pose1[6ull * ns + gbi]};
-                const float ha[3] = {half[ia], half[ldb + ia], half[2 * ldb + ia]};
-                const float hb[3] = {half[ib], half[ldb + ib], half[2 * ldb + ib]};
-                F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
-                float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
-                process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
-                                 __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
-                                 f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
-                                 f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
-                if (SB.im(ia) != 0.f) {
-                    atomicAdd(&grow(G.gout, ns, 0, ga), xab.x);
-                    atomicAdd(&grow(G.gout, ns, 1, ga), xab.y);
-                    atomicAdd(&grow(G.gout, ns, 2, ga), xab.z);
-                    for (int c = 0; c < 4; ++c) atomicAdd(&grow(G.gout, ns, 3 + c, ga), qab[c]);
+                LocalPair L;
+                for (int j = 0; j < 2; ++j) {
+                    const uint32_t bi = j ? ib : ia;
+                    const int o = j ? 13 : 0;
+                    for (int c = 0; c < 3; ++c) L.p[j][c] = r[static_cast<size_t>(o + c) * rs];
+                    for (int c = 0; c < 4; ++c) L.q[j][c] = r[static_cast<size_t>(o + 3 + c) * rs];
+                    for (int c = 0; c < 3; ++c) L.v[j][c] = r[static_cast<size_t>(o + 7 + c) * rs];
+                    for (int c = 0; c < 3; ++c) L.w[j][c] = r[static_cast<size_t>(o + 10 + c) * rs];
+                    L.m[j] = SB.im(bi);
+                    L.I[j][0] = SB.ixx(bi); L.I[j][1] = SB.iyy(bi); L.I[j][2] = SB.izz(bi);
+                    L.I[j][3] = SB.ixy(bi); L.I[j][4] = SB.ixz(bi); L.I[j][5] = SB.iyz(bi);
                 }
-                if (SB.im(ib) != 0.f) {
-                    atomicAdd(&grow(G.gout, ns, 0, gbi), xbb.x);
-                    atomicAdd(&grow(G.gout, ns, 1, gbi), xbb.y);
-                    atomicAdd(&grow(G.gout, ns, 2, gbi), xbb.z);
-                    for (int c = 0; c < 4; ++c) atomicAdd(&grow(G.gout, ns, 3 + c, gbi), qbb[c]);
+                BodyBar G0, G1;
+                BodyBar* Gs[2] = {&G0, &G1};
+                for (int j = 0; j < 2; ++j) {
+                    const uint32_t gi = b0 + (j ? ib : ia);
+                    BodyBar& Gj = *Gs[j];
+                    Gj.x = f3(grow(G.gout, ns, 0, gi), grow(G.gout, ns, 1, gi), grow(G.gout, ns, 2, gi));
+                    for (int c = 0; c < 4; ++c) Gj.q[c] = grow(G.gout, ns, 3 + c, gi);
+                    Gj.v = f3(grow(G.gout, ns, 7, gi), grow(G.gout, ns, 8, gi), grow(G.gout, ns, 9, gi));
+                    Gj.w = f3(grow(G.gout, ns, 10, gi), grow(G.gout, ns, 11, gi), grow(G.gout, ns, 12, gi));
+                    Gj.im = 0.f;
                 }
+                F3 pb = f3(0.f, 0.f, 0.f), nb3 = pb;
+                float db = 0.f;
+                solve_contact_adj(L, ct, P_.mu, P_.dt, r[26ull * rs], __float_as_uint(r[35ull * rs]), G0, G1, pb,
+                                  nb3, db);
+                for (int j = 0; j < 2; ++j) {
+                    if (L.m[j] == 0.f) continue;  // a static body's state is not a variable
+                    const uint32_t gi = b0 + (j ? ib : ia);
+                    const BodyBar& Gj = *Gs[j];
+                    grow(G.gout, ns, 0, gi) = Gj.x.x; grow(G.gout, ns, 1, gi) = Gj.x.y;
+                    grow(G.gout, ns, 2, gi) = Gj.x.z;
+                    for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, gi) = Gj.q[c];
+                    grow(G.gout, ns, 7, gi) = Gj.v.x; grow(G.gout, ns, 8, gi) = Gj.v.y;
+                    grow(G.gout, ns, 9, gi) = Gj.v.z;
+                    grow(G.gout, ns, 10, gi) = Gj.w.x; grow(G.gout, ns, 11, gi) = Gj.w.y;
+                    grow(G.gout, ns, 12, gi) = Gj.w.z;
+                    G.gim[gi] += Gj.im;
+                }
+                float* w = A.rec + cbase + k;
+                w[28ull * rs] = pb.x; w[29ull * rs] = pb.y; w[30ull * rs] = pb.z;
+                w[31ull * rs] = nb3.x; w[32ull * rs] = nb3.y; w[33ull * rs] = nb3.z;
+                w[34ull * rs] = db;
             }
             T.sync();
         }
-        // ── integration, from the state at the frame's start ──
-        const GlobalBodies B0{P_.gb};
-        for (uint32_t i = T.rank(); i < nb; i += T.size()) {
-            const uint32_t gi = b0 + i;
-            if (SB.im(i) == 0.f) {
-                for (int r = 0; r < 13; ++r) grow(G.gout, ns, r, gi) = 0.f;
-                continue;
+        // ── narrowphase: geometry adjoints -> poses after integrate ──
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
+            const float* r = A.rec + cbase + k;
+            if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
+            const Contact ct = SC.contact(k);
+            const uint32_t ia = ct.a, ib = ct.b;
+            const uint32_t ga = b0 + ia, gbi = b0 + ib;
+            const F3 xa = f3(A.pose1[ga], A.pose1[ns + ga], A.pose1[2ull * ns + ga]);
+            const F3 xb = f3(A.pose1[gbi], A.pose1[ns + gbi], A.pose1[2ull * ns + gbi]);
+            const float qa[4] = {A.pose1[3ull * ns + ga], A.pose1[4ull * ns + ga], A.pose1[5ull * ns + ga],
+                                 A.pose1[6ull * ns + ga]};
+            const float qb[4] = {A.pose1[3ull * ns + gbi], A.pose1[4ull * ns + gbi], A.pose1[5ull * ns + gbi],
+                                 A.pose1[6ull * ns + gbi]};
+            const float ha[3] = {half[ia], half[ldb + ia], half[2 * ldb + ia]};
+            const float hb[3] = {half[ib], half[ldb + ib], half[2 * ldb + ib]};
+            F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
+            float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
+            process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
+                             __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
+                             f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
+                             f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
+            if (SB.im(ia) != 0.f) {
+                atomicAdd(&grow(G.gout, ns, 0, ga), xab.x);
+                atomicAdd(&grow(G.gout, ns, 1, ga), xab.y);
+                atomicAdd(&grow(G.gout, ns, 2, ga), xab.z);
+                for (int c = 0; c < 4; ++c) atomicAdd(&grow(G.gout, ns, 3 + c, ga), qab[c]);
             }
-            if ((info[i] >> 8) & kFlagSleeping) continue;  // not integrated: identity
-            const Pose p0{B0.px(gi), B0.py(gi), B0.pz(gi), B0.qw(gi), B0.qx(gi), B0.qy(gi), B0.qz(gi),
-                          B0.vx(gi), B0.vy(gi), B0.vz(gi)};
-            F3 xb = f3(grow(G.gout, ns, 0, gi), grow(G.gout, ns, 1, gi), grow(G.gout, ns, 2, gi));
-            float qb[4] = {grow(G.gout, ns, 3, gi), grow(G.gout, ns, 4, gi), grow(G.gout, ns, 5, gi),
-                           grow(G.gout, ns, 6, gi)};
-            F3 vb = f3(grow(G.gout, ns, 7, gi), grow(G.gout, ns, 8, gi), grow(G.gout, ns, 9, gi));
-            F3 wb = f3(grow(G.gout, ns, 10, gi), grow(G.gout, ns, 11, gi), grow(G.gout, ns, 12, gi));
-            if (!integrate_body_adj(p0, B0.wx(gi), B0.wy(gi), B0.wz(gi), P_.gx, P_.gy, P_.gz, P_.sub_dt, P_.half_dt,
-                                    P_.n_substeps, xb, qb, vb, wb))
-                atomicOr(A.flag, 4u);
-            grow(G.gout, ns, 0, gi) = xb.x; grow(G.gout, ns, 1, gi) = xb.y; grow(G.gout, ns, 2, gi) = xb.z;
-            for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, gi) = qb[c];
-            grow(G.gout, ns, 7, gi) = vb.x; grow(G.gout, ns, 8, gi) = vb.y; grow(G.gout, ns, 9, gi) = vb.z;
-            grow(G.gout, ns, 10, gi) = wb.x; grow(G.gout, ns, 11, gi) = wb.y; grow(G.gout, ns, 12, gi) = wb.z;
+            if (SB.im(ib) != 0.f) {
+                atomicAdd(&grow(G.gout, ns, 0, gbi), xbb.x);
+                atomicAdd(&grow(G.gout, ns, 1, gbi), xbb.y);
+                atomicAdd(&grow(G.gout, ns, 2, gbi), xbb.z);
+                for (int c = 0; c < 4; ++c) atomicAdd(&grow(G.gout, ns, 3 + c, gbi), qbb[c]);
+            }
         }
         T.sync();
+    }
+    // ── integration, from the state at the frame's start ──
+    const GlobalBodies B0{P_.gb};
+    for (uint32_t i = T.rank(); i < nb; i += T.size()) {
+        const uint32_t gi = b0 + i;
+        if (SB.im(i) == 0.f) {
+            for (int r = 0; r < 13; ++r) grow(G.gout, ns, r, gi) = 0.f;
+            continue;
+        }
+        if ((info[i] >> 8) & kFlagSleeping) continue;  // not integrated: identity
+        const Pose p0{B0.px(gi), B0.py(gi), B0.pz(gi), B0.qw(gi), B0.qx(gi), B0.qy(gi), B0.qz(gi),
+                      B0.vx(gi), B0.vy(gi), B0.vz(gi)};
+        F3 xb = f3(grow(G.gout, ns, 0, gi), grow(G.gout, ns, 1, gi), grow(G.gout, ns, 2, gi));
+        float qb[4] = {grow(G.gout, ns, 3, gi), grow(G.gout, ns, 4, gi), grow(G.gout, ns, 5, gi),
+                       grow(G.gout, ns, 6, gi)};
+        F3 vb = f3(grow(G.gout, ns, 7, gi), grow(G.gout, ns, 8, gi), grow(G.gout, ns, 9, gi));
+        F3 wb = f3(grow(G.gout, ns, 10, gi), grow(G.gout, ns, 11, gi), grow(G.gout, ns, 12, gi));
+        if (!integrate_body_adj(p0, B0.wx(gi), B0.wy(gi), B0.wz(gi), P_.gx, P_.gy, P_.gz, P_.sub_dt, P_.half_dt,
+                                P_.n_substeps, xb, qb, vb, wb))
+            atomicOr(A.flag, 4u);
+        grow(G.gout, ns, 0, gi) = xb.x; grow(G.gout, ns, 1, gi) = xb.y; grow(G.gout, ns, 2, gi) = xb.z;
+        for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, gi) = qb[c];
+        grow(G.gout, ns, 7, gi) = vb.x; grow(G.gout, ns, 8, gi) = vb.y; grow(G.gout, ns, 9, gi) = vb.z;
+        grow(G.gout, ns, 10, gi) = wb.x; grow(G.gout, ns, 11, gi) = wb.y; grow(G.gout, ns, 12, gi) = wb.z;
+    }
+    T.sync();
+}
+
+// Work items as for scene_frame_kernel: a large scene per block, or up to
+// four small scenes, one per warp.
+__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_adjoint_kernel(SceneBufs S, FrameBufs F,
+                                                                               FrameParams P_, AdjRun A,
+                                                                               AdjFrame G,
+                                                                               const uint32_t* __restrict__ items,
+                                                                               uint32_t n_items) {
+    extern __shared__ __align__(16) unsigned char scene_smem[];
+    __shared__ SceneShared sh[kSceneThreads / 32];
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t share = (S.smem_bytes / 4u) & ~15u;
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+        if (items[4 * it + 1] == kItemBlock) {
+            adjoint_scene(BlockTeam{}, items[4 * it], scene_smem, S.smem_bytes, sh[0], S, F, P_, A, G);
+        } else {
+            const uint32_t s = items[4 * it + warp];
+            if (s != kItemEmpty)
+                adjoint_scene(WarpTeam{}, s, scene_smem + warp * share, share, sh[warp], S, F, P_, A, G);
+        }
+        __syncthreads();
     }
 }
 

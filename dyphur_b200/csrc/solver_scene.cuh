@@ -224,7 +224,8 @@ constexpr int kRecWords = 36;  // per-contact record rows (see SolveRecord)
 struct SolveRecord {
     // rows r of contact k at rec[r * stride + base + k]: 0-12 body a state,
     // 13-25 body b state, 26 lambda before, 27 narrowphase branch word,
-    // 28-34 contact geometry adjoint (point, normal, depth), 35 acted
+    // 28-34 contact geometry adjoint (point, normal, depth), 35 the solve's
+    // branch flags (bits of a float; 0 when the contact did not act)
     float* rec;
     uint32_t stride, base;
     float* qs;           // [4][qs_stride] quaternions after the sweeps, at body b0 + i
@@ -261,7 +262,7 @@ __device__ void scene_sweep(const Team& T, uint32_t groups, const SceneBodies& S
                 if (solve_contact(SB, ct, mu, lc, dt, &fl) == kSolveDeferred) *s_flag = 1;
                 if (fl & kSfActive) {
                     r[26ull * rec->stride] = lc0;
-                    r[35ull * rec->stride] = 1.f;
+                    r[35ull * rec->stride] = __uint_as_float(fl);
                     if (iter > 0) atomicOr(rec->flag, 1u);  // acted after a renormalisation
                 } else if (iter == 0) {
                     r[35ull * rec->stride] = 0.f;

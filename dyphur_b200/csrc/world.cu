@@ -733,7 +733,8 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
                           ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->meta,
                           w->bp->counts, w->np->counts, w->stats + 4, nullptr};
             AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
-            scene_frame_adjoint_kernel<<<w->bp->n_scenes, kSceneThreads, w->frame_smem, cs>>>(S, F, P, A, G);
+            scene_frame_adjoint_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, cs>>>(S, F, P, A, G, w->f_items,
+                                                                                          w->f_n_items);
             DYPH_CUDA_TRY(cudaGetLastError());
             cur ^= 1;
         }
