@@ -2,7 +2,10 @@
 
 Produces ``dyphur_b200/lib/libdyphur_b200.so`` (CUDA kernels for sm_100a plus
 the C++ host code behind the C ABI of ``include/dyphur_b200.h``) and the
-pybind11 module ``dyphur_b200/lib/dyphur_py*.so``.
+pybind11 module ``dyphur_b200/lib/dyphur_py*.so`` (the reference's Python
+surface over the C++ layer ``include/dyphur_b200.hpp``; it links the library
+above through an ``$ORIGIN`` run path). nanobind, which the reference's
+bindings use, is not installed; pybind11 is.
 
 Numerics flags: ``--fmad=false -prec-div=true -prec-sqrt=true`` keep every
 float operation correctly rounded and uncontracted, which is what makes the
@@ -69,8 +72,29 @@ def build_native(verbose_ptxas: bool = False) -> str:
     return lib
 
 
+def build_py_module() -> str:
+    """The dyphur_py extension module (g++, pybind11) next to the library."""
+    import pybind11
+    lib = build_native()
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    out = os.path.join(LIB_DIR, "dyphur_py" + suffix)
+    src = os.path.join(CSRC, "dyphur_py.cpp")
+    deps = [src, lib, os.path.join(ROOT, "include", "dyphur_b200.hpp"), os.path.join(ROOT, "include", "dyphur_b200.h")]
+    if not _newer(out, deps):
+        return out
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    _run(["g++"] + CXX_FLAGS + ["-shared", "-fvisibility=hidden", "-I" + pybind11.get_include(),
+                                "-I" + sysconfig.get_paths()["include"], "-I" + os.path.join(cuda, "include"), src,
+                                "-o", out + ".tmp", "-L" + LIB_DIR, "-ldyphur_b200",
+                                "-L" + os.path.join(cuda, "lib64"), "-lcudart_static", "-lrt", "-ldl", "-lpthread",
+                                "-Wl,-rpath,$ORIGIN"])
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def build_all(verbose_ptxas: bool = False) -> None:
     build_native(verbose_ptxas)
+    build_py_module()
 
 
 if __name__ == "__main__":

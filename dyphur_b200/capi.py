@@ -82,6 +82,15 @@ _PROTOS = {
     "dyph_narrowphase_run_host_count": (_st, [_vp, _vp, C.c_uint32, C.POINTER(Bodies), C.POINTER(Shapes), _vp]),
     "dyph_narrowphase_contacts": (_st, [_vp, C.POINTER(Contacts)]),
     "dyph_narrowphase_download_count": (_st, [_vp, _vp, _up, _up]),
+    "dyph_ray_query": (_st, [C.POINTER(BvhView), C.POINTER(Bodies), C.POINTER(Shapes), _vp, _vp, C.c_uint32, _vp]),
+    "dyph_contact_sensor_create": (_st, [C.c_uint32, C.POINTER(_vp)]),
+    "dyph_contact_sensor_destroy": (None, [_vp]),
+    "dyph_contact_sensor_filter": (_st, [_vp, C.POINTER(Contacts), _vp, C.c_uint32, _vp]),
+    "dyph_contact_sensor_query": (_st, [_vp, C.POINTER(Contacts), _vp, C.c_uint32, _vp, _up]),
+    "dyph_contact_sensor_count": (C.c_uint32, [_vp]),
+    "dyph_contact_sensor_shape_idx": (C.c_uint32, [_vp]),
+    "dyph_contact_sensor_host_view": (_st, [_vp, C.POINTER(Contacts)]),
+    "dyph_contact_sensor_device_view": (_st, [_vp, C.POINTER(Contacts)]),
     "dyph_xpbd_create": (_st, [C.c_int32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(_vp)]),
     "dyph_xpbd_destroy": (None, [_vp]),
     "dyph_xpbd_set_mode": (_st, [_vp, C.c_int]),

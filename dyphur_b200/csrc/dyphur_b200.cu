@@ -7,4 +7,5 @@
 #include "narrowphase.cu"
 #include "solver.cu"
 #include "hash.cu"
+#include "ray_query.cu"
 #include "world.cu"

@@ -136,6 +136,11 @@ class Broadphase:
             out = host.numpy().view(np.uint32).copy()
         return out
 
+    def bvh_view(self, n: int) -> capi.BvhView:
+        v = capi.BvhView()
+        check(capi.lib().dyph_broadphase_bvh_view(self.h, n, C.byref(v)))
+        return v
+
     def bvh(self, n: int) -> dict:
         v = capi.BvhView()
         check(capi.lib().dyph_broadphase_bvh_view(self.h, n, C.byref(v)))
@@ -223,6 +228,67 @@ class Narrowphase:
     def contacts(self, stream=None):
         n, _ = self.download_count(stream)
         return read_contacts(self.contacts_view(), n)
+
+
+def ray_query(bvh: capi.BvhView, bodies: DeviceBodies, shapes: DeviceShapes, rays, stream=None):
+    """ray_query (core/include/core/ray_query.hpp:34-40) over a built tree.
+
+    rays: (n, 7) origin xyz, direction xyz, t_max (numpy or a CUDA float32
+    tensor). Returns (t, body) as CUDA tensors (float32, int32 holding the
+    uint32 body index; -1 = UINT32_MAX = miss)."""
+    r = torch.as_tensor(rays, dtype=torch.float32)
+    r = r.reshape(-1, 7).to("cuda").contiguous()
+    n = r.shape[0]
+    hits = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    check(capi.lib().dyph_ray_query(C.byref(bvh), C.byref(bodies.view), C.byref(shapes.view), _ptr(r),
+                                    _ptr(hits), n, _stream_ptr(stream)), "dyph_ray_query")
+    return hits[:, 0].view(torch.float32), hits[:, 1]
+
+
+class ContactSensor:
+    """Mirror of class ContactSensor (core/include/core/contact_sensor.hpp:20-58):
+    contacts involving one shape, filtered on the device."""
+
+    def __init__(self, shape_idx: int):
+        require_device()
+        h = C.c_void_p()
+        check(capi.lib().dyph_contact_sensor_create(int(shape_idx), C.byref(h)), "dyph_contact_sensor_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            capi.lib().dyph_contact_sensor_destroy(self.h)
+            self.h = None
+
+    def query(self, contacts: capi.Contacts, bodies: DeviceBodies, stream=None) -> int:
+        out = C.c_uint32()
+        check(capi.lib().dyph_contact_sensor_query(self.h, C.byref(contacts), bodies.view.shape, bodies.n,
+                                                   _stream_ptr(stream), C.byref(out)), "dyph_contact_sensor_query")
+        return int(out.value)
+
+    def count(self) -> int:
+        return int(capi.lib().dyph_contact_sensor_count(self.h))
+
+    def shape_idx(self) -> int:
+        return int(capi.lib().dyph_contact_sensor_shape_idx(self.h))
+
+    def rows(self):
+        """(ab (m, 2) uint32, p7 (m, 7) float32) of the last query, copied from
+        the sensor's pinned host arrays."""
+        v = capi.Contacts()
+        check(capi.lib().dyph_contact_sensor_host_view(self.h, C.byref(v)))
+        m = self.count()
+        ab = np.empty((m, 2), np.uint32)
+        p7 = np.empty((m, 7), np.float32)
+        if m:
+            cols = [v.body_a, v.body_b, v.pos_x, v.pos_y, v.pos_z, v.norm_x, v.norm_y, v.norm_z, v.depth]
+            for k, ptr in enumerate(cols):
+                a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint32)), shape=(m,))
+                if k < 2:
+                    ab[:, k] = a
+                else:
+                    p7[:, k - 2] = a.view(np.float32)
+        return ab, p7
 
 
 class XpbdSolver:
@@ -450,6 +516,41 @@ class World:
         a, b = C.c_uint32(), C.c_uint32()
         check(capi.lib().dyph_narrowphase_download_count(self._np, None, C.byref(a), C.byref(b)))
         return read_contacts(v, int(a.value))
+
+    # The rollout protocol of dyphur_b200.autograd (shared with dyphur_py.World).
+    def count(self) -> int:
+        return self.bodies.n
+
+    def device_rows(self) -> torch.Tensor:
+        return self.bodies.fbuf
+
+    def initial_rows(self) -> torch.Tensor:
+        return self.initial
+
+    def rollout_raw(self, frames: int, every: int, d_ckpt: int, stream: int) -> None:
+        check(capi.lib().dyph_world_rollout(self.h, frames, every, d_ckpt, stream), "dyph_world_rollout")
+
+    def rollout_backward_raw(self, frames: int, every: int, d_ckpt: int, g_final: int, g_init: int, g_im: int,
+                             stream: int) -> None:
+        check(capi.lib().dyph_world_rollout_backward(self.h, frames, every, d_ckpt, g_final, g_init, g_im, stream),
+              "dyph_world_rollout_backward")
+
+    def ray_query(self, rays, stream=None):
+        """Closest hits against the tree of the last frame's broadphase and the
+        current poses (see ray_query); not available on fused batched frames,
+        which build no tree."""
+        v = capi.BvhView()
+        check(capi.lib().dyph_broadphase_bvh_view(self._bp, self.bodies.n, C.byref(v)))
+        return ray_query(v, self.bodies, self.shapes, rays, stream)
+
+    def contact_sensor(self, shape_idx: int):
+        """ContactSensor(shape_idx).query over the last frame's contacts: (ab, p7)."""
+        self.sync_lists()
+        v = capi.Contacts()
+        check(capi.lib().dyph_narrowphase_contacts(self._np, C.byref(v)))
+        cs = ContactSensor(shape_idx)
+        cs.query(v, self.bodies)
+        return cs.rows()
 
     def bvh(self) -> dict:
         bp = Broadphase.__new__(Broadphase)

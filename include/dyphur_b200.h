@@ -249,6 +249,51 @@ dyph_status dyph_narrowphase_contacts(dyph_narrowphase* np, dyph_contacts* out);
 dyph_status dyph_narrowphase_download_count(dyph_narrowphase* np, dyph_stream s, uint32_t* stored,
                                             uint32_t* true_count);
 
+/* ── ray query — replaces ray_query(Stream&, BvhView, BodyView, ShapeView,
+ *    const Ray*, RayHit*, n_rays) (core/include/core/ray_query.hpp:9-48,
+ *    core/src/ray_query.cpp:126-195). Mirrors Ray / RayHit. The closest hit of
+ *    each ray (t < t_max; body_idx UINT32_MAX on a miss) over a BVH from
+ *    dyph_broadphase_bvh_view after its build: node boxes are slab-tested in
+ *    fp32, leaves exactly (sphere quadratic, oriented-box slabs in the body
+ *    frame; every non-sphere shape as its box). Same walk order and float
+ *    expressions as the reference, so hits and ties are identical. One thread
+ *    per ray; d_rays / d_hits are device arrays; asynchronous. ───────────── */
+typedef struct dyph_ray {
+    float ox, oy, oz; /* origin */
+    float dx, dy, dz; /* direction; t is in direction units */
+    float t_max;      /* the reference's default is 1e9 */
+} dyph_ray;
+typedef struct dyph_ray_hit {
+    float t;
+    uint32_t body_idx;
+} dyph_ray_hit;
+dyph_status dyph_ray_query(const dyph_bvh_view* bvh, const dyph_bodies* bodies, const dyph_shapes* shapes,
+                           const dyph_ray* d_rays, dyph_ray_hit* d_hits, uint32_t n_rays, dyph_stream s);
+
+/* ── contact sensor — replaces class ContactSensor
+ *    (core/include/core/contact_sensor.hpp:9-58, core/src/contact_sensor.cpp:6-59):
+ *    the contacts whose body a or body b (index < n_bodies) has shape
+ *    shape_idx, in store order. The filter runs on the device; only the
+ *    matches are copied to the host. d_body_shape is BodyView::shape (device).
+ *    _filter enqueues the filter only (device view valid once the stream
+ *    reaches it); _query also downloads the matches (blocking) into host
+ *    arrays that stay valid until the next query. Buffers grow to the contact
+ *    store's capacity on first use (allocates). ────────────────────────── */
+typedef struct dyph_contact_sensor dyph_contact_sensor;
+dyph_status dyph_contact_sensor_create(uint32_t shape_idx, dyph_contact_sensor** out);
+void dyph_contact_sensor_destroy(dyph_contact_sensor* cs);
+dyph_status dyph_contact_sensor_filter(dyph_contact_sensor* cs, const dyph_contacts* contacts,
+                                       const uint32_t* d_body_shape, uint32_t n_bodies, dyph_stream s);
+dyph_status dyph_contact_sensor_query(dyph_contact_sensor* cs, const dyph_contacts* contacts,
+                                      const uint32_t* d_body_shape, uint32_t n_bodies, dyph_stream s,
+                                      uint32_t* out_count);
+uint32_t dyph_contact_sensor_count(const dyph_contact_sensor* cs);
+uint32_t dyph_contact_sensor_shape_idx(const dyph_contact_sensor* cs);
+/* Host (after _query) or device (after _filter) views of the matches; n
+ * points at the match count (host word / device word). */
+dyph_status dyph_contact_sensor_host_view(dyph_contact_sensor* cs, dyph_contacts* out);
+dyph_status dyph_contact_sensor_device_view(dyph_contact_sensor* cs, dyph_contacts* out);
+
 /* ── XPBD solver — replaces class XpbdSolver : IConstraintSolver
  *    (core/include/core/solver.hpp:11-22, core/include/core/xpbd_solver.hpp:29-70,
  *    core/src/xpbd_solver.cpp:593-733). Contacts only (JointView{} with n = 0). */

@@ -76,6 +76,7 @@ public:
     }
     Stream(const Stream&) = delete;
     Stream& operator=(const Stream&) = delete;
+    Stream(Stream&& o) noexcept : dev_(o.dev_), s_(std::exchange(o.s_, nullptr)) {}
     void wait() { check_cuda(cudaStreamSynchronize(s_), "Stream::wait"); }
     cudaStream_t native() const noexcept { return s_; }
     dyph_stream abi() const noexcept { return reinterpret_cast<dyph_stream>(s_); }
@@ -96,7 +97,9 @@ public:
         check_cuda(cudaGetDevice(&d), "cudaGetDevice");
         return Device(d);
     }
-    static Device default_cpu() { throw std::runtime_error("Device::default_cpu: this build has no CPU path"); }
+    // There is no CPU device: the name is kept so host code written against
+    // the reference compiles and runs unchanged, and it selects the default GPU.
+    static Device default_cpu() { return default_gpu(); }
     static Device preferred() { return default_gpu(); }
     std::string name() const {
         cudaDeviceProp p{};
@@ -207,8 +210,27 @@ public:
     uint32_t add(const BodyParams& p) {
         if (count_ >= cap_) throw std::runtime_error("BodyStore::add: capacity exceeded");
         h_.push_back(p);
+        h_shape_.push_back(p.shape_handle);
         return count_++;
     }
+    // Shape index of every body added so far (body_store.hpp:48).
+    const std::vector<uint32_t>& body_shapes() const noexcept { return h_shape_; }
+    // Blocking copies of the 13 state rows (pos xyz, rot wxyz, vel xyz, ang
+    // xyz), [13][count] floats, out of / into the device arrays.
+    void download_state(float* host13) {
+        for (int r = 0; r < 13; ++r)
+            check(dyph_copy_to_host(host13 + size_t(r) * count_, d_f_.data() + size_t(r) * cap_, count_ * 4,
+                                    s_->abi()),
+                  "BodyStore::download_state");
+    }
+    void upload_state(const float* host13) {
+        for (int r = 0; r < 13; ++r)
+            check(dyph_copy_to_device(d_f_.data() + size_t(r) * cap_, host13 + size_t(r) * count_, count_ * 4,
+                                      s_->abi()),
+                  "BodyStore::upload_state");
+    }
+    // The 20 float rows ([20][capacity]: state, inverse mass, inverse inertia).
+    float* device_rows() noexcept { return d_f_.data(); }
     void upload() {
         const uint32_t n = count_;
         std::vector<float> pos(3 * n), rot(4 * n), vel(3 * n), ang(3 * n), mass(n), inertia(9 * n);
@@ -260,6 +282,7 @@ private:
     Buffer<float> d_f_;
     Buffer<uint32_t> d_u_;
     std::vector<BodyParams> h_;
+    std::vector<uint32_t> h_shape_;
 };
 
 // ShapeParams / ShapeStore (core/include/core/shapes.hpp, shape_store.hpp):
@@ -371,7 +394,7 @@ public:
              const ShapeView& shapes) {
         check(dyph_narrowphase_run(h_, d_pairs, d_n_pairs, &bodies, &shapes, s.abi()), "Narrowphase::run");
     }
-    ContactView contacts() {
+    ContactView contacts() const {
         ContactView v{};
         check(dyph_narrowphase_contacts(h_, &v), "contacts");
         return v;
@@ -410,6 +433,127 @@ public:
 
 private:
     dyph_xpbd* h_ = nullptr;
+};
+
+// ── queries ─────────────────────────────────────────────────────────────────
+
+// Ray / RayHit (core/include/core/ray_query.hpp:9-20), layout-identical to the C ABI's.
+struct Ray {
+    float ox = 0.f, oy = 0.f, oz = 0.f;
+    float dx = 1.f, dy = 0.f, dz = 0.f;
+    float t_max = 1e9f;
+};
+struct RayHit {
+    float t;
+    uint32_t body_idx;  // UINT32_MAX on a miss
+};
+static_assert(sizeof(Ray) == sizeof(dyph_ray) && sizeof(RayHit) == sizeof(dyph_ray_hit));
+
+// ray_query (core/include/core/ray_query.hpp:34-40); d_rays / d_hits on the device.
+inline void ray_query(Stream& s, const BvhView& bvh, const BodyView& bodies, const ShapeView& shapes,
+                      const Ray* d_rays, RayHit* d_hits, uint32_t n_rays) {
+    check(dyph_ray_query(&bvh, &bodies, &shapes, reinterpret_cast<const dyph_ray*>(d_rays),
+                         reinterpret_cast<dyph_ray_hit*>(d_hits), n_rays, s.abi()),
+          "ray_query");
+}
+
+// ContactSensor (core/include/core/contact_sensor.hpp:20-58). The filter runs
+// on the device; query() blocks and leaves the matches in host arrays.
+class ContactSensor {
+public:
+    explicit ContactSensor(uint32_t shape_idx) { check(dyph_contact_sensor_create(shape_idx, &h_), "ContactSensor"); }
+    ~ContactSensor() { dyph_contact_sensor_destroy(h_); }
+    ContactSensor(const ContactSensor&) = delete;
+    ContactSensor& operator=(const ContactSensor&) = delete;
+    uint32_t query(Stream& s, const Narrowphase& np, const std::vector<uint32_t>& body_shapes) {
+        const uint32_t n = static_cast<uint32_t>(body_shapes.size());
+        if (n > shapes_.size()) shapes_ = Buffer<uint32_t>(s, n);
+        if (n) shapes_.upload(body_shapes.data(), n);
+        ContactView cv = np.contacts();
+        uint32_t m = 0;
+        check(dyph_contact_sensor_query(h_, &cv, shapes_.data(), n, s.abi(), &m), "ContactSensor::query");
+        check(dyph_contact_sensor_host_view(h_, &host_), "ContactSensor::query");
+        return m;
+    }
+    uint32_t count() const noexcept { return dyph_contact_sensor_count(h_); }
+    uint32_t shape_idx() const noexcept { return dyph_contact_sensor_shape_idx(h_); }
+    const uint32_t* body_a() const noexcept { return host_.body_a; }
+    const uint32_t* body_b() const noexcept { return host_.body_b; }
+    const float* pos_x() const noexcept { return host_.pos_x; }
+    const float* pos_y() const noexcept { return host_.pos_y; }
+    const float* pos_z() const noexcept { return host_.pos_z; }
+    const float* norm_x() const noexcept { return host_.norm_x; }
+    const float* norm_y() const noexcept { return host_.norm_y; }
+    const float* norm_z() const noexcept { return host_.norm_z; }
+    const float* depth() const noexcept { return host_.depth; }
+
+private:
+    dyph_contact_sensor* h_ = nullptr;
+    Buffer<uint32_t> shapes_;
+    ContactView host_{};
+};
+
+// ── the whole frame step ────────────────────────────────────────────────────
+
+// One scene (or a batch of scenes) stepped as examples/stress_test_blocks/
+// main.cpp:264-279 does it, graph-replayed, over a BodyStore's device arrays.
+class World {
+public:
+    World(Stream& s, BodyStore& bodies, ShapeStore& shapes, const AABB& scene_bounds,
+          const IntegratorParams& ip = {}, uint32_t max_pairs = 0, uint32_t max_contacts = 0, int n_iters = 10,
+          float friction = 0.5f, dyph_solver_mode mode = DYPH_SOLVER_REFERENCE)
+        : bodies_(&bodies), initial_(s, size_t(13) * bodies.capacity()) {
+        const uint32_t n = bodies.count();
+        dyph_world_desc d{};
+        d.bodies = bodies.view();
+        d.shapes = shapes.view();
+        d.scene_bounds = scene_bounds;
+        d.integrator = dyph_integrator_params{{ip.gravity[0], ip.gravity[1], ip.gravity[2]}, ip.dt, ip.n_substeps};
+        d.max_pairs = max_pairs ? max_pairs : 48 * n + 64;
+        d.max_contacts = max_contacts ? max_contacts : 16 * n + 64;
+        d.n_iters = n_iters;
+        d.friction = friction;
+        d.mode = mode;
+        check(dyph_world_create(&d, s.abi(), &h_), "World");
+        check_cuda(cudaMemcpyAsync(initial_.data(), bodies.device_rows(), initial_.size() * 4,
+                                   cudaMemcpyDeviceToDevice, s.native()),
+                   "World");
+        s.wait();
+    }
+    ~World() { dyph_world_destroy(h_); }
+    World(const World&) = delete;
+    World& operator=(const World&) = delete;
+    // Batched scenes: bodies [body_offset[k], body_offset[k+1]) form scene k.
+    void set_scenes(const std::vector<uint32_t>& body_offset, const std::vector<AABB>& bounds) {
+        if (body_offset.size() != bounds.size() + 1) throw std::runtime_error("World::set_scenes: sizes");
+        check(dyph_world_set_scenes(h_, static_cast<uint32_t>(bounds.size()), body_offset.data(), bounds.data()),
+              "World::set_scenes");
+    }
+    void step(Stream& s, int n_frames) { check(dyph_world_step(h_, n_frames, s.abi()), "World::step"); }
+    // Checkpointed rollout and its adjoint (dyph_world_rollout / _backward).
+    void rollout(Stream& s, int n_frames, int every, float* d_ckpt) {
+        check(dyph_world_rollout(h_, n_frames, every, d_ckpt, s.abi()), "World::rollout");
+    }
+    void rollout_backward(Stream& s, int n_frames, int every, const float* d_ckpt, const float* d_grad_final,
+                          float* d_grad_init, float* d_grad_inv_mass) {
+        check(dyph_world_rollout_backward(h_, n_frames, every, d_ckpt, d_grad_final, d_grad_init, d_grad_inv_mass,
+                                          s.abi()),
+              "World::rollout_backward");
+    }
+    std::vector<uint64_t> scene_hashes(Stream& s, uint32_t n_scenes) {
+        std::vector<uint64_t> out(n_scenes);
+        check(dyph_world_scene_hashes(h_, s.abi(), out.data(), n_scenes), "World::scene_hashes");
+        return out;
+    }
+    // State rows at creation ([13][capacity], device), the start of rollouts.
+    const float* initial_rows() const noexcept { return initial_.data(); }
+    BodyStore& bodies() noexcept { return *bodies_; }
+    dyph_world* handle() noexcept { return h_; }
+
+private:
+    dyph_world* h_ = nullptr;
+    BodyStore* bodies_;
+    Buffer<float> initial_;
 };
 
 // FNV-1a-64 over pos_x..rot_z (examples/stress_test_blocks/main.cpp:34-41, 301-311).

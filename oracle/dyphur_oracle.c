@@ -100,6 +100,7 @@ typedef struct world {
     uint64_t* keys;
     uint32_t* sorted_idx;
     int32_t *left, *right, *parent;
+    int32_t root;
     node_box* aabb;
     uint32_t* pairs; /* 2 * max_pairs */
     uint32_t n_pairs; /* true count of the last build */
@@ -321,6 +322,7 @@ static uint32_t broadphase(world* w) { /* Broadphase::build_and_query, broadphas
     int root = 0;
     for (int i = 0; i < ni - 1; ++i)
         if (w->parent[i] == -1) root = i;
+    w->root = root;
     /* Step 6a: leaf boxes (:216-251). */
     for (int k = 0; k < ni; ++k) {
         uint32_t body = w->sorted_idx[k];
@@ -995,6 +997,142 @@ uint32_t dyo_get_colors(void* p, uint32_t* out, uint32_t cap) {
     uint32_t m = w->nc < cap ? w->nc : cap;
     for (uint32_t c = 0; c < m; ++c) out[c] = w->colored_last ? w->color[c] : 0xFFFFFFFFu;
     return w->nc;
+}
+
+/* ── ray query and contact sensor ─────────────────────────────────────────── */
+
+/* Slab test against a node box (core/src/ray_query.cpp:14-33). */
+static int ray_node_hit(const float* r, const float* inv, float mnx, float mny, float mnz, float mxx, float mxy,
+                        float mxz, float best_t) {
+    float t1x = (mnx - r[0]) * inv[0], t2x = (mxx - r[0]) * inv[0];
+    float t1y = (mny - r[1]) * inv[1], t2y = (mxy - r[1]) * inv[1];
+    float t1z = (mnz - r[2]) * inv[2], t2z = (mxz - r[2]) * inv[2];
+    float tmin = t1x < t2x ? t1x : t2x, tmax = t1x < t2x ? t2x : t1x;
+    float ylo = t1y < t2y ? t1y : t2y, yhi = t1y < t2y ? t2y : t1y;
+    float zlo = t1z < t2z ? t1z : t2z, zhi = t1z < t2z ? t2z : t1z;
+    tmin = tmin > ylo ? tmin : ylo;
+    tmax = tmax < yhi ? tmax : yhi;
+    tmin = tmin > zlo ? tmin : zlo;
+    tmax = tmax < zhi ? tmax : zhi;
+    return tmax >= 0.f && tmax >= tmin && tmin < best_t;
+}
+
+/* v by the conjugate of q (Quat::rotate, core/include/core/math/quat.hpp:39-42). */
+static void rot_conj(float qw, float qx, float qy, float qz, const float v[3], float o[3]) {
+    float ux = -qx, uy = -qy, uz = -qz;
+    float tx = (uy * v[2] - uz * v[1]) * 2.f, ty = (uz * v[0] - ux * v[2]) * 2.f, tz = (ux * v[1] - uy * v[0]) * 2.f;
+    o[0] = (v[0] + tx * qw) + (uy * tz - uz * ty);
+    o[1] = (v[1] + ty * qw) + (uz * tx - ux * tz);
+    o[2] = (v[2] + tz * qw) + (ux * ty - uy * tx);
+}
+
+/* Exact leaf test (core/src/ray_query.cpp:37-123). */
+static void ray_leaf(const world* w, uint32_t bi, const float* r, float* best_t, uint32_t* best_body) {
+    uint32_t sh = w->shape[bi];
+    float hx = w->hx[sh], t;
+    if (w->stype[sh] == 1u) { /* sphere */
+        float ocx = r[0] - w->px[bi], ocy = r[1] - w->py[bi], ocz = r[2] - w->pz[bi];
+        float a = r[3] * r[3] + r[4] * r[4] + r[5] * r[5];
+        float b = r[3] * ocx + r[4] * ocy + r[5] * ocz;
+        float c = ocx * ocx + ocy * ocy + ocz * ocz - hx * hx;
+        float disc = b * b - a * c;
+        if (disc < 0.f) {
+            t = -1.f;
+        } else {
+            float sq = sqrtf(disc);
+            t = (-b - sq) / a;
+            if (t < 0.f) t = (-b + sq) / a;
+            t = (t >= 0.f && t < *best_t) ? t : -1.f;
+        }
+    } else { /* box, and every other type as its box */
+        float oc[3] = {r[0] - w->px[bi], r[1] - w->py[bi], r[2] - w->pz[bi]}, d[3] = {r[3], r[4], r[5]};
+        float lo[3], ld[3];
+        rot_conj(w->qw[bi], w->qx[bi], w->qy[bi], w->qz[bi], oc, lo);
+        rot_conj(w->qw[bi], w->qx[bi], w->qy[bi], w->qz[bi], d, ld);
+        float h[3] = {hx, w->hy[sh], w->hz[sh]};
+        float tmin = 0.f, tmax = 0.f;
+        for (int k = 0; k < 3; ++k) {
+            float inv = 1.f / ld[k];
+            float t1 = (-h[k] - lo[k]) * inv, t2 = (h[k] - lo[k]) * inv;
+            float l = t1 < t2 ? t1 : t2, u = t1 < t2 ? t2 : t1;
+            if (k == 0) {
+                tmin = l;
+                tmax = u;
+            } else {
+                tmin = tmin > l ? tmin : l;
+                tmax = tmax < u ? tmax : u;
+            }
+        }
+        if (tmax < 0.f || tmin > tmax) {
+            t = -1.f;
+        } else {
+            t = tmin >= 0.f ? tmin : tmax;
+            t = (t >= 0.f && t < *best_t) ? t : -1.f;
+        }
+    }
+    if (t >= 0.f) {
+        *best_t = t;
+        *best_body = bi;
+    }
+}
+
+/* ray_query (core/src/ray_query.cpp:126-195) over the tree of the last
+ * broadphase stage and the current poses. rays: [7 n_rays] = origin xyz,
+ * direction xyz, t_max. */
+void dyo_ray_query(void* p, const float* rays, uint32_t n_rays, float* out_t, uint32_t* out_body) {
+    world* w = (world*)p;
+    for (uint32_t q = 0; q < n_rays; ++q) {
+        const float* r = rays + 7 * (size_t)q;
+        float best_t = r[6];
+        uint32_t best_body = 0xFFFFFFFFu;
+        float inv[3] = {1.f / r[3], 1.f / r[4], 1.f / r[5]};
+        if (w->n == 1) {
+            ray_leaf(w, 0u, r, &best_t, &best_body);
+        } else if (w->n > 1) {
+            int32_t stack[64];
+            int top = 0;
+            const int32_t n_int = (int32_t)w->n - 1;
+            stack[top++] = w->root;
+            while (top > 0) {
+                int32_t node = stack[--top];
+                const node_box* nb = &w->aabb[node];
+                if (!ray_node_hit(r, inv, f16_to_f32(nb->h[0]), f16_to_f32(nb->h[1]), f16_to_f32(nb->h[2]),
+                                  f16_to_f32(nb->h[3]), f16_to_f32(nb->h[4]), f16_to_f32(nb->h[5]), best_t))
+                    continue;
+                if (node >= n_int) {
+                    ray_leaf(w, w->sorted_idx[node - n_int], r, &best_t, &best_body);
+                } else if (top + 1 < 64) {
+                    stack[top++] = w->right[node];
+                    stack[top++] = w->left[node];
+                }
+            }
+        }
+        out_t[q] = best_t;
+        out_body[q] = best_body;
+    }
+}
+
+/* ContactSensor::query (core/src/contact_sensor.cpp:6-59) on the contacts of
+ * the last narrowphase stage, with the bodies' shapes as body_shapes. Writes
+ * ab[2m], p7[7m] like dyo_get_contacts; returns the match count. */
+uint32_t dyo_contact_sensor(void* p, uint32_t shape_idx, uint32_t* ab, float* p7, uint32_t cap) {
+    world* w = (world*)p;
+    uint32_t m = 0;
+    for (uint32_t c = 0; c < w->nc; ++c) {
+        uint32_t a = w->ca[c], b = w->cb[c];
+        int hit = (a < w->n && w->shape[a] == shape_idx) || (b < w->n && w->shape[b] == shape_idx);
+        if (!hit) continue;
+        if (m < cap) {
+            ab[2 * m] = a;
+            ab[2 * m + 1] = b;
+            float* o = p7 + 7 * (size_t)m;
+            o[0] = w->cpx[c]; o[1] = w->cpy[c]; o[2] = w->cpz[c];
+            o[3] = w->cnx[c]; o[4] = w->cny[c]; o[5] = w->cnz[c];
+            o[6] = w->cd[c];
+        }
+        ++m;
+    }
+    return m;
 }
 
 /* Stand-alone helpers for unit KATs. */

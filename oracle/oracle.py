@@ -135,6 +135,10 @@ class Checker:
         self.f_bvh = getattr(L, p + "get_bvh"); self.f_bvh.argtypes = [vp] * 7
         self.f_colors = getattr(L, p + "get_colors"); self.f_colors.restype = u32
         self.f_colors.argtypes = [vp, vp, u32]
+        self.f_rays = getattr(L, p + "ray_query"); self.f_rays.restype = None
+        self.f_rays.argtypes = [vp, vp, u32, vp, vp]
+        self.f_sensor = getattr(L, p + "contact_sensor"); self.f_sensor.restype = u32
+        self.f_sensor.argtypes = [vp, u32, vp, vp, u32]
 
 
 class World:
@@ -230,6 +234,25 @@ class World:
                       parent.ctypes.data, aabb.ctypes.data)
         return dict(keys=keys, sorted_idx=si, left=left[:n - 1], right=right[:n - 1],
                     parent=parent[:2 * n - 1], aabb=aabb[:2 * n - 1])
+
+    def ray_query(self, rays: np.ndarray):
+        """Closest hits of rays (n, 7) = origin xyz, direction xyz, t_max over
+        the tree of the last broadphase stage: (t float32 (n,), body uint32 (n,))."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 7)
+        t = np.empty(rays.shape[0], np.float32)
+        body = np.empty(rays.shape[0], np.uint32)
+        self.ck.f_rays(self.h, rays.ctypes.data, rays.shape[0], t.ctypes.data, body.ctypes.data)
+        return t, body
+
+    def contact_sensor(self, shape_idx: int):
+        """Contacts of the last narrowphase stage that involve shape_idx:
+        (ab (m, 2) uint32, p7 (m, 7) float32) in store order."""
+        cap = self.max_contacts
+        ab = np.empty((cap, 2), np.uint32)
+        p7 = np.empty((cap, 7), np.float32)
+        m = int(self.ck.f_sensor(self.h, int(shape_idx), ab.ctypes.data, p7.ctypes.data, cap))
+        m = min(m, cap)
+        return ab[:m].copy(), p7[:m].copy()
 
     def colors(self):
         cap = self.max_contacts

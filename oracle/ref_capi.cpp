@@ -23,8 +23,10 @@
 #include <core/articulation.hpp>
 #include <core/body_store.hpp>
 #include <core/broadphase.hpp>
+#include <core/contact_sensor.hpp>
 #include <core/integrator.hpp>
 #include <core/narrowphase.hpp>
+#include <core/ray_query.hpp>
 #include <core/shape_store.hpp>
 #include <core/xpbd_solver.hpp>
 #undef private
@@ -263,6 +265,43 @@ uint32_t dyr_get_colors(void* w, uint32_t* out, uint32_t cap) {
     }
     std::memcpy(out, rw->solver.color_.data(), m * sizeof(uint32_t));
     return nc;
+}
+
+// ray_query (core/src/ray_query.cpp:126-195) over the tree of the last
+// broadphase stage. rays: [7 n_rays] = origin xyz, direction xyz, t_max.
+void dyr_ray_query(void* w, const float* rays, uint32_t n_rays, float* out_t, uint32_t* out_body) {
+    auto* rw = static_cast<RefWorld*>(w);
+    if (n_rays == 0) return;
+    std::vector<Ray> r(n_rays);
+    std::vector<RayHit> h(n_rays);
+    for (uint32_t q = 0; q < n_rays; ++q) {
+        const float* x = rays + 7 * static_cast<size_t>(q);
+        r[q] = Ray{x[0], x[1], x[2], x[3], x[4], x[5], x[6]};
+    }
+    ray_query(rw->s, rw->bp.bvh_view(rw->n), rw->bs.view(), rw->ss.view(), r.data(), h.data(), n_rays);
+    rw->s.wait();
+    for (uint32_t q = 0; q < n_rays; ++q) {
+        out_t[q] = h[q].t;
+        out_body[q] = h[q].body_idx;
+    }
+}
+
+// ContactSensor(shape_idx).query(s, np, bs.body_shapes()) on the contacts of
+// the last narrowphase stage (core/src/contact_sensor.cpp:6-59). Writes
+// ab[2m], p7[7m]; returns the match count.
+uint32_t dyr_contact_sensor(void* w, uint32_t shape_idx, uint32_t* ab, float* p7, uint32_t cap) {
+    auto* rw = static_cast<RefWorld*>(w);
+    ContactSensor cs(shape_idx);
+    uint32_t m = cs.query(rw->s, rw->np, rw->bs.body_shapes());
+    for (uint32_t c = 0; c < std::min(m, cap); ++c) {
+        ab[2 * c] = cs.body_a()[c];
+        ab[2 * c + 1] = cs.body_b()[c];
+        float* o = p7 + 7 * static_cast<size_t>(c);
+        o[0] = cs.pos_x()[c]; o[1] = cs.pos_y()[c]; o[2] = cs.pos_z()[c];
+        o[3] = cs.norm_x()[c]; o[4] = cs.norm_y()[c]; o[5] = cs.norm_z()[c];
+        o[6] = cs.depth()[c];
+    }
+    return m;
 }
 
 }  // extern "C"
