@@ -82,6 +82,10 @@ _PROTOS = {
     "dyph_narrowphase_run_host_count": (_st, [_vp, _vp, C.c_uint32, C.POINTER(Bodies), C.POINTER(Shapes), _vp]),
     "dyph_narrowphase_contacts": (_st, [_vp, C.POINTER(Contacts)]),
     "dyph_narrowphase_download_count": (_st, [_vp, _vp, _up, _up]),
+    "dyph_set_spin_limit": (_st, [C.c_uint32]),
+    "dyph_wait_selftest": (_st, [C.c_int, _vp]),
+    "dyph_bodies_check_finite": (_st, [C.POINTER(Bodies), _vp, _up]),
+    "dyph_world_check_finite": (_st, [_vp, _vp, _up]),
     "dyph_ray_query": (_st, [C.POINTER(BvhView), C.POINTER(Bodies), C.POINTER(Shapes), _vp, _vp, C.c_uint32, _vp]),
     "dyph_contact_sensor_create": (_st, [C.c_uint32, C.POINTER(_vp)]),
     "dyph_contact_sensor_destroy": (None, [_vp]),

@@ -19,8 +19,10 @@ constexpr uint32_t kFlagSleeping = 4u;  // BodyFlag::Sleeping (core/include/core
 constexpr uint32_t kShapeBox = 0u;
 constexpr uint32_t kShapeSphere = 1u;
 
-// Iteration limit for every device-side spin (look-back, grid barrier). With
-// the nanosleep back-off this is well over a second of waiting.
+// Default iteration limit for every device-side spin (look-back, grid
+// barrier, dataflow polls). With the nanosleep back-off this is well over a
+// second of waiting. The limit in force is the device variable g_spin_limit
+// (dyph_set_spin_limit), so a test can make a wait give up quickly.
 constexpr uint32_t kSpinLimit = 1u << 24;
 
 // Sticky device error word (DYPH_ERR_TIMEOUT ...), read by dyph_download_device_error.
@@ -30,6 +32,12 @@ __device__ uint32_t g_device_error = 0u;
 // Where the first error was raised (1 look-back, 2 sort look-back, 3 grid
 // barrier, 5 sequential schedule, 6 / 7 tree walk, 8 narrowphase pair index).
 __device__ uint32_t g_device_error_site = 0u;
+
+// Iteration limit of the bounded waits in force (the default unless a
+// caller of dyph_set_spin_limit changed it).
+__device__ uint32_t g_spin_limit = kSpinLimit;
+
+__device__ __forceinline__ uint32_t spin_limit() { return __ldg(&g_spin_limit); }
 
 __device__ __forceinline__ void raise_error(uint32_t code, uint32_t site = 0u) {
     if (atomicCAS(&g_device_error, 0u, code) == 0u) g_device_error_site = site;
@@ -100,6 +108,7 @@ __device__ __forceinline__ uint32_t lookback_warp(uint32_t* status, uint32_t til
     uint32_t exclusive = 0;
     int64_t base = static_cast<int64_t>(tile) - 1;
     uint32_t spins = 0;
+    const uint32_t limit = spin_limit();
     while (true) {
         int64_t t = base - lane;
         uint32_t s = (t >= 0) ? ld_acquire(&status[t]) : kLbPrefix;
@@ -111,7 +120,7 @@ __device__ __forceinline__ uint32_t lookback_warp(uint32_t* status, uint32_t til
         unsigned first_prefix = is_prefix ? static_cast<unsigned>(__ffs(is_prefix) - 1) : 32u;
         unsigned need = (first_prefix >= 31u) ? 0xffffffffu : ((1u << (first_prefix + 1u)) - 1u);
         if (not_ready & need) {
-            if (++spins > kSpinLimit) {
+            if (++spins > limit) {
                 raise_error(DYPH_ERR_TIMEOUT, 1u);
                 return 0u;
             }
@@ -154,8 +163,9 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t n_blocks) {
             st_release(&bar[1], gen + 1u);
         } else {
             uint32_t spins = 0;
+            const uint32_t limit = spin_limit();
             while (ld_acquire(&bar[1]) == gen) {
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     raise_error(DYPH_ERR_TIMEOUT, 3u);
                     ok = 0;
                     break;

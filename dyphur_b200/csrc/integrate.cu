@@ -1,5 +1,7 @@
 // Symplectic Euler integration (core/src/integrator.cpp:7-71) and the
 // library-level C entry points (status strings, device check, error word).
+#include <algorithm>
+
 #include <cuda_runtime.h>
 
 #include "internal.cuh"
@@ -40,7 +42,71 @@ dyph_status integrate_launch(const dyph_bodies* bodies, const dyph_integrator_pa
     return DYPH_OK;
 }
 
+// ── diagnostics ─────────────────────────────────────────────────────────────
+
+// Smallest index of a body with a NaN / Inf in its 13 state floats.
+__global__ void finite_kernel(dyph_bodies b, uint32_t* __restrict__ first_bad) {
+    const float* rows[13] = {b.pos_x, b.pos_y, b.pos_z, b.rot_w, b.rot_x, b.rot_y, b.rot_z,
+                             b.vel_x, b.vel_y, b.vel_z, b.ang_x, b.ang_y, b.ang_z};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.n; i += gridDim.x * blockDim.x) {
+        bool ok = true;
+#pragma unroll
+        for (int r = 0; r < 13; ++r) ok = ok && isfinite(rows[r][i]);
+        if (!ok) atomicMin(first_bad, i);
+    }
+}
+
+// A wait that nothing ends: which 1 = the look-back of tile 1 on a tile 0 that
+// never publishes (site 1), which 3 = a grid barrier of two blocks launched
+// as one (site 3). Each gives up after the spin limit and the kernel returns.
+__device__ uint32_t g_selftest_words[4];
+
+__global__ void wait_selftest_kernel(int which) {
+    if (which == 1) {
+        if (threadIdx.x < 32) lookback_warp(g_selftest_words, 1u, 7u);
+    } else {
+        grid_barrier(g_selftest_words + 2, 2u);
+    }
+}
+
 }  // namespace dyph
+
+extern "C" dyph_status dyph_set_spin_limit(uint32_t limit) {
+    const uint32_t v = limit ? limit : dyph::kSpinLimit;
+    DYPH_CUDA_TRY(cudaMemcpyToSymbol(dyph::g_spin_limit, &v, sizeof(v)));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_wait_selftest(int which, dyph_stream s) {
+    if (which != 1 && which != 3) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    void* words = nullptr;
+    DYPH_CUDA_TRY(cudaGetSymbolAddress(&words, dyph::g_selftest_words));
+    DYPH_CUDA_TRY(cudaMemsetAsync(words, 0, 4 * sizeof(uint32_t), cs));
+    dyph::wait_selftest_kernel<<<1, 32, 0, cs>>>(which);
+    DYPH_CUDA_TRY(cudaGetLastError());
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_bodies_check_finite(const dyph_bodies* bodies, dyph_stream s, uint32_t* out_first_bad) {
+    if (!bodies) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    uint32_t first = 0xFFFFFFFFu;
+    if (bodies->n > 0) {
+        uint32_t* d = nullptr;
+        DYPH_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(uint32_t), cs));
+        DYPH_CUDA_TRY(cudaMemsetAsync(d, 0xFF, sizeof(uint32_t), cs));
+        const uint32_t blocks = std::min<uint32_t>((bodies->n + 255) / 256, 148u * 8u);
+        dyph::finite_kernel<<<blocks, 256, 0, cs>>>(*bodies, d);
+        DYPH_CUDA_TRY(cudaGetLastError());
+        DYPH_CUDA_TRY(cudaMemcpyAsync(&first, d, sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+        DYPH_CUDA_TRY(cudaFreeAsync(d, cs));
+        DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    }
+    if (out_first_bad) *out_first_bad = first;
+    return first == 0xFFFFFFFFu ? DYPH_OK : DYPH_ERR_NOT_FINITE;
+}
 
 extern "C" dyph_status dyph_integrate(const dyph_bodies* bodies, const dyph_integrator_params* params,
                                       dyph_stream s) {

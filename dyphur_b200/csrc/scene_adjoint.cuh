@@ -147,40 +147,47 @@ __device__ void adjoint_scene(const Team& T, uint32_t s, unsigned char* smem, ui
             T.sync();
         }
         // ── narrowphase: geometry adjoints -> poses after integrate ──
-        for (uint32_t k = T.rank(); k < m; k += T.size()) {
-            const float* r = A.rec + cbase + k;
-            if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
-            const Contact ct = SC.contact(k);
-            const uint32_t ia = ct.a, ib = ct.b;
-            const uint32_t ga = b0 + ia, gbi = b0 + ib;
-            const F3 xa = f3(A.pose1[ga], A.pose1[ns + ga], A.pose1[2ull * ns + ga]);
-            const F3 xb = f3(A.pose1[gbi], A.pose1[ns + gbi], A.pose1[2ull * ns + gbi]);
-            const float qa[4] = {A.pose1[3ull * ns + ga], A.pose1[4ull * ns + ga], A.pose1[5ull * ns + ga],
-                                 A.pose1[6ull * ns + ga]};
-            const float qb[4] = {A.pose1[3ull * ns + gbi], A.pose1[4ull * ns + gbi], A.pose1[5ull * ns + gbi],
-                                 A.pose1[6ull * ns + gbi]};
-            const float ha[3] = {half[ia], half[ldb + ia], half[2 * ldb + ia]};
-            const float hb[3] = {half[ib], half[ldb + ib], half[2 * ldb + ib]};
-            F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
-            float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
-            process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
-                             __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
-                             f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
-                             f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
-            if (SB.im(ia) != 0.f) {
-                atomicAdd(&grow(G.gout, ns, 0, ga), xab.x);
-                atomicAdd(&grow(G.gout, ns, 1, ga), xab.y);
-                atomicAdd(&grow(G.gout, ns, 2, ga), xab.z);
-                for (int c = 0; c < 4; ++c) atomicAdd(&grow(G.gout, ns, 3 + c, ga), qab[c]);
+        // Group by group (no dynamic body twice in a group), so every body's
+        // sum is taken in one fixed order without atomics: the gradients are
+        // the same from run to run, bit for bit.
+        for (uint32_t g = 0; g < fo.groups; ++g) {
+            const uint32_t end = SC.pa(g + 1);
+            for (uint32_t idx = SC.pa(g) + T.rank(); idx < end; idx += T.size()) {
+                const uint32_t k = SC.ent(idx);
+                const float* r = A.rec + cbase + k;
+                if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
+                const Contact ct = SC.contact(k);
+                const uint32_t ia = ct.a, ib = ct.b;
+                const uint32_t ga = b0 + ia, gbi = b0 + ib;
+                const F3 xa = f3(A.pose1[ga], A.pose1[ns + ga], A.pose1[2ull * ns + ga]);
+                const F3 xb = f3(A.pose1[gbi], A.pose1[ns + gbi], A.pose1[2ull * ns + gbi]);
+                const float qa[4] = {A.pose1[3ull * ns + ga], A.pose1[4ull * ns + ga], A.pose1[5ull * ns + ga],
+                                     A.pose1[6ull * ns + ga]};
+                const float qb[4] = {A.pose1[3ull * ns + gbi], A.pose1[4ull * ns + gbi], A.pose1[5ull * ns + gbi],
+                                     A.pose1[6ull * ns + gbi]};
+                const float ha[3] = {half[ia], half[ldb + ia], half[2 * ldb + ia]};
+                const float hb[3] = {half[ib], half[ldb + ib], half[2 * ldb + ib]};
+                F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
+                float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
+                process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
+                                 __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
+                                 f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
+                                 f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
+                if (SB.im(ia) != 0.f) {
+                    grow(G.gout, ns, 0, ga) += xab.x;
+                    grow(G.gout, ns, 1, ga) += xab.y;
+                    grow(G.gout, ns, 2, ga) += xab.z;
+                    for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, ga) += qab[c];
+                }
+                if (SB.im(ib) != 0.f) {
+                    grow(G.gout, ns, 0, gbi) += xbb.x;
+                    grow(G.gout, ns, 1, gbi) += xbb.y;
+                    grow(G.gout, ns, 2, gbi) += xbb.z;
+                    for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, gbi) += qbb[c];
+                }
             }
-            if (SB.im(ib) != 0.f) {
-                atomicAdd(&grow(G.gout, ns, 0, gbi), xbb.x);
-                atomicAdd(&grow(G.gout, ns, 1, gbi), xbb.y);
-                atomicAdd(&grow(G.gout, ns, 2, gbi), xbb.z);
-                for (int c = 0; c < 4; ++c) atomicAdd(&grow(G.gout, ns, 3 + c, gbi), qbb[c]);
-            }
+            T.sync();
         }
-        T.sync();
     }
     // ── integration, from the state at the frame's start ──
     const GlobalBodies B0{P_.gb};

@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
             if (__any_sync(0xffffffffu, progressed)) {
                 idle = 0;
             } else {
-                if (++idle > kSpinLimit) {
+                if (++idle > spin_limit()) {
                     raise_error(DYPH_ERR_TIMEOUT, 9u);
                     break;
                 }
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kFlowThreads) flow_solve_kernel(dyph_contacts 
                 if (__any_sync(0xffffffffu, progressed)) {
                     idle = 0;
                 } else {
-                    if (++idle > kSpinLimit) {
+                    if (++idle > spin_limit()) {
                         raise_error(DYPH_ERR_TIMEOUT, 10u);
                         break;
                     }

@@ -72,7 +72,7 @@ __device__ __forceinline__ uint32_t lookback_column(uint32_t* status, uint32_t t
         uint32_t s = ld_acquire(&status[static_cast<size_t>(t) * 256 + col]);
         uint32_t flag = s & ~kLbMask;
         if (flag == 0u) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit()) {
                 raise_error(DYPH_ERR_TIMEOUT, 2u);
                 return 0u;
             }

@@ -363,6 +363,11 @@ extern "C" dyph_status dyph_event_elapsed_ms(void* start, void* end, float* ms) 
     return DYPH_OK;
 }
 
+extern "C" dyph_status dyph_world_check_finite(dyph_world* w, dyph_stream s, uint32_t* out_first_bad) {
+    if (!w) return DYPH_ERR_INVALID;
+    return dyph_bodies_check_finite(&w->desc.bodies, s, out_first_bad);
+}
+
 extern "C" dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* last_pairs,
                                                  uint32_t* last_contacts, uint32_t* peak_pairs,
                                                  uint32_t* peak_contacts, uint32_t* status) {

@@ -344,6 +344,25 @@ def device_error_site(stream=None) -> tuple:
     return int(code.value), int(site.value)
 
 
+def set_spin_limit(limit: int) -> None:
+    """Iteration limit of every bounded device wait (0 = the default)."""
+    check(capi.lib().dyph_set_spin_limit(int(limit)), "dyph_set_spin_limit")
+
+
+def wait_selftest(which: int, stream=None) -> None:
+    """A bounded wait that nothing ends (1 look-back, 3 grid barrier)."""
+    check(capi.lib().dyph_wait_selftest(int(which), _stream_ptr(stream)), "dyph_wait_selftest")
+
+
+def check_finite(bodies: DeviceBodies, stream=None) -> tuple:
+    """(status, first bad body index) of dyph_bodies_check_finite."""
+    first = C.c_uint32()
+    st = capi.lib().dyph_bodies_check_finite(C.byref(bodies.view), _stream_ptr(stream), C.byref(first))
+    if st not in (capi.OK, capi.ERR_NOT_FINITE):
+        check(st, "dyph_bodies_check_finite")
+    return int(st), int(first.value)
+
+
 def state_hash(bodies: DeviceBodies, stream=None) -> int:
     out = torch.zeros(1, dtype=torch.int64, device=bodies.fbuf.device)
     check(capi.lib().dyph_fnv1a64_state(C.byref(bodies.view), _ptr(out), _stream_ptr(stream)))

@@ -149,6 +149,22 @@ dyph_status dyph_download_device_error(dyph_stream s, uint32_t* out_code);
  * look-back, 3 grid barrier, 5 sequential solve schedule, 6 / 7 tree walk,
  * 8 narrowphase pair index. Both words are cleared. */
 dyph_status dyph_download_device_error_site(dyph_stream s, uint32_t* out_code, uint32_t* out_site);
+/* Iteration limit of every bounded device wait (look-backs, grid barriers,
+ * dataflow polls) on the current device; 0 restores the default (2^24 polls
+ * with a back-off, over a second). Synchronous. A wait that reaches the limit
+ * raises DYPH_ERR_TIMEOUT in the sticky device error word and its kernel
+ * returns. */
+dyph_status dyph_set_spin_limit(uint32_t limit);
+/* Runs one bounded wait that nothing ends, so the timeout path can be checked
+ * without a fault: which 1 = a tile look-back whose predecessor never
+ * publishes (error site 1), 3 = a grid barrier waiting for a block that is
+ * never launched (site 3). Blocking; afterwards dyph_download_device_error_site
+ * reports DYPH_ERR_TIMEOUT and the site. */
+dyph_status dyph_wait_selftest(int which, dyph_stream s);
+/* Blocking: DYPH_ERR_NOT_FINITE if any body's 13 state floats (pos, rot,
+ * vel, ang) hold a NaN or Inf, with the smallest such body index in
+ * *out_first_bad (UINT32_MAX and DYPH_OK otherwise). */
+dyph_status dyph_bodies_check_finite(const dyph_bodies* bodies, dyph_stream s, uint32_t* out_first_bad);
 /* Blocking raw copies between host memory and device memory (the Buffer<T>
  * upload / download of compute/include/compute/buffer.hpp:41-49). */
 dyph_status dyph_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, dyph_stream s);
@@ -413,6 +429,8 @@ dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_frames, int32_t
 /* Blocking: FNV-1a-64 of every scene's pose arrays (one value for a single
  * scene); cap >= number of scenes. */
 dyph_status dyph_world_scene_hashes(dyph_world* w, dyph_stream s, uint64_t* host_out, uint32_t cap);
+/* dyph_bodies_check_finite over the world's bodies. */
+dyph_status dyph_world_check_finite(dyph_world* w, dyph_stream s, uint32_t* out_first_bad);
 /* Blocking: peak pair / contact counts and the sticky status of the frames
  * stepped so far (overflow or timeout). */
 dyph_status dyph_world_download_stats(dyph_world* w, dyph_stream s, uint32_t* last_pairs,
