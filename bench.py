@@ -307,6 +307,15 @@ def flow_kernel_bytes(n: int, contacts: np.ndarray) -> np.ndarray:
     return 132.0 * n + 36.0 * contacts.astype(np.float64)
 
 
+def frame_kernel_bytes(n: int, pairs: np.ndarray, contacts: np.ndarray) -> np.ndarray:
+    """Compulsory bytes of one fused batched-frame launch (scene_frame_kernel):
+    per body the state it reads (80 B), its shape index, flags, shape type and
+    half extents (24 B) and the state it writes (52 B); per stored pair its
+    4-byte record; per contact its 36-byte row and 4-byte colour. Pairs and
+    contacts otherwise live in shared memory."""
+    return 156.0 * n + 4.0 * pairs.astype(np.float64) + 40.0 * contacts.astype(np.float64)
+
+
 def flow_kernel_active(contacts: np.ndarray, mode: int) -> np.ndarray:
     """Frames on which the dataflow kernel does the solve: the sequential order
     at <= 2048 contacts and the reference order at <= 256 run the one-block
@@ -317,8 +326,10 @@ def flow_kernel_active(contacts: np.ndarray, mode: int) -> np.ndarray:
     return (c > 0) & ~(seq & (c <= 2048)) & (c <= 16 * FLOW_THREADS)
 
 
-def kernels_per_frame(n: int, n_scenes: int = 1) -> int:
-    """Library kernels one frame launches (matches the ncu launch list in profiles/)."""
+def kernels_per_frame(n: int, n_scenes: int = 1, fused: bool = False) -> int:
+    """Library kernels one frame launches (matches the ncu launch lists in profiles/)."""
+    if fused:  # the fused frame kernel and the frame's statistics
+        return 2
     if n_scenes > 1:  # (scene << 30 | code) keys: histogram + one pass per 8 key bits, + scene ranges
         key_bits = 30 + max(1, (n_scenes - 1).bit_length())
         sort = (1 if n <= 4096 else 1 + (key_bits + 7) // 8) + 1
@@ -428,10 +439,11 @@ def e2e_episodes(w, init, frames, steps, torch, barrier):
     return ms, h2d, d2h
 
 
-def probe_flow_kernel(w, frames, mode, torch):
-    """Per-frame device time of the dataflow solver kernel alone (events in the
+def probe_flow_kernel(w, frames, mode, torch, fused=False):
+    """Per-frame device time of the dominant kernel alone (events in the
     episode graph around that launch), the counts of the frames, and the
-    roofline of that kernel."""
+    roofline of that kernel: the dataflow solver kernel of a single scene, or
+    the fused frame kernel of a batch whose frames run fused."""
     stream = torch.cuda.current_stream()
     fb = w.bodies.fbuf
     init = fb.clone()
@@ -445,30 +457,77 @@ def probe_flow_kernel(w, frames, mode, torch):
     fb.copy_(init)
     torch.cuda.synchronize()
     n = w.bodies.n
-    act = flow_kernel_active(contacts, mode)
-    b = flow_kernel_bytes(n, contacts)
+    if fused:
+        kernel = "scene_frame_kernel"
+        act = np.ones(frames, bool)
+        b = frame_kernel_bytes(n, pairs, contacts)
+        rule = ("156 B per body (read state 80 + shape and flags 24, write state 52) + 4 B per stored pair + "
+                "40 B per contact (row 36 + colour 4)")
+    else:
+        kernel = "flow_solve_kernel"
+        act = flow_kernel_active(contacts, mode)
+        b = flow_kernel_bytes(n, contacts)
+        rule = "132 B per body (read 80, write 52) + 36 B per contact row"
     peak, peak_kind = peaks()
     achieved = float(b[act].sum() / (probe[act].sum() / 1e3) / 1e9) if act.any() and probe[act].sum() > 0 else None
-    return {"bound": "hbm", "kernel": "flow_solve_kernel",
-            "launches_timed": int(act.sum()),
-            "algorithmic_bytes_per_launch": float(b[act].mean()) if act.any() else None,
-            "bytes_rule": "132 B per body (read 80, write 52) + 36 B per contact row",
-            "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": (achieved / peak) if achieved else None, "peak_source": f"{peak_kind} hbm_gbs",
-            "traffic": committed_traffic("flow_solve_kernel", float(b[act].mean())) if act.any() else None,
-            "kernel_ms_per_launch": float(probe[act].mean()) if act.any() else None}, pairs, contacts, probe
+    out = {"bound": "hbm", "kernel": kernel, "launches_timed": int(act.sum()),
+           "algorithmic_bytes_per_launch": float(b[act].mean()) if act.any() else None,
+           "bytes_rule": rule, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": (achieved / peak) if achieved else None, "peak_source": f"{peak_kind} hbm_gbs",
+           "traffic": committed_traffic(kernel, float(b[act].mean())) if act.any() else None,
+           "kernel_ms_per_launch": float(probe[act].mean()) if act.any() else None}
+    if fused and act.any():  # the frame's compulsory bytes over the one launch that does the whole frame
+        fb_ = frame_bytes(n, pairs, contacts)
+        out["frame_rule_achieved"] = float(fb_.sum() / (probe.sum() / 1e3) / 1e9)
+        out["frame_rule_frac"] = out["frame_rule_achieved"] / peak
+    return out, pairs, contacts, probe
 
 
 def gpu_workload(scene, mode, frames, args, torch, barrier, clocks=None, roofline=True):
     from dyphur_b200 import device
     w = device.World(scene, mode=mode)
+    tuned = w.autotune(16) if scene.n_scenes > 1 else None  # before the episode is captured
     w.capture_episode(frames, -1)
     ms, ck, init = timed_episodes(w, args.steps, args.warmup, torch, barrier, clocks)
     st = w.stats()
-    out = {"ms": ms, "clocks": ck, "status": st["status"], "world": w, "init": init}
+    out = {"ms": ms, "clocks": ck, "status": st["status"], "world": w, "init": init, "fused_config": tuned}
     if roofline:
-        out["roofline"], out["pairs"], out["contacts"], _ = probe_flow_kernel(w, frames, mode, torch)
+        out["roofline"], out["pairs"], out["contacts"], _ = probe_flow_kernel(w, frames, mode, torch,
+                                                                              fused=scene.n_scenes > 1)
     return out
+
+
+def fp64_error_report(scene, mode: int, frames: int, sample: int = 8, carried=(10, 30)) -> dict:
+    """Error of the float frame step against an FP64 re-run of the same
+    frames along the float run's contact set and branches
+    (oracle/dual_oracle.cpp, dyd_fp64_run), on a sample of the scenes, in
+    solver order `mode`. The per-frame figure restarts the FP64 run from the
+    float state every frame (each frame's own rounding error); the carried
+    figure keeps the FP64 state, which contact-rich scenes amplify like any
+    perturbation, so it is given only over the first frames."""
+    from dyphur_b200 import device
+    from oracle import oracle
+    idx = np.linspace(0, scene.n_scenes - 1, min(sample, scene.n_scenes)).astype(int)
+    per_frame_max, per_frame_mean, rot_max, carried_max = [], [], [], {c: 0.0 for c in carried}
+    for i in idx:
+        sc = scene.scene(int(i)) if scene.n_scenes > 1 else scene
+        st, im, ii, fl = device.pack_bodies(sc)
+        args = (st, im, ii, sc.shape_type[sc.shape], np.ascontiguousarray(sc.shape_half[sc.shape].T), fl)
+        ep, er, _, _ = oracle.fp64_run(*args, frames, sc.dt, sc.gravity, sc.n_substeps, sc.n_iters, sc.friction,
+                                       mode, local=True)
+        per_frame_max.append(float(ep.max()))
+        per_frame_mean.append(float(ep.mean()))
+        rot_max.append(float(er.max()))
+        epc, _, _, _ = oracle.fp64_run(*args, max(carried), sc.dt, sc.gravity, sc.n_substeps, sc.n_iters,
+                                       sc.friction, mode, local=False)
+        for c in carried:
+            carried_max[c] = max(carried_max[c], float(epc[c - 1]))
+    return {"vs": "FP64 re-run of the same frames along the float run's contacts and branches",
+            "solver_mode": {0: "reference", 1: "sequential", 2: "colored"}[mode],
+            "sample": f"{len(idx)} scenes, {frames} frames" if scene.n_scenes > 1 else f"{frames} frames",
+            "per_frame_pos_err_max_m": max(per_frame_max), "per_frame_pos_err_mean_m": float(np.mean(per_frame_mean)),
+            "per_frame_rot_err_max": max(rot_max),
+            "carried_pos_err_max_m": {str(c): carried_max[c] for c in carried}}
 
 
 def final_state(scene, mode, frames, torch):
@@ -753,6 +812,13 @@ def run_b200(args) -> None:
         note("per-scene path")
         drift = drift_report(scene, frames, torch)
         note("drift")
+        fp64 = [fp64_error_report(scene, mode, frames, sample=6), fp64_error_report(scene, 2, frames, sample=6)]
+        stress = scenes.stress_blocks()
+        config1 = {"workload": "the reference's stress_test_blocks scene: 1024 boxes (8x16x8, spacing 0.85 m, "
+                               "jitter 0.01) + ground",
+                   "fp64_error": fp64_error_report(stress, 0, 120, sample=1),
+                   "colored_drift": drift_report(stress, 300, torch)}
+        note("fp64 error + config-1 drift")
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -769,13 +835,17 @@ def run_b200(args) -> None:
             "colored": {"value": value_c, "unit": METRIC, "ms_per_step": ms_c / args.steps,
                         "over_per_scene": value_c / per_scene["value"], "over_sequential": value_c / value,
                         "drift": drift},
+            "fp64_error": fp64,
+            "config1": config1,
             "e2e": {"value": body_steps / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "trajectory_every_frames": 2},
             "roofline": r["roofline"],
             "frame_roofline": {"bound": "hbm", "achieved": frame_ach, "peak": peak, "unit": "GB/s",
                                "frac": frame_ach / peak, "peak_source": f"{peak_kind} hbm_gbs",
                                "bytes_rule": "424 B per body + 32 B per candidate pair + 72 B per contact, per frame"},
-            "gpu_launches": int(args.steps * frames * kernels_per_frame(n, scene.n_scenes)),
+            "gpu_launches": int(args.steps * frames * kernels_per_frame(n, scene.n_scenes,
+                                                                       fused=r["fused_config"] is not None)),
+            "fused_config": r["fused_config"], "colored_fused_config": rc["fused_config"],
             "clocks": r["clocks"], "overflow_status": r["status"],
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -31,6 +31,12 @@ class Contacts(C.Structure):
                                           "norm_z", "depth", "n")] + [("capacity", C.c_uint32)]
 
 
+class FusedConfig(C.Structure):
+    _fields_ = [("smem_bytes", C.c_uint32), ("warp_teams", C.c_uint32), ("warp_scenes", C.c_uint32),
+                ("block_scenes", C.c_uint32), ("blocks", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("ms_per_frame", C.c_float), ("candidates", C.c_uint32)]
+
+
 class AABB(C.Structure):
     _fields_ = [(f, C.c_float) for f in ("min_x", "min_y", "min_z", "max_x", "max_y", "max_z")]
 
@@ -86,6 +92,9 @@ _PROTOS = {
     "dyph_wait_selftest": (_st, [C.c_int, _vp]),
     "dyph_bodies_check_finite": (_st, [C.POINTER(Bodies), _vp, _up]),
     "dyph_world_check_finite": (_st, [_vp, _vp, _up]),
+    "dyph_world_fused_config": (_st, [_vp, C.POINTER(FusedConfig)]),
+    "dyph_world_set_fused_config": (_st, [_vp, C.c_uint32, C.c_int]),
+    "dyph_world_autotune": (_st, [_vp, C.c_int32, _vp, C.POINTER(FusedConfig)]),
     "dyph_ray_query": (_st, [C.POINTER(BvhView), C.POINTER(Bodies), C.POINTER(Shapes), _vp, _vp, C.c_uint32, _vp]),
     "dyph_contact_sensor_create": (_st, [C.c_uint32, C.POINTER(_vp)]),
     "dyph_contact_sensor_destroy": (None, [_vp]),

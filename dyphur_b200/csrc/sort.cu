@@ -298,16 +298,25 @@ dyph_status radix_sort(K* keys, uint32_t* vals, size_t n, int key_bits, void* ws
 
 }  // namespace
 
+// The dynamic shared memory opt-in of the one-block sorts, set once per
+// device (a function attribute is per device).
+constexpr int kSortMaxDevices = 64;
+bool g_sort_configured[kSortMaxDevices] = {};
+std::mutex g_sort_configured_mu;
+
 dyph_status sort_prepare() {
-    static bool configured = false;
-    if (configured) return DYPH_OK;
+    int dev = 0;
+    DYPH_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kSortMaxDevices) return DYPH_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_sort_configured_mu);
+    if (g_sort_configured[dev]) return DYPH_OK;
     DYPH_CUDA_TRY(cudaFuncSetAttribute(small_sort_kernel<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(small_smem_bytes<uint32_t, true>())));
     DYPH_CUDA_TRY(cudaFuncSetAttribute(small_sort_kernel<uint64_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(small_smem_bytes<uint64_t, true>())));
     DYPH_CUDA_TRY(cudaFuncSetAttribute(small_sort_kernel<uint64_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(small_smem_bytes<uint64_t, false>())));
-    configured = true;
+    g_sort_configured[dev] = true;
     return DYPH_OK;
 }
 

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -63,6 +65,13 @@ struct dyph_world {
     uint32_t a_seg_frames = 0;
     uint32_t* a_flag = nullptr;
     uint32_t f_words_stride = 0, f_contact_slots = 0;
+    // Knobs of the fused kernel (dyph_world_set_fused_config / dyph_world_autotune).
+    std::vector<uint32_t> h_body_offset;  // host copy of the scenes' body ranges
+    uint32_t f_smem_cap = 0;              // shared memory cap per block (0 = what the largest scene needs)
+    bool f_warp_teams = true;             // small scenes one per warp, four to a block
+    uint32_t f_warp_scenes = 0, f_block_scenes = 0;
+    float f_tuned_ms = 0.f;
+    uint32_t f_tuned_candidates = 0;
 };
 
 namespace dyph {
@@ -426,8 +435,19 @@ namespace {
 // scene's own capacities when stepped alone (48 n + 64 pairs, 16 n + 64
 // contacts), and one block's shared memory for the largest scene's bodies
 // plus about two contacts per body.
+// Shared memory a block needs for the largest scene's bodies plus its pair
+// and contact words, and the least it can run with (bodies plus 64 contacts'
+// words; pair and contact lists then live in global memory).
+constexpr uint32_t kMaxSmem = 200u * 1024u;
+
+uint32_t fused_smem_need(uint32_t max_nb) {
+    return std::min(kMaxSmem, frame_body_bytes(max_nb) + (4u + kSceneWords * 4u) * 2u * std::max(64u, max_nb));
+}
+uint32_t fused_smem_floor(uint32_t max_nb) { return frame_body_bytes(max_nb) + 56u * 64u; }
+
 dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset) {
     w->fused = false;
+    w->h_body_offset.assign(body_offset, body_offset + n_scenes + 1);
     uint32_t max_nb = 0;
     std::vector<uint32_t> pb(n_scenes + 1, 0u), cb(n_scenes + 1, 0u);
     for (uint32_t i = 0; i < n_scenes; ++i) {
@@ -436,11 +456,12 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
         pb[i + 1] = pb[i] + std::max(64u, 48u * nb + 64u);
         cb[i + 1] = cb[i] + std::max(64u, 16u * nb + 64u);
     }
-    constexpr uint32_t kMaxSmem = 200u * 1024u;
-    const uint32_t body_bytes = frame_body_bytes(max_nb);
-    if (body_bytes + 56u * 64u > kMaxSmem) return DYPH_ERR_TOO_LARGE;
-    const uint32_t smem = std::min(kMaxSmem, body_bytes + (4u + kSceneWords * 4u) * 2u * std::max(64u, max_nb));
+    if (fused_smem_floor(max_nb) > kMaxSmem) return DYPH_ERR_TOO_LARGE;
+    uint32_t smem = fused_smem_need(max_nb);
+    if (w->f_smem_cap) smem = std::max(fused_smem_floor(max_nb), std::min(smem, w->f_smem_cap & ~15u));
     DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem)));
     uint32_t** bufs[] = {&w->f_pair_base, &w->f_contact_base, &w->f_pair_raw, &w->f_contact_raw, &w->f_color_raw,
                          &w->f_counts, &w->f_words, &w->f_pos};
@@ -471,7 +492,7 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     std::vector<uint32_t> small;
     for (uint32_t s : order) {
         const uint32_t nb = body_offset[s + 1] - body_offset[s];
-        if (frame_body_bytes(nb) + 146u * nb <= share) {
+        if (w->f_warp_teams && frame_body_bytes(nb) + 146u * nb <= share) {
             small.push_back(s);
         } else {
             items.insert(items.end(), {s, kItemBlock, kItemEmpty, kItemEmpty});
@@ -486,8 +507,60 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     DYPH_CUDA_TRY(cudaMemcpy(w->f_contact_base, cb.data(), cb.size() * 4, cudaMemcpyHostToDevice));
     DYPH_CUDA_TRY(cudaMemset(w->f_counts, 0, 4ull * n_scenes * sizeof(uint32_t)));
     w->frame_smem = smem;
+    w->f_warp_scenes = static_cast<uint32_t>(small.size());
+    w->f_block_scenes = n_scenes - w->f_warp_scenes;
     w->fused = true;
     return DYPH_OK;
+}
+
+void drop_graphs(dyph_world* w) {
+    if (w->graph) cudaGraphExecDestroy(w->graph);
+    if (w->episode) cudaGraphExecDestroy(w->episode);
+    w->graph = w->episode = nullptr;
+    w->episode_frames = 0;
+}
+
+void fused_report(const dyph_world* w, dyph_fused_config* out) {
+    *out = dyph_fused_config{};
+    if (!w->fused) return;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scene_frame_kernel, kSceneThreads, w->frame_smem);
+    out->smem_bytes = w->frame_smem;
+    out->warp_teams = w->f_warp_teams ? 1u : 0u;
+    out->warp_scenes = w->f_warp_scenes;
+    out->block_scenes = w->f_block_scenes;
+    out->blocks = w->f_n_items;
+    out->blocks_per_sm = static_cast<uint32_t>(per_sm);
+    out->ms_per_frame = w->f_tuned_ms;
+    out->candidates = w->f_tuned_candidates;
+}
+
+// Tuned configurations, per device and batch profile (scene sizes, solver
+// settings), for the life of the process.
+struct TunedConfig {
+    uint32_t smem_cap;
+    bool warp_teams;
+    float ms;
+};
+std::mutex g_tuned_mu;
+std::map<uint64_t, TunedConfig> g_tuned;
+
+uint64_t tune_key(const dyph_world* w) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    uint64_t h = 0xcbf29ce484222325ull;
+    auto mix = [&h](uint64_t v) {
+        for (int b = 0; b < 8; ++b) {
+            h ^= (v >> (8 * b)) & 0xFFu;
+            h *= 0x100000001b3ull;
+        }
+    };
+    mix(static_cast<uint64_t>(dev));
+    mix(static_cast<uint64_t>(w->sv->mode));
+    mix(static_cast<uint64_t>(w->sv->n_iters));
+    mix(static_cast<uint64_t>(w->desc.integrator.n_substeps));
+    for (uint32_t v : w->h_body_offset) mix(v);
+    return h;
 }
 
 }  // namespace
@@ -508,6 +581,131 @@ extern "C" dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s) {
     DYPH_CUDA_TRY(cudaEventRecord(w->ev_out, w->stream));
     DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->ev_out, 0));
     return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config* out) {
+    if (!w || !out) return DYPH_ERR_INVALID;
+    fused_report(w, out);
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams) {
+    if (!w || !w->fused) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    w->f_smem_cap = smem_cap;
+    w->f_warp_teams = warp_teams != 0;
+    const std::vector<uint32_t> off = w->h_body_offset;
+    dyph_status st = setup_fused(w, static_cast<uint32_t>(off.size() - 1), off.data());
+    drop_graphs(w);
+    return st;
+}
+
+extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out) {
+    if (!w || !w->fused || frames <= 0) return DYPH_ERR_INVALID;
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
+    DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    DYPH_CUDA_TRY(cudaStreamSynchronize(cs));
+    const uint64_t key = tune_key(w);
+    {
+        std::lock_guard<std::mutex> lock(g_tuned_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            dyph_status st = dyph_world_set_fused_config(w, it->second.smem_cap, it->second.warp_teams);
+            w->f_tuned_ms = it->second.ms;
+            w->f_tuned_candidates = 0;  // taken from the cache
+            if (out) fused_report(w, out);
+            return st;
+        }
+    }
+    const size_t n = w->desc.bodies.n;
+    uint32_t max_nb = 0;
+    for (size_t k = 0; k + 1 < w->h_body_offset.size(); ++k)
+        max_nb = std::max(max_nb, w->h_body_offset[k + 1] - w->h_body_offset[k]);
+    // The state, the statistics and the phase timer are put back after the trials.
+    float* saved = nullptr;
+    uint32_t saved_stats[5];
+    if (cudaMalloc(&saved, 13 * n * sizeof(float)) != cudaSuccess) return DYPH_ERR_NOMEM;
+    float* rows[13] = {w->desc.bodies.pos_x, w->desc.bodies.pos_y, w->desc.bodies.pos_z, w->desc.bodies.rot_w,
+                       w->desc.bodies.rot_x, w->desc.bodies.rot_y, w->desc.bodies.rot_z, w->desc.bodies.vel_x,
+                       w->desc.bodies.vel_y, w->desc.bodies.vel_z, w->desc.bodies.ang_x, w->desc.bodies.ang_y,
+                       w->desc.bodies.ang_z};
+    auto copy_rows = [&](bool save) -> cudaError_t {
+        for (int r = 0; r < 13; ++r) {
+            cudaError_t e = save ? cudaMemcpyAsync(saved + r * n, rows[r], n * 4, cudaMemcpyDeviceToDevice, w->stream)
+                                 : cudaMemcpyAsync(rows[r], saved + r * n, n * 4, cudaMemcpyDeviceToDevice, w->stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    dyph_status st = DYPH_OK;
+    unsigned long long* phase = w->f_phase;
+    w->f_phase = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const uint32_t need = fused_smem_need(max_nb), floor_ = fused_smem_floor(max_nb);
+    std::vector<uint32_t> caps = {need};
+    for (uint32_t c : {96u << 10, 72u << 10, 56u << 10, 48u << 10, 40u << 10, 32u << 10})
+        if (c < need && c >= floor_) caps.push_back(c);
+    TunedConfig best{need, true, 1e30f};
+    uint32_t tried = 0;
+    const uint32_t cap0 = w->f_smem_cap;
+    const bool teams0 = w->f_warp_teams;
+    do {
+        if (cudaMemcpyAsync(saved_stats, w->stats, sizeof(saved_stats), cudaMemcpyDeviceToHost, w->stream) !=
+                cudaSuccess ||
+            copy_rows(true) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+            cudaEventCreate(&e1) != cudaSuccess) {
+            st = DYPH_ERR_CUDA;
+            break;
+        }
+        for (uint32_t cap : caps) {
+            for (int teams = 1; teams >= 0 && st == DYPH_OK; --teams) {
+                w->f_smem_cap = cap;
+                w->f_warp_teams = teams != 0;
+                st = setup_fused(w, static_cast<uint32_t>(w->h_body_offset.size() - 1), w->h_body_offset.data());
+                if (st != DYPH_OK) break;
+                // one untimed frame, then the timed ones, each trial from the saved state
+                for (int f = 0; f <= frames && st == DYPH_OK; ++f) {
+                    if (f == 1 && cudaEventRecord(e0, w->stream) != cudaSuccess) st = DYPH_ERR_CUDA;
+                    if (st == DYPH_OK) st = enqueue_frame(w, w->stream);
+                }
+                if (st == DYPH_OK && cudaEventRecord(e1, w->stream) != cudaSuccess) st = DYPH_ERR_CUDA;
+                if (st == DYPH_OK && (copy_rows(false) != cudaSuccess || cudaStreamSynchronize(w->stream) != cudaSuccess))
+                    st = DYPH_ERR_CUDA;
+                float ms = 0.f;
+                if (st == DYPH_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) st = DYPH_ERR_CUDA;
+                if (st != DYPH_OK) break;
+                ++tried;
+                ms /= static_cast<float>(frames);
+                if (ms < best.ms) best = TunedConfig{cap, teams != 0, ms};
+            }
+            if (st != DYPH_OK) break;
+        }
+    } while (false);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    w->f_phase = phase;
+    if (st == DYPH_OK) {
+        w->f_smem_cap = best.smem_cap;
+        w->f_warp_teams = best.warp_teams;
+    } else {
+        w->f_smem_cap = cap0;
+        w->f_warp_teams = teams0;
+    }
+    const dyph_status st2 = setup_fused(w, static_cast<uint32_t>(w->h_body_offset.size() - 1), w->h_body_offset.data());
+    drop_graphs(w);
+    if (st == DYPH_OK && st2 == DYPH_OK) {
+        if (cudaMemcpyAsync(w->stats, saved_stats, sizeof(saved_stats), cudaMemcpyHostToDevice, w->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(w->stream) != cudaSuccess)
+            st = DYPH_ERR_CUDA;
+        w->f_tuned_ms = best.ms;
+        w->f_tuned_candidates = tried;
+        std::lock_guard<std::mutex> lock(g_tuned_mu);
+        g_tuned[key] = best;
+    }
+    cudaFree(saved);
+    if (out) fused_report(w, out);
+    return st != DYPH_OK ? st : st2;
 }
 
 extern "C" dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset,

@@ -536,6 +536,24 @@ class World:
         check(capi.lib().dyph_narrowphase_download_count(self._np, None, C.byref(a), C.byref(b)))
         return read_contacts(v, int(a.value))
 
+    def fused_config(self) -> dict:
+        """Knobs of the fused batched frame in force (dyph_world_fused_config)."""
+        c = capi.FusedConfig()
+        check(capi.lib().dyph_world_fused_config(self.h, C.byref(c)), "dyph_world_fused_config")
+        return {k: getattr(c, k) for k, _ in capi.FusedConfig._fields_}
+
+    def set_fused_config(self, smem_cap: int, warp_teams: bool = True) -> None:
+        check(capi.lib().dyph_world_set_fused_config(self.h, int(smem_cap), int(bool(warp_teams))),
+              "dyph_world_set_fused_config")
+
+    def autotune(self, frames: int = 16, stream=None) -> dict:
+        """Time the fused kernel's configurations from the current state and keep
+        the fastest (dyph_world_autotune); returns the chosen configuration."""
+        c = capi.FusedConfig()
+        check(capi.lib().dyph_world_autotune(self.h, int(frames), _stream_ptr(stream), C.byref(c)),
+              "dyph_world_autotune")
+        return {k: getattr(c, k) for k, _ in capi.FusedConfig._fields_}
+
     # The rollout protocol of dyphur_b200.autograd (shared with dyphur_py.World).
     def count(self) -> int:
         return self.bodies.n

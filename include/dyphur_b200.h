@@ -215,7 +215,11 @@ dyph_status dyph_sort_by_key_u32_u32(uint32_t* keys, uint32_t* values, size_t n,
  *
  * There is one scratch array per device: calls that overlap on a device (two
  * streams, two host threads, or two graph launches in flight together) race
- * on it and give wrong results. Serialise them, e.g. on one stream. */
+ * on it and give wrong results. Serialise them, e.g. on one stream.
+ *
+ * The looked-up address is kept per device index for the life of the
+ * process: do not call this entry point on a device after cudaDeviceReset
+ * has torn down the context it was first called in. */
 #define DYPH_SORT_NOALLOC_MAX_KEYS 262144u
 dyph_status dyph_sort_by_key_u64_u32_noalloc(uint64_t* keys, uint32_t* values, size_t n, dyph_stream s);
 
@@ -389,6 +393,35 @@ dyph_status dyph_world_set_scenes(dyph_world* w, uint32_t n_scenes, const uint32
  * list, the narrowphase's ContactView and the solver's colours (queued on s;
  * no-op for other worlds). Call it before reading those lists. */
 dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
+/* Knobs of the fused batched frame (no reference counterpart). Every setting
+ * gives the same results bit for bit; they move only where a scene's pair and
+ * contact words live (shared memory, or global memory past the cap) and how
+ * many blocks fit an SM:
+ *   smem_bytes     dynamic shared memory per block: what the largest scene
+ *                  needs, or less (smem_cap), down to its bodies plus 64
+ *                  contacts' words;
+ *   warp_teams     scenes whose frame fits a quarter of that run one per
+ *                  warp, four to a block (else every scene takes a block).
+ * dyph_world_autotune times `frames` frames of each candidate (smem caps
+ * 96/72/56/48/40/32 KB below the need, warp teams on and off) from the
+ * world's current state, keeps the fastest, and puts the state and the
+ * statistics back; the choice is cached per device and batch profile (scene
+ * sizes, solver mode, iterations, substeps) for the life of the process, so
+ * a second world of the same profile takes it without timing (candidates 0).
+ * Blocking; drops captured frames. */
+typedef struct dyph_fused_config {
+    uint32_t smem_bytes;    /* dynamic shared memory per block */
+    uint32_t warp_teams;    /* 1: small scenes one per warp */
+    uint32_t warp_scenes;   /* scenes run by one warp */
+    uint32_t block_scenes;  /* scenes run by a whole block */
+    uint32_t blocks;        /* thread blocks per frame */
+    uint32_t blocks_per_sm; /* resident blocks per SM at smem_bytes */
+    float ms_per_frame;     /* the autotuner's measurement (0 when not tuned) */
+    uint32_t candidates;    /* configurations the autotuner timed (0: cached or not tuned) */
+} dyph_fused_config;
+dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config* out);
+dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams);
+dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out);
 /* Phase timing of fused batched frames, the per-stage table of the
  * reference's --profile mode (examples/stress_test_blocks/main.cpp:199-254)
  * for a frame that is one kernel: with it on, every scene's team leader adds

@@ -24,6 +24,8 @@
 //                      body pair, inclusive overlap (:322-325), ascending (a, b)
 //   narrowphase        core/src/narrowphase.cpp:46-306, 920-1001
 //   solve              core/src/xpbd_solver.cpp:40-133, 413-521, 559-587
+//   colour order       (dyd_fp64_run) Jones–Plassmann colours, :620-733
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -31,7 +33,12 @@
 
 namespace {
 
-constexpr int kMaxT = 96;  // tangents carried (gradient parameters per call)
+// Tangents carried (gradient parameters per call). The FP64 re-run library
+// (libdyphur_fp64.so, dyd_fp64_run) is this file built with DYD_MAX_T=1.
+#ifndef DYD_MAX_T
+#define DYD_MAX_T 96
+#endif
+constexpr int kMaxT = DYD_MAX_T;
 int g_nt = 0;              // tangents in use
 bool g_at_float = false;   // evaluate the chain-rule coefficients at the float values
 
@@ -501,7 +508,12 @@ void solve_contact(std::vector<Body>& Bs, const Contact& ct, float mu, TD& lc, f
         TD vt2 = vtx * vtx + vty * vty + vtz * vtz;
         if (vt2.f > 1e-12f) {
             TD vt_len = tsqrt(vt2);
-            TD tx = vtx / vt_len, ty = vty / vt_len, tz = vtz / vt_len;
+            // Where the FP64 slip is exactly zero the float run's slip is
+            // rounding noise: the FP64 impulse j_t = |vt| / wt is 0 and the
+            // direction is immaterial, so divide by 1 there instead of 0.
+            TD dir_len = vt_len;
+            if (dir_len.v == 0.0) dir_len.v = 1.0;
+            TD tx = vtx / dir_len, ty = vty / dir_len, tz = vtz / dir_len;
             TD ratx = ray * tz - raz * ty, raty = raz * tx - rax * tz, ratz = rax * ty - ray * tx;
             TD rbtx = rby * tz - rbz * ty, rbty = rbz * tx - rbx * tz, rbtz = rbx * ty - rby * tx;
             TD fax, fay, faz, fbx, fby, fbz;
@@ -597,6 +609,142 @@ int dyd_rollout(uint32_t n, const float* state13, const float* inv_mass, const f
     }
     *loss = L.v;
     for (int p = 0; p < n_params; ++p) grad[p] = L.d[p];
+    for (uint32_t i = 0; i < n; ++i) {
+        const Body& B = Bs[i];
+        const TD* rows[13] = {&B.p[0], &B.p[1], &B.p[2], &B.q[0], &B.q[1], &B.q[2], &B.q[3],
+                              &B.v[0], &B.v[1], &B.v[2], &B.w[0], &B.w[1], &B.w[2]};
+        for (int r = 0; r < 13; ++r) {
+            final_f[static_cast<size_t>(r) * n + i] = rows[r]->f;
+            final_v[static_cast<size_t>(r) * n + i] = rows[r]->v;
+        }
+    }
+    return 0;
+}
+
+// FP64 re-run of the frame step along the float run's decisions, with the
+// solver order of `mode`: 0 the reference's (serial at <= 256 contacts, else
+// Jones–Plassmann colours, serial when the colouring fails), 1 serial, 2
+// colours at every contact count (core/src/xpbd_solver.cpp:603-733; colours
+// from the float run's contact list). Per frame f: err_pos[f] = max over
+// bodies of |x_float - x_fp64| (m), err_rot[f] = max over bodies of the
+// quaternion component error. With `local`, every frame's FP64 run starts
+// from the float state the frame starts from, so err_* is that frame's own
+// rounding error; without it the FP64 state is carried and err_* is the
+// accumulated error. Final float state and FP64 values as dyd_rollout.
+int dyd_fp64_run(uint32_t n, const float* state13, const float* inv_mass, const float* iI6, const uint32_t* type,
+                 const float* half3, const uint32_t* flags, int n_frames, float dt, const float* gravity, int n_sub,
+                 int n_iters, float mu, int mode, int local, double* err_pos, double* err_rot, float* final_f,
+                 double* final_v) {
+    g_nt = 0;
+    g_at_float = false;
+    std::vector<Body> Bs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        Body& B = Bs[i];
+        TD* rows[13] = {&B.p[0], &B.p[1], &B.p[2], &B.q[0], &B.q[1], &B.q[2], &B.q[3],
+                        &B.v[0], &B.v[1], &B.v[2], &B.w[0], &B.w[1], &B.w[2]};
+        for (int r = 0; r < 13; ++r) *rows[r] = cst(state13[static_cast<size_t>(r) * n + i]);
+        B.m = cst(inv_mass[i]);
+        for (int k = 0; k < 6; ++k) B.I[k] = iI6[static_cast<size_t>(k) * n + i];
+        B.type = type[i];
+        B.flags = flags[i];
+        for (int k = 0; k < 3; ++k) B.h[k] = half3[static_cast<size_t>(k) * n + i];
+    }
+    float g[3] = {gravity[0], gravity[1], gravity[2]};
+    const float sub_dt = dt / static_cast<float>(n_sub), half_dt = 0.5f * sub_dt;
+    std::vector<float> box(6 * n);
+    std::vector<Contact> contacts;
+    std::vector<uint32_t> color;
+    std::vector<uint64_t> bpri(n), bmask(n);
+    for (int f = 0; f < n_frames; ++f) {
+        if (local)
+            for (auto& B : Bs) {
+                TD* rows[13] = {&B.p[0], &B.p[1], &B.p[2], &B.q[0], &B.q[1], &B.q[2], &B.q[3],
+                                &B.v[0], &B.v[1], &B.v[2], &B.w[0], &B.w[1], &B.w[2]};
+                for (TD* r : rows) r->v = r->f;
+            }
+        for (auto& B : Bs) integrate(B, g, sub_dt, half_dt, n_sub);
+        for (uint32_t i = 0; i < n; ++i) leaf_box(Bs[i], &box[6 * i]);
+        contacts.clear();
+        for (uint32_t a = 0; a < n; ++a)
+            for (uint32_t b = a + 1; b < n; ++b) {
+                if (!overlap(&box[6 * b], &box[6 * a])) continue;
+                Contact c;
+                if (process_pair(Bs, a, b, c)) contacts.push_back(c);
+            }
+        const uint32_t nc = static_cast<uint32_t>(contacts.size());
+        if (nc > 0) {
+            // Jones–Plassmann colours of the float run (priorities hash(k) << 32 | k,
+            // 8 rounds per batch, at most 256 rounds and 64 colours).
+            uint32_t n_colors = 0;
+            if (mode == 2 || (mode == 0 && nc > 256u)) {
+                const uint32_t UNC = 0xFFFFFFFFu;
+                color.assign(nc, UNC);
+                std::fill(bmask.begin(), bmask.end(), 0ull);
+                uint32_t max_color = 0, rem = nc, r = 0;
+                bool overflow = false;
+                auto hash_u32 = [](uint32_t x) {
+                    x ^= x >> 16; x *= 0x85ebca6bu; x ^= x >> 13; x *= 0xc2b2ae35u; x ^= x >> 16;
+                    return x;
+                };
+                auto dyn = [&](uint32_t b) { return Bs[b].m.f != 0.f; };
+                while (rem > 0 && r < 256u) {
+                    for (uint32_t bi = 0; bi < 8u && r < 256u; ++bi, ++r) {
+                        std::fill(bpri.begin(), bpri.end(), 0ull);
+                        for (uint32_t k = 0; k < nc; ++k) {
+                            if (color[k] != UNC) continue;
+                            const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
+                            const uint32_t a = contacts[k].a, b = contacts[k].b;
+                            if (dyn(a) && bpri[a] < pk) bpri[a] = pk;
+                            if (dyn(b) && bpri[b] < pk) bpri[b] = pk;
+                        }
+                        for (uint32_t k = 0; k < nc; ++k) {
+                            if (color[k] != UNC) continue;
+                            const uint32_t a = contacts[k].a, b = contacts[k].b;
+                            const bool da = dyn(a), db = dyn(b);
+                            const uint64_t pk = (static_cast<uint64_t>(hash_u32(k)) << 32) | k;
+                            if ((da && bpri[a] != pk) || (db && bpri[b] != pk)) continue;
+                            const uint64_t used = (da ? bmask[a] : 0ull) | (db ? bmask[b] : 0ull);
+                            const uint64_t freebits = ~used;
+                            if (freebits == 0ull) {
+                                overflow = true;
+                                continue;
+                            }
+                            const uint32_t col = static_cast<uint32_t>(__builtin_ctzll(freebits));
+                            color[k] = col;
+                            if (da) bmask[a] |= 1ull << col;
+                            if (db) bmask[b] |= 1ull << col;
+                            max_color = std::max(max_color, col);
+                            --rem;
+                        }
+                    }
+                }
+                n_colors = (rem > 0 || overflow) ? 0u : max_color + 1u;
+            }
+            std::vector<TD> lam(nc, cst(0.f));
+            for (int it = 0; it < n_iters; ++it) {
+                if (n_colors == 0) {
+                    for (uint32_t c = 0; c < nc; ++c) solve_contact(Bs, contacts[c], mu, lam[c], dt);
+                } else {
+                    for (uint32_t ci = 0; ci < n_colors; ++ci)
+                        for (uint32_t c = 0; c < nc; ++c)
+                            if (color[c] == ci) solve_contact(Bs, contacts[c], mu, lam[c], dt);
+                }
+                for (auto& B : Bs) renormalize(B.q);
+            }
+        }
+        double ep = 0.0, er = 0.0;
+        for (const Body& B : Bs) {
+            double d2 = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                const double d = static_cast<double>(B.p[k].f) - B.p[k].v;
+                d2 += d * d;
+            }
+            ep = std::max(ep, std::sqrt(d2));
+            for (int k = 0; k < 4; ++k) er = std::max(er, std::fabs(static_cast<double>(B.q[k].f) - B.q[k].v));
+        }
+        err_pos[f] = ep;
+        err_rot[f] = er;
+    }
     for (uint32_t i = 0; i < n; ++i) {
         const Body& B = Bs[i];
         const TD* rows[13] = {&B.p[0], &B.p[1], &B.p[2], &B.q[0], &B.q[1], &B.q[2], &B.q[3],

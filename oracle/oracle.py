@@ -17,6 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libdyphur_oracle.so")
+FP64_SO = os.path.join(HERE, "_build", "libdyphur_fp64.so")
 DUAL_SO = os.path.join(HERE, "_build", "libdyphur_dual.so")
 REF_SO = os.path.join(HERE, "_ref", "libdyphur_ref.so")
 
@@ -39,8 +40,9 @@ class _Scene(ctypes.Structure):
 def build_oracle() -> str:
     """Compile the C restatement if needed (gcc only; works on any host)."""
     srcs = [os.path.join(HERE, f) for f in ("dyphur_oracle.c", "dual_oracle.cpp")]
-    stale = any(not os.path.exists(so) for so in (ORACLE_SO, DUAL_SO)) or \
-        os.path.getmtime(ORACLE_SO) < os.path.getmtime(srcs[0]) or os.path.getmtime(DUAL_SO) < os.path.getmtime(srcs[1])
+    stale = any(not os.path.exists(so) for so in (ORACLE_SO, DUAL_SO, FP64_SO)) or \
+        os.path.getmtime(ORACLE_SO) < os.path.getmtime(srcs[0]) or \
+        min(os.path.getmtime(DUAL_SO), os.path.getmtime(FP64_SO)) < os.path.getmtime(srcs[1])
     if stale:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return ORACLE_SO
@@ -87,6 +89,38 @@ def dual_rollout(state13, inv_mass, iI6, shape_type, half3, flags, n_frames, dt,
     if rc != 0:
         raise ValueError("too many gradient parameters for the dual-number oracle")
     return loss.value, grad, fin_f, fin_v
+
+
+def fp64_run(state13, inv_mass, iI6, shape_type, half3, flags, n_frames, dt, gravity, n_substeps, n_iters, mu,
+             mode=SOLVER_SERIAL, local=True):
+    """FP64 re-run of one scene's frame step along the float run's decisions
+    (oracle/dual_oracle.cpp, dyd_fp64_run) in solver order `mode` (0 the
+    reference's, 1 serial, 2 coloured). local: each frame's FP64 run starts
+    from the float state (the frame's own rounding error); otherwise the FP64
+    state is carried (the accumulated error, which contact-rich scenes amplify
+    without bound). Returns (err_pos [n_frames] = max |x_float - x_fp64| per
+    frame in m, err_rot [n_frames] = max quaternion component error, final
+    float state [13, n], final FP64 state [13, n])."""
+    build_oracle()
+    L = ctypes.CDLL(FP64_SO)
+    f = L.dyd_fp64_run
+    f.restype = ctypes.c_int
+    n = int(np.asarray(inv_mass).shape[0])
+    arrs = [np.ascontiguousarray(state13, np.float32), np.ascontiguousarray(inv_mass, np.float32),
+            np.ascontiguousarray(iI6, np.float32), np.ascontiguousarray(shape_type, np.uint32),
+            np.ascontiguousarray(half3, np.float32), np.ascontiguousarray(flags, np.uint32),
+            np.ascontiguousarray(gravity, np.float32)]
+    ep = np.zeros(n_frames, np.float64)
+    er = np.zeros(n_frames, np.float64)
+    fin_f = np.zeros((13, n), np.float32)
+    fin_v = np.zeros((13, n), np.float64)
+    vp = ctypes.c_void_p
+    f.argtypes = [ctypes.c_uint32] + [vp] * 6 + [ctypes.c_int, ctypes.c_float, vp, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+    f(n, *[a.ctypes.data for a in arrs[:6]], int(n_frames), float(dt), arrs[6].ctypes.data, int(n_substeps),
+      int(n_iters), float(mu), int(mode), int(bool(local)), ep.ctypes.data, er.ctypes.data, fin_f.ctypes.data,
+      fin_v.ctypes.data)
+    return ep, er, fin_f, fin_v
 
 
 def ref_available() -> bool:
