@@ -486,7 +486,13 @@ def probe_flow_kernel(w, frames, mode, torch, fused=False):
 def gpu_workload(scene, mode, frames, args, torch, barrier, clocks=None, roofline=True):
     from dyphur_b200 import device
     w = device.World(scene, mode=mode)
-    tuned = w.autotune(16) if scene.n_scenes > 1 else None  # before the episode is captured
+    tuned = None
+    if scene.n_scenes > 1:  # tuned on settled frames, before the episode is captured
+        init = w.bodies.fbuf.clone()
+        w.step(min(120, frames))
+        tuned = w.autotune(16)
+        w.bodies.fbuf.copy_(init)
+        torch.cuda.synchronize()
     w.capture_episode(frames, -1)
     ms, ck, init = timed_episodes(w, args.steps, args.warmup, torch, barrier, clocks)
     st = w.stats()

@@ -314,9 +314,15 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
 constexpr uint32_t kItemEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kItemBlock = 0xFFFFFFFEu;
 
-__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_kernel(SceneBufs S, FrameBufs F, FrameParams P_,
-                                                                       const uint32_t* __restrict__ items,
-                                                                       uint32_t n_items) {
+// kMinBlocks is the register budget: 4 resident blocks per SM (128
+// registers a thread), 5 (96) or 6 (80, a few bytes spilled). Which one runs
+// best depends on the batch (dyph_world_autotune picks it with the shared
+// memory cap); all three compute the same frames.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kSceneThreads, kMinBlocks) scene_frame_kernel(SceneBufs S, FrameBufs F,
+                                                                                FrameParams P_,
+                                                                                const uint32_t* __restrict__ items,
+                                                                                uint32_t n_items) {
     extern __shared__ __align__(16) unsigned char scene_smem[];
     __shared__ SceneShared sh[kSceneThreads / 32];
     const uint32_t warp = threadIdx.x >> 5;

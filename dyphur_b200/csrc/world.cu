@@ -69,6 +69,7 @@ struct dyph_world {
     std::vector<uint32_t> h_body_offset;  // host copy of the scenes' body ranges
     uint32_t f_smem_cap = 0;              // shared memory cap per block (0 = what the largest scene needs)
     bool f_warp_teams = true;             // small scenes one per warp, four to a block
+    uint32_t f_variant = 0;               // register budget: 4 (0), 5 (1) or 6 (2) blocks per SM
     uint32_t f_warp_scenes = 0, f_block_scenes = 0;
     float f_tuned_ms = 0.f;
     uint32_t f_tuned_candidates = 0;
@@ -165,7 +166,19 @@ dyph_status enqueue_frame(dyph_world* w, cudaStream_t s, int probe_stage = -1, v
         FrameParams P{d.bodies, d.shapes, ip.gravity[0], ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt,
                       w->sv->friction, ip.dt, ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters,
                       w->sv->meta, w->bp->counts, w->np->counts, w->stats + 4, w->f_phase};
-        scene_frame_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, s>>>(S, F, P, w->f_items, w->f_n_items);
+        switch (w->f_variant) {
+            case 1:
+                scene_frame_kernel<5><<<w->f_n_items, kSceneThreads, w->frame_smem, s>>>(S, F, P, w->f_items,
+                                                                                       w->f_n_items);
+                break;
+            case 2:
+                scene_frame_kernel<6><<<w->f_n_items, kSceneThreads, w->frame_smem, s>>>(S, F, P, w->f_items,
+                                                                                       w->f_n_items);
+                break;
+            default:
+                scene_frame_kernel<4><<<w->f_n_items, kSceneThreads, w->frame_smem, s>>>(S, F, P, w->f_items,
+                                                                                       w->f_n_items);
+        }
         DYPH_CUDA_TRY(cudaGetLastError());
         if (probe_stage >= 0 && (st = probe_record(ev1, s)) != DYPH_OK) return st;
         frame_stats_kernel<<<1, 1, 0, s>>>(w->bp->counts, w->np->counts, w->bp->max_pairs, w->np->max_contacts,
@@ -459,8 +472,10 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     if (fused_smem_floor(max_nb) > kMaxSmem) return DYPH_ERR_TOO_LARGE;
     uint32_t smem = fused_smem_need(max_nb);
     if (w->f_smem_cap) smem = std::max(fused_smem_floor(max_nb), std::min(smem, w->f_smem_cap & ~15u));
-    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem)));
+    for (const void* k : {reinterpret_cast<const void*>(scene_frame_kernel<4>),
+                          reinterpret_cast<const void*>(scene_frame_kernel<5>),
+                          reinterpret_cast<const void*>(scene_frame_kernel<6>)})
+        DYPH_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem)));
     uint32_t** bufs[] = {&w->f_pair_base, &w->f_contact_base, &w->f_pair_raw, &w->f_contact_raw, &w->f_color_raw,
@@ -524,13 +539,17 @@ void fused_report(const dyph_world* w, dyph_fused_config* out) {
     *out = dyph_fused_config{};
     if (!w->fused) return;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scene_frame_kernel, kSceneThreads, w->frame_smem);
+    const void* k = w->f_variant == 1   ? reinterpret_cast<const void*>(scene_frame_kernel<5>)
+                    : w->f_variant == 2 ? reinterpret_cast<const void*>(scene_frame_kernel<6>)
+                                        : reinterpret_cast<const void*>(scene_frame_kernel<4>);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kSceneThreads, w->frame_smem);
     out->smem_bytes = w->frame_smem;
     out->warp_teams = w->f_warp_teams ? 1u : 0u;
     out->warp_scenes = w->f_warp_scenes;
     out->block_scenes = w->f_block_scenes;
     out->blocks = w->f_n_items;
     out->blocks_per_sm = static_cast<uint32_t>(per_sm);
+    out->register_blocks = 4u + w->f_variant;
     out->ms_per_frame = w->f_tuned_ms;
     out->candidates = w->f_tuned_candidates;
 }
@@ -540,6 +559,7 @@ void fused_report(const dyph_world* w, dyph_fused_config* out) {
 struct TunedConfig {
     uint32_t smem_cap;
     bool warp_teams;
+    uint32_t variant;
     float ms;
 };
 std::mutex g_tuned_mu;
@@ -589,11 +609,14 @@ extern "C" dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config*
     return DYPH_OK;
 }
 
-extern "C" dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams) {
-    if (!w || !w->fused) return DYPH_ERR_INVALID;
+extern "C" dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams,
+                                                   uint32_t register_blocks) {
+    if (!w || !w->fused || (register_blocks != 0 && (register_blocks < 4 || register_blocks > 6)))
+        return DYPH_ERR_INVALID;
     DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
     w->f_smem_cap = smem_cap;
     w->f_warp_teams = warp_teams != 0;
+    w->f_variant = register_blocks ? register_blocks - 4u : 0u;
     const std::vector<uint32_t> off = w->h_body_offset;
     dyph_status st = setup_fused(w, static_cast<uint32_t>(off.size() - 1), off.data());
     drop_graphs(w);
@@ -610,7 +633,8 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
         std::lock_guard<std::mutex> lock(g_tuned_mu);
         auto it = g_tuned.find(key);
         if (it != g_tuned.end()) {
-            dyph_status st = dyph_world_set_fused_config(w, it->second.smem_cap, it->second.warp_teams);
+            dyph_status st =
+                dyph_world_set_fused_config(w, it->second.smem_cap, it->second.warp_teams, 4u + it->second.variant);
             w->f_tuned_ms = it->second.ms;
             w->f_tuned_candidates = 0;  // taken from the cache
             if (out) fused_report(w, out);
@@ -645,9 +669,9 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
     std::vector<uint32_t> caps = {need};
     for (uint32_t c : {96u << 10, 72u << 10, 56u << 10, 48u << 10, 40u << 10, 32u << 10})
         if (c < need && c >= floor_) caps.push_back(c);
-    TunedConfig best{need, true, 1e30f};
+    TunedConfig best{need, true, 0u, 1e30f};
     uint32_t tried = 0;
-    const uint32_t cap0 = w->f_smem_cap;
+    const uint32_t cap0 = w->f_smem_cap, variant0 = w->f_variant;
     const bool teams0 = w->f_warp_teams;
     do {
         if (cudaMemcpyAsync(saved_stats, w->stats, sizeof(saved_stats), cudaMemcpyDeviceToHost, w->stream) !=
@@ -658,9 +682,12 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
             break;
         }
         for (uint32_t cap : caps) {
-            for (int teams = 1; teams >= 0 && st == DYPH_OK; --teams) {
+            for (uint32_t combo = 0; combo < 6u && st == DYPH_OK; ++combo) {
+                const int teams = combo < 3u ? 1 : 0;
+                const uint32_t variant = combo % 3u;
                 w->f_smem_cap = cap;
                 w->f_warp_teams = teams != 0;
+                w->f_variant = variant;
                 st = setup_fused(w, static_cast<uint32_t>(w->h_body_offset.size() - 1), w->h_body_offset.data());
                 if (st != DYPH_OK) break;
                 // one untimed frame, then the timed ones, each trial from the saved state
@@ -676,7 +703,7 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
                 if (st != DYPH_OK) break;
                 ++tried;
                 ms /= static_cast<float>(frames);
-                if (ms < best.ms) best = TunedConfig{cap, teams != 0, ms};
+                if (ms < best.ms) best = TunedConfig{cap, teams != 0, variant, ms};
             }
             if (st != DYPH_OK) break;
         }
@@ -687,9 +714,11 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
     if (st == DYPH_OK) {
         w->f_smem_cap = best.smem_cap;
         w->f_warp_teams = best.warp_teams;
+        w->f_variant = best.variant;
     } else {
         w->f_smem_cap = cap0;
         w->f_warp_teams = teams0;
+        w->f_variant = variant0;
     }
     const dyph_status st2 = setup_fused(w, static_cast<uint32_t>(w->h_body_offset.size() - 1), w->h_body_offset.data());
     drop_graphs(w);

@@ -4,7 +4,8 @@ stress_test_blocks example (examples/stress_test_blocks/main.cpp).
     python -m dyphur_b200.run [out_prefix] [n_frames] [--grid NX NY NZ]
                               [--spacing S] [--jitter J] [--profile]
                               [--workload blocks|pile|batch] [--mode M]
-                              [--start-frame F]
+                              [--start-frame F] [--smem-cap B] [--no-warp-teams]
+                              [--autotune FRAMES]
 
 Writes <prefix>.scene, <prefix>.trajectory (poses every other frame),
 <prefix>.metrics.json and <prefix>.golden exactly as the example does. The
@@ -42,6 +43,13 @@ def parse(argv=None):
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--start-frame", type=int, default=0)
     ap.add_argument("--no-output", action="store_true", help="write no files")
+    ap.add_argument("--smem-cap", type=int, default=None,
+                    help="batch: shared memory cap per block of the fused frame (bytes; 0 = what it needs)")
+    ap.add_argument("--no-warp-teams", action="store_true", help="batch: every scene takes a whole block")
+    ap.add_argument("--register-blocks", type=int, default=0, choices=[0, 4, 5, 6],
+                    help="batch: register budget of the fused frame kernel (resident blocks per SM)")
+    ap.add_argument("--autotune", type=int, default=0, metavar="FRAMES",
+                    help="batch: autotune the fused frame on FRAMES frames (after --start-frame) first")
     return ap.parse_args(argv)
 
 
@@ -110,11 +118,22 @@ def main(argv=None) -> int:
     scene = build_scene(args)
     n = scene.n_bodies
     world = device.World(scene, mode=mode)
+    if args.smem_cap is not None or args.no_warp_teams or args.register_blocks:
+        world.set_fused_config(args.smem_cap or 0, not args.no_warp_teams, args.register_blocks)
+    if args.autotune:
+        init = world.bodies.fbuf.clone()
+        world.step(args.start_frame)
+        cfg = world.autotune(args.autotune)
+        world.bodies.fbuf.copy_(init)
+        torch.cuda.synchronize()
+        print(f"fused frame configuration: {cfg}")
     if args.start_frame:
         world.step(args.start_frame)
         world.step(args.n_frames)
         torch.cuda.synchronize()
-        print(f"stepped {args.start_frame} + {args.n_frames} frames, status {world.stats()['status']}")
+        st = world.stats()
+        print(f"stepped {args.start_frame} + {args.n_frames} frames, status {st['status']}, last frame "
+              f"{st['last_pairs']} candidate pairs, {st['last_contacts']} contacts, {n} bodies")
         return 0
     if args.profile:
         profile(world, scene, args.n_frames)

@@ -401,9 +401,12 @@ dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
  *                  needs, or less (smem_cap), down to its bodies plus 64
  *                  contacts' words;
  *   warp_teams     scenes whose frame fits a quarter of that run one per
- *                  warp, four to a block (else every scene takes a block).
+ *                  warp, four to a block (else every scene takes a block);
+ *   register_blocks the kernel's register budget: 4, 5 or 6 resident blocks
+ *                  per SM (128, 96 or 80 registers a thread; 0 = 4).
  * dyph_world_autotune times `frames` frames of each candidate (smem caps
- * 96/72/56/48/40/32 KB below the need, warp teams on and off) from the
+ * 96/72/56/48/40/32 KB below the need, warp teams on and off, each register
+ * budget) from the
  * world's current state, keeps the fastest, and puts the state and the
  * statistics back; the choice is cached per device and batch profile (scene
  * sizes, solver mode, iterations, substeps) for the life of the process, so
@@ -415,12 +418,13 @@ typedef struct dyph_fused_config {
     uint32_t warp_scenes;   /* scenes run by one warp */
     uint32_t block_scenes;  /* scenes run by a whole block */
     uint32_t blocks;        /* thread blocks per frame */
-    uint32_t blocks_per_sm; /* resident blocks per SM at smem_bytes */
+    uint32_t blocks_per_sm; /* resident blocks per SM at smem_bytes and the register budget */
+    uint32_t register_blocks; /* the kernel variant's register budget (blocks per SM) */
     float ms_per_frame;     /* the autotuner's measurement (0 when not tuned) */
     uint32_t candidates;    /* configurations the autotuner timed (0: cached or not tuned) */
 } dyph_fused_config;
 dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config* out);
-dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams);
+dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams, uint32_t register_blocks);
 dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out);
 /* Phase timing of fused batched frames, the per-stage table of the
  * reference's --profile mode (examples/stress_test_blocks/main.cpp:199-254)

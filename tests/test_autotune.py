@@ -29,11 +29,11 @@ def test_every_config_gives_the_same_frames(dev, mode):
     want = ref.state()
     need = ref.fused_config()["smem_bytes"]
     seen = set()
-    for cap, teams in ((0, True), (0, False), (48 << 10, True), (32 << 10, True), (1, False)):
+    for cap, teams, regs in ((0, True, 4), (0, False, 5), (48 << 10, True, 5), (32 << 10, True, 6), (1, False, 6)):
         w = dev.World(s, mode=mode)
-        w.set_fused_config(cap, teams)
+        w.set_fused_config(cap, teams, regs)
         cfg = w.fused_config()
-        assert cfg["smem_bytes"] <= need and cfg["warp_teams"] == int(teams)
+        assert cfg["smem_bytes"] <= need and cfg["warp_teams"] == int(teams) and cfg["register_blocks"] == regs
         assert cfg["warp_scenes"] + cfg["block_scenes"] == s.n_scenes
         seen.add((cfg["smem_bytes"], cfg["warp_scenes"]))
         w.step(30)
