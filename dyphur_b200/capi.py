@@ -32,8 +32,8 @@ class Contacts(C.Structure):
 
 
 class FusedConfig(C.Structure):
-    _fields_ = [("smem_bytes", C.c_uint32), ("warp_teams", C.c_uint32), ("warp_scenes", C.c_uint32),
-                ("block_scenes", C.c_uint32), ("blocks", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+    _fields_ = [("smem_bytes", C.c_uint32), ("teams", C.c_uint32), ("warp_scenes", C.c_uint32),
+                ("half_scenes", C.c_uint32), ("block_scenes", C.c_uint32), ("blocks", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("register_blocks", C.c_uint32), ("ms_per_frame", C.c_float), ("candidates", C.c_uint32)]
 
 
@@ -93,7 +93,7 @@ _PROTOS = {
     "dyph_bodies_check_finite": (_st, [C.POINTER(Bodies), _vp, _up]),
     "dyph_world_check_finite": (_st, [_vp, _vp, _up]),
     "dyph_world_fused_config": (_st, [_vp, C.POINTER(FusedConfig)]),
-    "dyph_world_set_fused_config": (_st, [_vp, C.c_uint32, C.c_int, C.c_uint32]),
+    "dyph_world_set_fused_config": (_st, [_vp, C.c_uint32, C.c_uint32, C.c_uint32]),
     "dyph_world_autotune": (_st, [_vp, C.c_int32, _vp, C.POINTER(FusedConfig)]),
     "dyph_ray_query": (_st, [C.POINTER(BvhView), C.POINTER(Bodies), C.POINTER(Shapes), _vp, _vp, C.c_uint32, _vp]),
     "dyph_contact_sensor_create": (_st, [C.c_uint32, C.POINTER(_vp)]),

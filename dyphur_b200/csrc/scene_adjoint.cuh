@@ -228,8 +228,14 @@ __global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_adjoint_kernel(S
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t share = (S.smem_bytes / 4u) & ~15u;
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-        if (items[4 * it + 1] == kItemBlock) {
+        const uint32_t kind = items[4 * it + 1];
+        if (kind == kItemBlock) {
             adjoint_scene(BlockTeam{}, items[4 * it], scene_smem, S.smem_bytes, sh[0], S, F, P_, A, G);
+        } else if (kind == kItemHalf) {
+            const uint32_t half = warp >> 1, s = items[4 * it + 2 * half];
+            if (s != kItemEmpty)
+                adjoint_scene(HalfTeam{half}, s, scene_smem + half * 2u * share, 2u * share, sh[2 * half], S, F, P_,
+                              A, G);
         } else {
             const uint32_t s = items[4 * it + warp];
             if (s != kItemEmpty)

@@ -308,11 +308,14 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
 }
 
 // Work item i: items[4 i] a large scene solved by the whole block when
-// items[4 i + 1] == kItemBlock; otherwise up to four small scenes, one per
-// warp (kItemEmpty marks an unused warp), each with a quarter of the block's
-// shared memory.
+// items[4 i + 1] == kItemBlock; two mid-size scenes items[4 i] and
+// items[4 i + 2], two warps and half the block's shared memory each, when
+// items[4 i + 1] == kItemHalf; otherwise up to four small scenes, one per
+// warp, each with a quarter of the shared memory. kItemEmpty marks an unused
+// team.
 constexpr uint32_t kItemEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kItemBlock = 0xFFFFFFFEu;
+constexpr uint32_t kItemHalf = 0xFFFFFFFDu;
 
 // kMinBlocks is the register budget: 4 resident blocks per SM (128
 // registers a thread), 5 (96) or 6 (80, a few bytes spilled). Which one runs
@@ -328,8 +331,13 @@ __global__ void __launch_bounds__(kSceneThreads, kMinBlocks) scene_frame_kernel(
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t share = (S.smem_bytes / 4u) & ~15u;
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-        if (items[4 * it + 1] == kItemBlock) {
+        const uint32_t kind = items[4 * it + 1];
+        if (kind == kItemBlock) {
             frame_scene(BlockTeam{}, items[4 * it], scene_smem, S.smem_bytes, sh[0], S, F, P_);
+        } else if (kind == kItemHalf) {
+            const uint32_t half = warp >> 1, s = items[4 * it + 2 * half];
+            if (s != kItemEmpty)
+                frame_scene(HalfTeam{half}, s, scene_smem + half * 2u * share, 2u * share, sh[2 * half], S, F, P_);
         } else {
             const uint32_t s = items[4 * it + warp];
             if (s != kItemEmpty) frame_scene(WarpTeam{}, s, scene_smem + warp * share, share, sh[warp], S, F, P_);

@@ -149,6 +149,46 @@ struct WarpTeam {
     }
 };
 
+// Two warps of a block (half 0: warps 0-1, half 1: warps 2-3), synchronised
+// on named barrier 1 + half; the block's own __syncthreads uses barrier 0.
+struct HalfTeam {
+    uint32_t half;
+    __device__ __forceinline__ uint32_t bar() const { return 1u + half; }
+    __device__ __forceinline__ uint32_t rank() const { return threadIdx.x & 63u; }
+    __device__ __forceinline__ uint32_t size() const { return 64u; }
+    __device__ __forceinline__ uint32_t warp() const { return (threadIdx.x >> 5) & 1u; }
+    __device__ __forceinline__ uint32_t warps() const { return 2u; }
+    __device__ __forceinline__ bool leader() const { return (threadIdx.x & 63u) == 0u; }
+    __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, 64;" ::"r"(bar()) : "memory"); }
+    __device__ __forceinline__ bool any(bool p) const {
+        uint32_t r;
+        asm volatile(
+            "{\n\t.reg .pred pin, pout;\n\t"
+            "setp.ne.u32 pin, %1, 0;\n\t"
+            "bar.red.or.pred pout, %2, 64, pin;\n\t"
+            "selp.u32 %0, 1, 0, pout;\n\t}"
+            : "=r"(r)
+            : "r"(static_cast<uint32_t>(p)), "r"(bar())
+            : "memory");
+        return r != 0u;
+    }
+    __device__ __forceinline__ uint32_t exclusive_scan(uint32_t v, uint32_t* scratch, uint32_t& total) const {
+        const uint32_t lane = threadIdx.x & 31u, w = warp();
+        uint32_t x = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= static_cast<uint32_t>(d)) x += y;
+        }
+        if (lane == 31u) scratch[w] = x;
+        sync();
+        const uint32_t t0 = scratch[0], t1 = scratch[1];
+        total = t0 + t1;
+        sync();  // the scratch words are free again for the next scan
+        return (w ? t0 : 0u) + x - v;
+    }
+};
+
 // Levels of the sequential order on one scene: level(k) = 1 + the larger
 // level of k's predecessors on its two dynamic bodies. Contacts of one level
 // share no dynamic body, and solving the levels in ascending order gives

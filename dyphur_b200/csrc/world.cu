@@ -68,9 +68,9 @@ struct dyph_world {
     // Knobs of the fused kernel (dyph_world_set_fused_config / dyph_world_autotune).
     std::vector<uint32_t> h_body_offset;  // host copy of the scenes' body ranges
     uint32_t f_smem_cap = 0;              // shared memory cap per block (0 = what the largest scene needs)
-    bool f_warp_teams = true;             // small scenes one per warp, four to a block
+    uint32_t f_teams = 2;                 // 0 blocks only, 1 + small scenes one per warp, 2 + mid-size two warps
     uint32_t f_variant = 0;               // register budget: 4 (0), 5 (1) or 6 (2) blocks per SM
-    uint32_t f_warp_scenes = 0, f_block_scenes = 0;
+    uint32_t f_warp_scenes = 0, f_half_scenes = 0, f_block_scenes = 0;
     float f_tuned_ms = 0.f;
     uint32_t f_tuned_candidates = 0;
 };
@@ -495,8 +495,9 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
         if (cudaMalloc(bufs[k], sizes[k] * sizeof(uint32_t)) != cudaSuccess) return DYPH_ERR_NOMEM;
     // Work items, largest scenes first: a scene whose frame is expected to fit
     // a quarter of the block's shared memory (about 4 pairs and 2.5 contacts
-    // per body) runs on one warp, four such scenes to a block; larger scenes
-    // take the whole block.
+    // per body) runs on one warp, four such scenes to a block; one that fits
+    // half of it on two warps, two to a block; larger scenes take the whole
+    // block.
     std::vector<uint32_t> order(n_scenes);
     for (uint32_t i = 0; i < n_scenes; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [body_offset](uint32_t x, uint32_t y) {
@@ -504,15 +505,20 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     });
     const uint32_t share = (smem / 4u) & ~15u;
     std::vector<uint32_t> items;
-    std::vector<uint32_t> small;
+    std::vector<uint32_t> small, mid;
     for (uint32_t s : order) {
         const uint32_t nb = body_offset[s + 1] - body_offset[s];
-        if (w->f_warp_teams && frame_body_bytes(nb) + 146u * nb <= share) {
+        const uint32_t est = frame_body_bytes(nb) + 146u * nb;
+        if (w->f_teams >= 1 && est <= share) {
             small.push_back(s);
+        } else if (w->f_teams >= 2 && est <= 2u * share) {
+            mid.push_back(s);
         } else {
             items.insert(items.end(), {s, kItemBlock, kItemEmpty, kItemEmpty});
         }
     }
+    for (size_t i = 0; i < mid.size(); i += 2)
+        items.insert(items.end(), {mid[i], kItemHalf, i + 1 < mid.size() ? mid[i + 1] : kItemEmpty, kItemHalf});
     for (size_t i = 0; i < small.size(); i += 4)
         for (size_t j = 0; j < 4; ++j) items.push_back(i + j < small.size() ? small[i + j] : kItemEmpty);
     w->f_n_items = static_cast<uint32_t>(items.size() / 4);
@@ -523,7 +529,8 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     DYPH_CUDA_TRY(cudaMemset(w->f_counts, 0, 4ull * n_scenes * sizeof(uint32_t)));
     w->frame_smem = smem;
     w->f_warp_scenes = static_cast<uint32_t>(small.size());
-    w->f_block_scenes = n_scenes - w->f_warp_scenes;
+    w->f_half_scenes = static_cast<uint32_t>(mid.size());
+    w->f_block_scenes = n_scenes - w->f_warp_scenes - w->f_half_scenes;
     w->fused = true;
     return DYPH_OK;
 }
@@ -544,8 +551,9 @@ void fused_report(const dyph_world* w, dyph_fused_config* out) {
                                         : reinterpret_cast<const void*>(scene_frame_kernel<4>);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kSceneThreads, w->frame_smem);
     out->smem_bytes = w->frame_smem;
-    out->warp_teams = w->f_warp_teams ? 1u : 0u;
+    out->teams = w->f_teams;
     out->warp_scenes = w->f_warp_scenes;
+    out->half_scenes = w->f_half_scenes;
     out->block_scenes = w->f_block_scenes;
     out->blocks = w->f_n_items;
     out->blocks_per_sm = static_cast<uint32_t>(per_sm);
@@ -558,7 +566,7 @@ void fused_report(const dyph_world* w, dyph_fused_config* out) {
 // settings), for the life of the process.
 struct TunedConfig {
     uint32_t smem_cap;
-    bool warp_teams;
+    uint32_t teams;
     uint32_t variant;
     float ms;
 };
@@ -609,13 +617,13 @@ extern "C" dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config*
     return DYPH_OK;
 }
 
-extern "C" dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams,
+extern "C" dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, uint32_t teams,
                                                    uint32_t register_blocks) {
-    if (!w || !w->fused || (register_blocks != 0 && (register_blocks < 4 || register_blocks > 6)))
+    if (!w || !w->fused || teams > 2u || (register_blocks != 0 && (register_blocks < 4 || register_blocks > 6)))
         return DYPH_ERR_INVALID;
     DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
     w->f_smem_cap = smem_cap;
-    w->f_warp_teams = warp_teams != 0;
+    w->f_teams = teams;
     w->f_variant = register_blocks ? register_blocks - 4u : 0u;
     const std::vector<uint32_t> off = w->h_body_offset;
     dyph_status st = setup_fused(w, static_cast<uint32_t>(off.size() - 1), off.data());
@@ -634,7 +642,7 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
         auto it = g_tuned.find(key);
         if (it != g_tuned.end()) {
             dyph_status st =
-                dyph_world_set_fused_config(w, it->second.smem_cap, it->second.warp_teams, 4u + it->second.variant);
+                dyph_world_set_fused_config(w, it->second.smem_cap, it->second.teams, 4u + it->second.variant);
             w->f_tuned_ms = it->second.ms;
             w->f_tuned_candidates = 0;  // taken from the cache
             if (out) fused_report(w, out);
@@ -669,10 +677,10 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
     std::vector<uint32_t> caps = {need};
     for (uint32_t c : {96u << 10, 72u << 10, 56u << 10, 48u << 10, 40u << 10, 32u << 10})
         if (c < need && c >= floor_) caps.push_back(c);
-    TunedConfig best{need, true, 0u, 1e30f};
+    TunedConfig best{need, 2u, 0u, 1e30f};
     uint32_t tried = 0;
     const uint32_t cap0 = w->f_smem_cap, variant0 = w->f_variant;
-    const bool teams0 = w->f_warp_teams;
+    const uint32_t teams0 = w->f_teams;
     do {
         if (cudaMemcpyAsync(saved_stats, w->stats, sizeof(saved_stats), cudaMemcpyDeviceToHost, w->stream) !=
                 cudaSuccess ||
@@ -682,11 +690,11 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
             break;
         }
         for (uint32_t cap : caps) {
-            for (uint32_t combo = 0; combo < 6u && st == DYPH_OK; ++combo) {
-                const int teams = combo < 3u ? 1 : 0;
+            for (uint32_t combo = 0; combo < 9u && st == DYPH_OK; ++combo) {
+                const uint32_t teams = 2u - combo / 3u;
                 const uint32_t variant = combo % 3u;
                 w->f_smem_cap = cap;
-                w->f_warp_teams = teams != 0;
+                w->f_teams = teams;
                 w->f_variant = variant;
                 st = setup_fused(w, static_cast<uint32_t>(w->h_body_offset.size() - 1), w->h_body_offset.data());
                 if (st != DYPH_OK) break;
@@ -703,7 +711,7 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
                 if (st != DYPH_OK) break;
                 ++tried;
                 ms /= static_cast<float>(frames);
-                if (ms < best.ms) best = TunedConfig{cap, teams != 0, variant, ms};
+                if (ms < best.ms) best = TunedConfig{cap, teams, variant, ms};
             }
             if (st != DYPH_OK) break;
         }
@@ -713,11 +721,11 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
     w->f_phase = phase;
     if (st == DYPH_OK) {
         w->f_smem_cap = best.smem_cap;
-        w->f_warp_teams = best.warp_teams;
+        w->f_teams = best.teams;
         w->f_variant = best.variant;
     } else {
         w->f_smem_cap = cap0;
-        w->f_warp_teams = teams0;
+        w->f_teams = teams0;
         w->f_variant = variant0;
     }
     const dyph_status st2 = setup_fused(w, static_cast<uint32_t>(w->h_body_offset.size() - 1), w->h_body_offset.data());

@@ -542,9 +542,10 @@ class World:
         check(capi.lib().dyph_world_fused_config(self.h, C.byref(c)), "dyph_world_fused_config")
         return {k: getattr(c, k) for k, _ in capi.FusedConfig._fields_}
 
-    def set_fused_config(self, smem_cap: int, warp_teams: bool = True, register_blocks: int = 0) -> None:
-        check(capi.lib().dyph_world_set_fused_config(self.h, int(smem_cap), int(bool(warp_teams)),
-                                                     int(register_blocks)), "dyph_world_set_fused_config")
+    def set_fused_config(self, smem_cap: int, teams: int = 2, register_blocks: int = 0) -> None:
+        """teams: 0 every scene a block, 1 small scenes one per warp, 2 also mid-size scenes on two warps."""
+        check(capi.lib().dyph_world_set_fused_config(self.h, int(smem_cap), int(teams), int(register_blocks)),
+              "dyph_world_set_fused_config")
 
     def autotune(self, frames: int = 16, stream=None) -> dict:
         """Time the fused kernel's configurations from the current state and keep

@@ -4,7 +4,7 @@ stress_test_blocks example (examples/stress_test_blocks/main.cpp).
     python -m dyphur_b200.run [out_prefix] [n_frames] [--grid NX NY NZ]
                               [--spacing S] [--jitter J] [--profile]
                               [--workload blocks|pile|batch] [--mode M]
-                              [--start-frame F] [--smem-cap B] [--no-warp-teams]
+                              [--start-frame F] [--smem-cap B] [--teams T]
                               [--autotune FRAMES]
 
 Writes <prefix>.scene, <prefix>.trajectory (poses every other frame),
@@ -45,7 +45,8 @@ def parse(argv=None):
     ap.add_argument("--no-output", action="store_true", help="write no files")
     ap.add_argument("--smem-cap", type=int, default=None,
                     help="batch: shared memory cap per block of the fused frame (bytes; 0 = what it needs)")
-    ap.add_argument("--no-warp-teams", action="store_true", help="batch: every scene takes a whole block")
+    ap.add_argument("--teams", type=int, default=None, choices=[0, 1, 2],
+                    help="batch: 0 every scene a block, 1 small scenes one per warp, 2 also mid-size on two warps")
     ap.add_argument("--register-blocks", type=int, default=0, choices=[0, 4, 5, 6],
                     help="batch: register budget of the fused frame kernel (resident blocks per SM)")
     ap.add_argument("--autotune", type=int, default=0, metavar="FRAMES",
@@ -118,8 +119,8 @@ def main(argv=None) -> int:
     scene = build_scene(args)
     n = scene.n_bodies
     world = device.World(scene, mode=mode)
-    if args.smem_cap is not None or args.no_warp_teams or args.register_blocks:
-        world.set_fused_config(args.smem_cap or 0, not args.no_warp_teams, args.register_blocks)
+    if args.smem_cap is not None or args.teams is not None or args.register_blocks:
+        world.set_fused_config(args.smem_cap or 0, 2 if args.teams is None else args.teams, args.register_blocks)
     if args.autotune:
         init = world.bodies.fbuf.clone()
         world.step(args.start_frame)

@@ -400,12 +400,13 @@ dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
  *   smem_bytes     dynamic shared memory per block: what the largest scene
  *                  needs, or less (smem_cap), down to its bodies plus 64
  *                  contacts' words;
- *   warp_teams     scenes whose frame fits a quarter of that run one per
- *                  warp, four to a block (else every scene takes a block);
+ *   teams          0: every scene takes a block; 1: scenes whose frame fits
+ *                  a quarter of that run one per warp, four to a block; 2: also
+ *                  scenes that fit half of it on two warps, two to a block;
  *   register_blocks the kernel's register budget: 4, 5 or 6 resident blocks
  *                  per SM (128, 96 or 80 registers a thread; 0 = 4).
  * dyph_world_autotune times `frames` frames of each candidate (smem caps
- * 96/72/56/48/40/32 KB below the need, warp teams on and off, each register
+ * 96/72/56/48/40/32 KB below the need, each team policy, each register
  * budget) from the
  * world's current state, keeps the fastest, and puts the state and the
  * statistics back; the choice is cached per device and batch profile (scene
@@ -414,8 +415,9 @@ dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
  * Blocking; drops captured frames. */
 typedef struct dyph_fused_config {
     uint32_t smem_bytes;    /* dynamic shared memory per block */
-    uint32_t warp_teams;    /* 1: small scenes one per warp */
+    uint32_t teams;         /* team policy (0, 1, 2) */
     uint32_t warp_scenes;   /* scenes run by one warp */
+    uint32_t half_scenes;   /* scenes run by two warps */
     uint32_t block_scenes;  /* scenes run by a whole block */
     uint32_t blocks;        /* thread blocks per frame */
     uint32_t blocks_per_sm; /* resident blocks per SM at smem_bytes and the register budget */
@@ -424,7 +426,7 @@ typedef struct dyph_fused_config {
     uint32_t candidates;    /* configurations the autotuner timed (0: cached or not tuned) */
 } dyph_fused_config;
 dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config* out);
-dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, int warp_teams, uint32_t register_blocks);
+dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, uint32_t teams, uint32_t register_blocks);
 dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out);
 /* Phase timing of fused batched frames, the per-stage table of the
  * reference's --profile mode (examples/stress_test_blocks/main.cpp:199-254)

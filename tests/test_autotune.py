@@ -29,17 +29,19 @@ def test_every_config_gives_the_same_frames(dev, mode):
     want = ref.state()
     need = ref.fused_config()["smem_bytes"]
     seen = set()
-    for cap, teams, regs in ((0, True, 4), (0, False, 5), (48 << 10, True, 5), (32 << 10, True, 6), (1, False, 6)):
+    for cap, teams, regs in ((0, 2, 4), (0, 1, 4), (0, 0, 5), (48 << 10, 2, 5), (48 << 10, 1, 6), (32 << 10, 2, 6),
+                             (1, 0, 6)):
         w = dev.World(s, mode=mode)
         w.set_fused_config(cap, teams, regs)
         cfg = w.fused_config()
-        assert cfg["smem_bytes"] <= need and cfg["warp_teams"] == int(teams) and cfg["register_blocks"] == regs
-        assert cfg["warp_scenes"] + cfg["block_scenes"] == s.n_scenes
-        seen.add((cfg["smem_bytes"], cfg["warp_scenes"]))
+        assert cfg["smem_bytes"] <= need and cfg["teams"] == teams and cfg["register_blocks"] == regs
+        assert cfg["warp_scenes"] + cfg["half_scenes"] + cfg["block_scenes"] == s.n_scenes
+        assert (teams >= 2) or cfg["half_scenes"] == 0
+        seen.add((cfg["smem_bytes"], cfg["warp_scenes"], cfg["half_scenes"]))
         w.step(30)
         assert np.array_equal(bits(w.state()), bits(want)), (cap, teams)
         assert w.stats()["status"] == 0 and dev.device_error() == 0
-    assert len(seen) >= 4  # the configurations really differ
+    assert len(seen) >= 5 and any(k[2] > 0 for k in seen)  # the configurations really differ
 
 
 def test_autotune_keeps_state_and_caches(dev):
