@@ -9,10 +9,9 @@
 //   * pairs: the candidate-pair set is the set of body pairs whose fp16 leaf
 //     boxes (core/src/broadphase.cpp:216-251) overlap under the traversal's
 //     inclusive test (:322-325), because internal nodes merge the leaf boxes
-//     exactly. So a sort and sweep on the boxes' min x finds that set, and
-//     the pairs are written in ascending (a << 32 | b) order, as
-//     Broadphase::sort_pairs leaves them; a scene keeps the first max_pairs of
-//     them, as it does alone;
+//     exactly. So every (a, b) with a < b is tested directly and the pairs
+//     come out in ascending (a << 32 | b) order, as Broadphase::sort_pairs
+//     leaves them; a scene keeps the first max_pairs of them, as it does alone;
 //   * narrowphase: process_pair (core/src/narrowphase.cpp:920-1001) per pair,
 //     contacts compacted in pair order, the first max_contacts kept;
 //   * solve: scene_solve (solver_scene.cuh).
@@ -165,65 +164,20 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     T.sync();
     phase_mark(T, P_, 0, t0);
     // ── candidate pairs: per body a, the partners b > a in ascending order ──
-    // Sort and sweep on the boxes' min x: bodies ranked by (min x, index), and
-    // from each body the later ones are tested while their min x is at most
-    // its max x. Every overlapping pair is met exactly once (from whichever of
-    // the two ranks first: every body ranked between them starts no further
-    // right than the later one), and the full inclusive test decides it, so
-    // the set is the all-pairs set. A NaN bound makes that test pass for any
-    // partner (it is written as "not separated"), which no ordering captures:
-    // such a scene takes the all-pairs count and write instead.
-    uint32_t* key = reinterpret_cast<uint32_t*>(R.pri);  // [ldb] orderable min-x keys
-    uint32_t* rank_of = key + ldb;                        // [ldb] bodies in key order
-    bool nan_box = false;
-    for (uint32_t i = T.rank(); i < nb; i += T.size()) {
-        for (int r = 0; r < 6; ++r) nan_box = nan_box || isnan(box[r * ldb + i]);
-        const uint32_t u = __float_as_uint(box[i]);
-        key[i] = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-        R.cnt[i] = 0u;
-    }
-    T.sync();
-    const bool sweep = !T.any(nan_box);
-    if (sweep) {
-        for (uint32_t i = T.rank(); i < nb; i += T.size()) {
-            const uint32_t ki = key[i];
-            uint32_t r = 0;
-            for (uint32_t j = 0; j < nb; ++j) {
-                const uint32_t kj = key[j];
-                r += (kj < ki || (kj == ki && j < i)) ? 1u : 0u;
+    for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
+        const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
+        uint32_t c = 0;
+        for (uint32_t j0 = a + 1; j0 < nb; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            bool ov = false;
+            if (j < nb) {
+                const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
+                             box[5 * ldb + j]};
+                ov = box_overlap(n, q);
             }
-            rank_of[r] = i;
+            c += __popc(__ballot_sync(0xffffffffu, ov));
         }
-        T.sync();
-        for (uint32_t p = T.rank(); p < nb; p += T.size()) {
-            const uint32_t a = rank_of[p];
-            const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a],
-                         box[5 * ldb + a]};
-            for (uint32_t r = p + 1; r < nb; ++r) {
-                const uint32_t b = rank_of[r];
-                if (box[b] > q.mxx) break;
-                const BoxF n{box[b], box[ldb + b], box[2 * ldb + b], box[3 * ldb + b], box[4 * ldb + b],
-                             box[5 * ldb + b]};
-                if (box_overlap(n, q)) atomicAdd(&R.cnt[min(a, b)], 1u);
-            }
-        }
-    } else {
-        for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
-            const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a],
-                         box[5 * ldb + a]};
-            uint32_t c = 0;
-            for (uint32_t j0 = a + 1; j0 < nb; j0 += 32u) {
-                const uint32_t j = j0 + lane;
-                bool ov = false;
-                if (j < nb) {
-                    const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
-                                 box[5 * ldb + j]};
-                    ov = box_overlap(n, q);
-                }
-                c += __popc(__ballot_sync(0xffffffffu, ov));
-            }
-            if (lane == 0) R.cnt[a] = c;
-        }
+        if (lane == 0) R.cnt[a] = c;
     }
     if (T.leader()) sh.carry = 0u;
     T.sync();
@@ -249,56 +203,21 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(smem + body_bytes) + pwords
                                    : F.words + F.contact_base[s] + s,
                            in_smem ? ldc : F.words_stride};
-    if (sweep && p_true <= pcap) {
-        // the same sweep writes each pair into its smaller body's segment (in
-        // sweep order) in the contact words, which are free until the
-        // narrowphase (13 rows of at least min(P, capacity) + 1 words hold P);
-        // each pair then moves to its rank by partner within the segment
-        const uint32_t L = in_smem ? ldc : ccap + 1u;  // words of one row this scene owns
-        auto tmp = [&](uint32_t e) -> uint32_t& { return SC.w[(e / L) * SC.ld + e % L]; };
-        for (uint32_t i = T.rank(); i < nb; i += T.size()) R.cnt[i] = 0u;
-        T.sync();
-        for (uint32_t p = T.rank(); p < nb; p += T.size()) {
-            const uint32_t a = rank_of[p];
-            const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a],
-                         box[5 * ldb + a]};
-            for (uint32_t r = p + 1; r < nb; ++r) {
-                const uint32_t b = rank_of[r];
-                if (box[b] > q.mxx) break;
-                const BoxF n{box[b], box[ldb + b], box[2 * ldb + b], box[3 * ldb + b], box[4 * ldb + b],
-                             box[5 * ldb + b]};
-                if (box_overlap(n, q)) {
-                    const uint32_t lo = min(a, b), hi = max(a, b);
-                    tmp(R.off[lo] + atomicAdd(&R.cnt[lo], 1u)) = lo | (hi << 16);
-                }
+    for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
+        const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
+        uint32_t pos = R.off[a];
+        for (uint32_t j0 = a + 1; j0 < nb && pos < P; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            bool ov = false;
+            if (j < nb) {
+                const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
+                             box[5 * ldb + j]};
+                ov = box_overlap(n, q);
             }
-        }
-        T.sync();
-        for (uint32_t e = T.rank(); e < P; e += T.size()) {
-            const uint32_t w = tmp(e), lo = w & 0xFFFFu;
-            const uint32_t s0 = R.off[lo], n = R.cnt[lo];
-            uint32_t r = 0;
-            for (uint32_t f = s0; f < s0 + n; ++f) r += tmp(f) < w ? 1u : 0u;
-            pairs[s0 + r] = w;
-        }
-    } else {
-        for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
-            const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a],
-                         box[5 * ldb + a]};
-            uint32_t pos = R.off[a];
-            for (uint32_t j0 = a + 1; j0 < nb && pos < P; j0 += 32u) {
-                const uint32_t j = j0 + lane;
-                bool ov = false;
-                if (j < nb) {
-                    const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
-                                 box[5 * ldb + j]};
-                    ov = box_overlap(n, q);
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, ov);
-                const uint32_t at = pos + __popc(bal & ((1u << lane) - 1u));
-                if (ov && at < P) pairs[at] = a | (j << 16);
-                pos += __popc(bal);
-            }
+            const unsigned bal = __ballot_sync(0xffffffffu, ov);
+            const uint32_t at = pos + __popc(bal & ((1u << lane) - 1u));
+            if (ov && at < P) pairs[at] = a | (j << 16);
+            pos += __popc(bal);
         }
     }
     T.sync();
