@@ -153,23 +153,39 @@ struct WarpTeam {
 // on named barrier 1 + half; the block's own __syncthreads uses barrier 0.
 struct HalfTeam {
     uint32_t half;
-    __device__ __forceinline__ uint32_t bar() const { return 1u + half; }
     __device__ __forceinline__ uint32_t rank() const { return threadIdx.x & 63u; }
     __device__ __forceinline__ uint32_t size() const { return 64u; }
     __device__ __forceinline__ uint32_t warp() const { return (threadIdx.x >> 5) & 1u; }
     __device__ __forceinline__ uint32_t warps() const { return 2u; }
     __device__ __forceinline__ bool leader() const { return (threadIdx.x & 63u) == 0u; }
-    __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, 64;" ::"r"(bar()) : "memory"); }
+    // Immediate barrier ids (the branch is uniform over the team), so the
+    // kernel reserves barriers 0-2 only.
+    __device__ __forceinline__ void sync() const {
+        if (half)
+            asm volatile("bar.sync 2, 64;" ::: "memory");
+        else
+            asm volatile("bar.sync 1, 64;" ::: "memory");
+    }
     __device__ __forceinline__ bool any(bool p) const {
         uint32_t r;
-        asm volatile(
-            "{\n\t.reg .pred pin, pout;\n\t"
-            "setp.ne.u32 pin, %1, 0;\n\t"
-            "bar.red.or.pred pout, %2, 64, pin;\n\t"
-            "selp.u32 %0, 1, 0, pout;\n\t}"
-            : "=r"(r)
-            : "r"(static_cast<uint32_t>(p)), "r"(bar())
-            : "memory");
+        if (half)
+            asm volatile(
+                "{\n\t.reg .pred pin, pout;\n\t"
+                "setp.ne.u32 pin, %1, 0;\n\t"
+                "bar.red.or.pred pout, 2, 64, pin;\n\t"
+                "selp.u32 %0, 1, 0, pout;\n\t}"
+                : "=r"(r)
+                : "r"(static_cast<uint32_t>(p))
+                : "memory");
+        else
+            asm volatile(
+                "{\n\t.reg .pred pin, pout;\n\t"
+                "setp.ne.u32 pin, %1, 0;\n\t"
+                "bar.red.or.pred pout, 1, 64, pin;\n\t"
+                "selp.u32 %0, 1, 0, pout;\n\t}"
+                : "=r"(r)
+                : "r"(static_cast<uint32_t>(p))
+                : "memory");
         return r != 0u;
     }
     __device__ __forceinline__ uint32_t exclusive_scan(uint32_t v, uint32_t* scratch, uint32_t& total) const {
