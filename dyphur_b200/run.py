@@ -51,6 +51,8 @@ def parse(argv=None):
                     help="batch: register budget of the fused frame kernel (resident blocks per SM)")
     ap.add_argument("--autotune", type=int, default=0, metavar="FRAMES",
                     help="batch: autotune the fused frame on FRAMES frames (after --start-frame) first")
+    ap.add_argument("--rays", type=int, default=0, metavar="N",
+                    help="after the run, cast N seeded rays at the bodies through the last frame's tree")
     return ap.parse_args(argv)
 
 
@@ -108,6 +110,28 @@ def profile(world, scene, frames: int, warm: int = 30) -> None:
     print(f"  {'TOTAL':<16} {total:8.3f} ms   ({1000.0 / total:.1f} fps, stage-summed)")
 
 
+def cast_rays(world, scene, n_rays: int, seed: int = 9) -> None:
+    """N rays from random points of the scene's box aimed near random bodies,
+    through the last frame's tree (ray_query); prints hits and rays/s."""
+    import torch
+    rng = np.random.default_rng(seed)
+    st = world.state()
+    lo, hi = scene.bounds[0, :3], scene.bounds[0, 3:]
+    target = st[:3].T[rng.integers(0, scene.n_bodies, n_rays)] + rng.normal(0.0, 0.3, (n_rays, 3))
+    origin = rng.uniform(lo, hi, (n_rays, 3))
+    rays = torch.from_numpy(np.concatenate([origin, target - origin, np.full((n_rays, 1), 1e9)], 1)
+                            .astype(np.float32)).cuda()
+    world.ray_query(rays)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    t, body = world.ray_query(rays)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    hits = int((body != -1).sum())
+    print(f"rays: {n_rays} cast, {hits} hit, {ms:.3f} ms ({n_rays / ms / 1e3:.1f} M rays/s)")
+
+
 def main(argv=None) -> int:
     import torch
 
@@ -135,6 +159,8 @@ def main(argv=None) -> int:
         st = world.stats()
         print(f"stepped {args.start_frame} + {args.n_frames} frames, status {st['status']}, last frame "
               f"{st['last_pairs']} candidate pairs, {st['last_contacts']} contacts, {n} bodies")
+        if args.rays:
+            cast_rays(world, scene, args.rays)
         return 0
     if args.profile:
         profile(world, scene, args.n_frames)
