@@ -613,7 +613,8 @@ def _dual_error(w, scene, i, frames, g_vel, g_ang, g_im, at_float, loss_mask, sc
     return float(np.linalg.norm(g - g_d) / max(np.linalg.norm(g_d), 1e-30))
 
 
-def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask, reps: int = 3) -> dict:
+def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask, reps: int = 3,
+                   checker: bool = True) -> dict:
     """Forward rollout and forward + adjoint of a differentiable batch
     (sequential order), loss = mean over the masked bodies of |x_final -
     target|^2: body-steps/s of each, their ratio, the device memory the
@@ -658,10 +659,12 @@ def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask,
         a, b, _, _, _ = once(frames)
         per_frame = (a + b) / a
         every = every_cfg
-    err_full = _dual_error(w, scene, 0, frames, gv, ga, gm, True, loss_mask, scale)
-    _, _, gv10, ga10, gm10 = once(10)
-    err_10 = _dual_error(w, scene, 0, 10, gv10.cpu().numpy(), ga10.cpu().numpy(), gm10.cpu().numpy(), False,
-                         loss_mask, scale)
+    err_full = err_10 = None
+    if checker:  # the CPU checker leg: FP64 dual numbers (oracle/) on scene 0
+        err_full = _dual_error(w, scene, 0, frames, gv, ga, gm, True, loss_mask, scale)
+        _, _, gv10, ga10, gm10 = once(10)
+        err_10 = _dual_error(w, scene, 0, 10, gv10.cpu().numpy(), ga10.cpu().numpy(), gm10.cpu().numpy(), False,
+                             loss_mask, scale)
     n_ckpt = (frames + every - 1) // every
     slots = int(sum(max(64, 16 * int(b) + 64) for b in np.diff(scene.body_offset)))
     act = 4 * (n_ckpt * 13 * n + every * 13 * n + 36 * slots + (7 + 4 + 26) * n)
@@ -818,12 +821,14 @@ def run_b200(args) -> None:
         note("per-scene path")
         drift = drift_report(scene, frames, torch)
         note("drift")
-        fp64 = [fp64_error_report(scene, mode, frames, sample=6), fp64_error_report(scene, 2, frames, sample=6)]
         stress = scenes.stress_blocks()
         config1 = {"workload": "the reference's stress_test_blocks scene: 1024 boxes (8x16x8, spacing 0.85 m, "
                                "jitter 0.01) + ground",
-                   "fp64_error": fp64_error_report(stress, 0, 120, sample=1),
                    "colored_drift": drift_report(stress, 300, torch)}
+        fp64 = None
+        if not args.no_cpu_baseline:  # the CPU checker leg: FP64 re-runs (oracle/) beside the GPU numbers
+            fp64 = [fp64_error_report(scene, mode, frames, sample=6), fp64_error_report(scene, 2, frames, sample=6)]
+            config1["fp64_error"] = fp64_error_report(stress, 0, 120, sample=1)
         note("fp64 error + config-1 drift")
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -864,12 +869,12 @@ def run_b200(args) -> None:
                 boxes[push.body_offset[i]:push.body_offset[i] + 64] = True
             mixed = scenes.batch_mixed(1024, 16, 512, seed=5)
             line["adjoint"] = [
-                adjoint_report(torch, push, 120, 10,
+                adjoint_report(torch, push, 120, 10, checker=not args.no_cpu_baseline, label=
                                "differentiable push: 256 scenes of 64 boxes + a 5 kg pusher, loss = mean squared "
-                               "distance of the boxes' final centroids to seeded targets, 120 frames", boxes),
-                adjoint_report(torch, mixed, 60, 1,
+                               "distance of the boxes' final centroids to seeded targets, 120 frames", loss_mask=boxes),
+                adjoint_report(torch, mixed, 60, 1, checker=not args.no_cpu_baseline, label=
                                "batched fwd+bwd: 1024 scenes of 16-512 mixed boxes / spheres, loss = mean squared "
-                               "final position of every dynamic body, 60 frames", mixed.mass > 0)]
+                               "final position of every dynamic body, 60 frames", loss_mask=mixed.mass > 0)]
             note("adjoint")
         if not args.no_single and world == 1:
             line["single_scene"] = single_line(args, torch, barrier, 1, 0, local, SINGLE["seed"], SINGLE["frames"],
