@@ -147,47 +147,103 @@ __device__ void adjoint_scene(const Team& T, uint32_t s, unsigned char* smem, ui
             T.sync();
         }
         // ── narrowphase: geometry adjoints -> poses after integrate ──
-        // Group by group (no dynamic body twice in a group), so every body's
-        // sum is taken in one fixed order without atomics: the gradients are
-        // the same from run to run, bit for bit.
-        for (uint32_t g = 0; g < fo.groups; ++g) {
-            const uint32_t end = SC.pa(g + 1);
-            for (uint32_t idx = SC.pa(g) + T.rank(); idx < end; idx += T.size()) {
-                const uint32_t k = SC.ent(idx);
-                const float* r = A.rec + cbase + k;
-                if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
-                const Contact ct = SC.contact(k);
-                const uint32_t ia = ct.a, ib = ct.b;
-                const uint32_t ga = b0 + ia, gbi = b0 + ib;
-                const F3 xa = f3(A.pose1[ga], A.pose1[ns + ga], A.pose1[2ull * ns + ga]);
-                const F3 xb = f3(A.pose1[gbi], A.pose1[ns + gbi], A.pose1[2ull * ns + gbi]);
-                const float qa[4] = {A.pose1[3ull * ns + ga], A.pose1[4ull * ns + ga], A.pose1[5ull * ns + ga],
-                                     A.pose1[6ull * ns + ga]};
-                const float qb[4] = {A.pose1[3ull * ns + gbi], A.pose1[4ull * ns + gbi], A.pose1[5ull * ns + gbi],
-                                     A.pose1[6ull * ns + gbi]};
-                const float ha[3] = {half[ia], half[ldb + ia], half[2 * ldb + ia]};
-                const float hb[3] = {half[ib], half[ldb + ib], half[2 * ldb + ib]};
-                F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
-                float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
-                process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
-                                 __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
-                                 f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
-                                 f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
-                if (SB.im(ia) != 0.f) {
-                    grow(G.gout, ns, 0, ga) += xab.x;
-                    grow(G.gout, ns, 1, ga) += xab.y;
-                    grow(G.gout, ns, 2, ga) += xab.z;
-                    for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, ga) += qab[c];
-                }
-                if (SB.im(ib) != 0.f) {
-                    grow(G.gout, ns, 0, gbi) += xbb.x;
-                    grow(G.gout, ns, 1, gbi) += xbb.y;
-                    grow(G.gout, ns, 2, gbi) += xbb.z;
-                    for (int c = 0; c < 4; ++c) grow(G.gout, ns, 3 + c, gbi) += qbb[c];
-                }
+        // Each acting contact's adjoints for its two bodies go to its record
+        // (rows 0-13, free once the solve's adjoint has run); then every body
+        // adds its contacts' adjoints in contact order. Each sum is taken in
+        // one fixed order without atomics, so the gradients are the same from
+        // run to run, bit for bit, and no barrier is needed per group.
+        // Per-body lists of acting contacts (both sides, dynamic bodies):
+        // counts, scan, fill, sort; entries in the free pb / done rows.
+        auto entry = [&](uint32_t e) -> uint32_t& { return e < m ? SC.pb(e) : SC.done(e - m); };
+        for (uint32_t i = T.rank(); i < nb; i += T.size()) R.cnt[i] = 0u;
+        T.sync();
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
+            if (A.rec[cbase + k + 35ull * rs] == 0.f) continue;
+            const uint32_t ab = SC.ab(k), a = ab & 0xFFFFu, b = ab >> 16;
+            if (SB.im(a) != 0.f) atomicAdd(&R.cnt[a], 1u);
+            if (SB.im(b) != 0.f) atomicAdd(&R.cnt[b], 1u);
+        }
+        if (T.leader()) sh.carry = 0u;
+        T.sync();
+        for (uint32_t base = 0; base < nb; base += T.size()) {
+            const uint32_t i = base + T.rank();
+            uint32_t tot;
+            const uint32_t ex = T.exclusive_scan(i < nb ? R.cnt[i] : 0u, sh.scan, tot);
+            if (i < nb) {
+                R.off[i] = sh.carry + ex;
+                R.cnt[i] = 0u;
             }
             T.sync();
+            if (T.leader()) sh.carry += tot;
+            T.sync();
         }
+        if (T.leader()) R.off[nb] = sh.carry;
+        T.sync();
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
+            if (A.rec[cbase + k + 35ull * rs] == 0.f) continue;
+            const uint32_t ab = SC.ab(k), a = ab & 0xFFFFu, b = ab >> 16;
+            if (SB.im(a) != 0.f) entry(R.off[a] + atomicAdd(&R.cnt[a], 1u)) = k;
+            if (SB.im(b) != 0.f) entry(R.off[b] + atomicAdd(&R.cnt[b], 1u)) = k;
+        }
+        T.sync();
+        for (uint32_t x = T.rank(); x < nb; x += T.size()) {
+            const uint32_t lo = R.off[x], hi = R.off[x + 1];
+            for (uint32_t i = lo + 1; i < hi; ++i) {
+                const uint32_t v = entry(i);
+                uint32_t j = i;
+                while (j > lo && entry(j - 1) > v) {
+                    entry(j) = entry(j - 1);
+                    --j;
+                }
+                entry(j) = v;
+            }
+        }
+        // the contacts' geometry adjoints, into their records
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
+            float* r = A.rec + cbase + k;
+            if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
+            const Contact ct = SC.contact(k);
+            const uint32_t ia = ct.a, ib = ct.b;
+            const uint32_t ga = b0 + ia, gbi = b0 + ib;
+            const F3 xa = f3(A.pose1[ga], A.pose1[ns + ga], A.pose1[2ull * ns + ga]);
+            const F3 xb = f3(A.pose1[gbi], A.pose1[ns + gbi], A.pose1[2ull * ns + gbi]);
+            const float qa[4] = {A.pose1[3ull * ns + ga], A.pose1[4ull * ns + ga], A.pose1[5ull * ns + ga],
+                                 A.pose1[6ull * ns + ga]};
+            const float qb[4] = {A.pose1[3ull * ns + gbi], A.pose1[4ull * ns + gbi], A.pose1[5ull * ns + gbi],
+                                 A.pose1[6ull * ns + gbi]};
+            const float ha[3] = {half[ia], half[ldb + ia], half[2 * ldb + ia]};
+            const float hb[3] = {half[ib], half[ldb + ib], half[2 * ldb + ib]};
+            F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
+            float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
+            process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
+                             __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
+                             f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
+                             f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
+            const float out[14] = {xab.x, xab.y, xab.z, qab[0], qab[1], qab[2], qab[3],
+                                   xbb.x, xbb.y, xbb.z, qbb[0], qbb[1], qbb[2], qbb[3]};
+#pragma unroll
+            for (int c = 0; c < 14; ++c) r[static_cast<size_t>(c) * rs] = out[c];
+        }
+        T.sync();
+        // every body's sum over its contacts, in contact order
+        for (uint32_t x = T.rank(); x < nb; x += T.size()) {
+            const uint32_t lo = R.off[x], hi = R.off[x + 1];
+            if (lo == hi) continue;
+            const uint32_t gx = b0 + x;
+            float acc[7];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) acc[c] = grow(G.gout, ns, c, gx);
+            for (uint32_t e = lo; e < hi; ++e) {
+                const uint32_t k = entry(e);
+                const uint32_t side = (SC.ab(k) & 0xFFFFu) == x ? 0u : 7u;
+                const float* r = A.rec + cbase + k;
+#pragma unroll
+                for (int c = 0; c < 7; ++c) acc[c] += r[static_cast<size_t>(side + c) * rs];
+            }
+#pragma unroll
+            for (int c = 0; c < 7; ++c) grow(G.gout, ns, c, gx) = acc[c];
+        }
+        T.sync();
     }
     // ── integration, from the state at the frame's start ──
     const GlobalBodies B0{P_.gb};
