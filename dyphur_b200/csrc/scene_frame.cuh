@@ -33,6 +33,20 @@ __host__ __device__ __forceinline__ uint32_t frame_body_bytes(uint32_t nb) {
     return scene_body_bytes(nb) + kFrameBodyRows * 4u * ldb;
 }
 
+// Overlap bits of the candidate-pair search: body a has ceil((nb - 1 - a) /
+// 32) words, one per chunk of 32 partners b > a, laid out by ascending a.
+// S(t) = sum over u = 1..t of ceil(u / 32) = 16 q (q + 1) + (q + 1) r, t = 32 q + r.
+__host__ __device__ __forceinline__ uint32_t chunk_prefix(uint32_t t) {
+    const uint32_t q = t >> 5, r = t & 31u;
+    return 16u * q * (q + 1u) + (q + 1u) * r;
+}
+__host__ __device__ __forceinline__ uint32_t overlap_mask_words(uint32_t nb) {
+    return nb ? chunk_prefix(nb - 1u) : 0u;
+}
+__host__ __device__ __forceinline__ uint32_t overlap_mask_base(uint32_t nb, uint32_t a) {
+    return chunk_prefix(nb - 1u) - chunk_prefix(nb - 1u - a);
+}
+
 struct FrameBufs {
     const uint32_t* pair_base;     // [n_scenes + 1] first pair slot of each scene (capacity 48 n + 64)
     const uint32_t* contact_base;  // [n_scenes + 1] first contact slot of each scene (capacity 16 n + 64)
@@ -164,10 +178,17 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     T.sync();
     phase_mark(T, P_, 0, t0);
     // ── candidate pairs: per body a, the partners b > a in ascending order ──
+    // The count pass keeps each 32-partner chunk's overlap bits at the end of
+    // the team's shared memory when they fit there, so the write pass reads
+    // them instead of testing the boxes again.
+    const uint32_t mask_words = overlap_mask_words(nb);
+    const uint32_t mask_off = (smem_bytes - 4u * mask_words) & ~15u;
+    const bool keep_masks = 4u * mask_words <= smem_bytes && frame_body_bytes(nb) <= mask_off;
+    uint32_t* masks = reinterpret_cast<uint32_t*>(smem + mask_off);
     for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
         const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
-        uint32_t c = 0;
-        for (uint32_t j0 = a + 1; j0 < nb; j0 += 32u) {
+        uint32_t c = 0, w = overlap_mask_base(nb, a);
+        for (uint32_t j0 = a + 1; j0 < nb; j0 += 32u, ++w) {
             const uint32_t j = j0 + lane;
             bool ov = false;
             if (j < nb) {
@@ -175,7 +196,9 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
                              box[5 * ldb + j]};
                 ov = box_overlap(n, q);
             }
-            c += __popc(__ballot_sync(0xffffffffu, ov));
+            const unsigned bal = __ballot_sync(0xffffffffu, ov);
+            if (keep_masks && lane == 0) masks[w] = bal;
+            c += __popc(bal);
         }
         if (lane == 0) R.cnt[a] = c;
     }
@@ -203,18 +226,26 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     const SceneContacts SC{in_smem ? reinterpret_cast<uint32_t*>(smem + body_bytes) + pwords
                                    : F.words + F.contact_base[s] + s,
                            in_smem ? ldc : F.words_stride};
+    // the masks survive the write pass unless the pairs themselves reach them
+    const bool use_masks = keep_masks && (!in_smem || body_bytes + 4u * pwords <= mask_off);
     for (uint32_t a = T.warp(); a < nb; a += T.warps()) {
         const BoxF q{box[a], box[ldb + a], box[2 * ldb + a], box[3 * ldb + a], box[4 * ldb + a], box[5 * ldb + a]};
-        uint32_t pos = R.off[a];
-        for (uint32_t j0 = a + 1; j0 < nb && pos < P; j0 += 32u) {
+        uint32_t pos = R.off[a], w = overlap_mask_base(nb, a);
+        for (uint32_t j0 = a + 1; j0 < nb && pos < P; j0 += 32u, ++w) {
             const uint32_t j = j0 + lane;
-            bool ov = false;
-            if (j < nb) {
-                const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
-                             box[5 * ldb + j]};
-                ov = box_overlap(n, q);
+            unsigned bal;
+            if (use_masks) {
+                bal = masks[w];
+            } else {
+                bool ov = false;
+                if (j < nb) {
+                    const BoxF n{box[j], box[ldb + j], box[2 * ldb + j], box[3 * ldb + j], box[4 * ldb + j],
+                                 box[5 * ldb + j]};
+                    ov = box_overlap(n, q);
+                }
+                bal = __ballot_sync(0xffffffffu, ov);
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, ov);
+            const bool ov = (bal >> lane) & 1u;
             const uint32_t at = pos + __popc(bal & ((1u << lane) - 1u));
             if (ov && at < P) pairs[at] = a | (j << 16);
             pos += __popc(bal);
