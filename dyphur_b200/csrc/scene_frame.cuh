@@ -90,8 +90,9 @@ struct FrameParams {
 
 // Phases of a scene's fused frame, timed per scene by its team leader when
 // phase_ns is set: 0 staging + integrate + leaf boxes, 1 pair search,
-// 2 narrowphase, 3 contact solve, 4 write-back.
-constexpr int kFramePhases = 5;
+// 2 narrowphase, 3 contact-solve set-up (lists, colours or levels, groups),
+// 4 sweep + renormalisation, 5 write-back.
+constexpr int kFramePhases = 6;
 
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
@@ -321,9 +322,14 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     if (m > 0) {
         SolveRecord rec{};
         if (adj) rec = SolveRecord{adj->rec, adj->rec_stride, cbase, adj->qs, adj->n_stride, b0, adj->flag};
+        uint64_t t_sweep = 0;
         if (!scene_solve(T, nb, m, SB, R, SC, P_.mode, P_.n_iters, P_.mu, P_.dt, sh, colored, n_colors, rounds,
-                         adj ? &rec : nullptr, &groups))
+                         adj ? &rec : nullptr, &groups, P_.phase_ns ? &t_sweep : nullptr))
             return false;
+        if (P_.phase_ns && T.leader()) {
+            atomicAdd(&P_.phase_ns[3], static_cast<unsigned long long>(t_sweep - t0));
+            t0 = t_sweep;
+        }
         if (!adj) {
             for (uint32_t k = T.rank(); k < m; k += T.size())
                 F.color_raw[cbase + k] = colored ? SC.done(k) : kUncolored;
@@ -331,10 +337,10 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
         }
     }
     if (out) *out = FrameOut{SC, m, groups};
-    phase_mark(T, P_, 3, t0);
+    phase_mark(T, P_, 4, t0);
     if (!adj) scene_store_bodies(T, B, b0, nb, SB);
     T.sync();
-    phase_mark(T, P_, 4, t0);
+    phase_mark(T, P_, 5, t0);
     return true;
 }
 

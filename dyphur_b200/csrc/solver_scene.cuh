@@ -392,7 +392,8 @@ template <class Team>
 __device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneBodies& SB, const SceneSolverRows& R,
                             const SceneContacts& SC, int mode, int n_iters, float mu, float dt, SceneShared& sh,
                             bool& colored_out, uint32_t& n_colors_out, uint32_t& rounds_out,
-                            const SolveRecord* rec = nullptr, uint32_t* groups_out = nullptr) {
+                            const SolveRecord* rec = nullptr, uint32_t* groups_out = nullptr,
+                            uint64_t* sweep_start = nullptr) {
     // ── predecessors in contact order: b-side lists (scan, fill, sort) ──
     if (T.leader()) {
         sh.carry = 0u;
@@ -501,6 +502,11 @@ __device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneB
         }
     }
     scene_group(T, m, groups, base, SC, sh.scan, &sh.carry);
+    if (sweep_start && T.leader()) {
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        *sweep_start = t;
+    }
     // ── sweeps and renormalisation ──
     bool deferred = false;
     if (groups_out) *groups_out = groups;

@@ -509,9 +509,10 @@ class World:
 
     def phase_ns(self) -> np.ndarray:
         """Summed ns of the fused frames' phases since the last read: staging + integrate + boxes,
-        pair search, narrowphase, contact solve, write-back."""
-        out = np.zeros(5, np.uint64)
-        check(capi.lib().dyph_world_download_phase_ns(self.h, None, out.ctypes.data, 5), "phase_ns")
+        pair search, narrowphase, solve set-up (lists, colours or levels, groups), sweep +
+        renormalisation, write-back."""
+        out = np.zeros(6, np.uint64)
+        check(capi.lib().dyph_world_download_phase_ns(self.h, None, out.ctypes.data, 6), "phase_ns")
         return out
 
     def sync_lists(self) -> None:

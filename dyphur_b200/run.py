@@ -89,7 +89,8 @@ def profile(world, scene, frames: int, warm: int = 30) -> None:
         ph = world.phase_ns().astype(np.float64)
         world.phase_timing(False)
         fb.copy_(init)
-        labels = ("stage+integrate+boxes", "pair search", "narrowphase", "contact solve", "write-back")
+        labels = ("stage+integrate+boxes", "pair search", "narrowphase", "solve set-up", "sweep+renorm",
+                  "write-back")
         print(f"-- Fused frame: {ms:.3f} ms per frame over {frames} warm frames ({scene.n_scenes} scenes, "
               f"{scene.n_bodies} bodies); phases, share of the scenes' summed work time --")
         for name, v in zip(labels, ph):

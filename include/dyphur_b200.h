@@ -432,10 +432,11 @@ dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dy
  * reference's --profile mode (examples/stress_test_blocks/main.cpp:199-254)
  * for a frame that is one kernel: with it on, every scene's team leader adds
  * the device-clock ns of its phases — 0 staging, integrate and leaf boxes,
- * 1 pair search, 2 narrowphase, 3 contact solve, 4 write-back — summed over
- * scenes (work time, not wall time). Drops captured graphs; invalid for
- * worlds that are not fused. dyph_world_download_phase_ns reads (cap >= 5)
- * and clears the sums (blocking). */
+ * 1 pair search, 2 narrowphase, 3 contact-solve set-up (contact lists,
+ * colours or levels, groups), 4 sweep and renormalisation, 5 write-back —
+ * summed over scenes (work time, not wall time). Drops captured graphs;
+ * invalid for worlds that are not fused. dyph_world_download_phase_ns reads
+ * (cap >= 6) and clears the sums (blocking). */
 dyph_status dyph_world_set_phase_timing(dyph_world* w, int on);
 dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s, uint64_t* out, uint32_t cap);
 /* ── adjoint: gradients through fused batched frames. No reference
