@@ -61,10 +61,14 @@ struct dyph_world {
     float* a_pose1 = nullptr;            // [7][n]
     float* a_qs = nullptr;               // [4][n]
     float* a_g[2] = {nullptr, nullptr};  // [13][n] adjoint ping-pong
-    float* a_seg = nullptr;              // [a_seg_frames][13][n] states of one checkpoint segment
+    float* a_seg[2] = {nullptr, nullptr};  // [a_seg_frames][13][n] states of a checkpoint segment (double buffer)
     uint32_t a_seg_frames = 0;
+    uint32_t* a_words = nullptr;         // contact words of spilled scenes, the adjoint's own
+    uint32_t* a_pairs = nullptr;         // pair slots of spilled scenes, the adjoint's own
+    cudaStream_t a_stream = nullptr;     // re-steps the next segment while the adjoint runs
+    cudaEvent_t a_free = nullptr, a_ready = nullptr;
     uint32_t* a_flag = nullptr;
-    uint32_t f_words_stride = 0, f_contact_slots = 0;
+    uint32_t f_words_stride = 0, f_contact_slots = 0, f_pair_slots = 0;
     // Knobs of the fused kernel (dyph_world_set_fused_config / dyph_world_autotune).
     std::vector<uint32_t> h_body_offset;  // host copy of the scenes' body ranges
     uint32_t f_smem_cap = 0;              // shared memory cap per block (0 = what the largest scene needs)
@@ -232,9 +236,12 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
                   w->f_words, w->f_pos, w->f_items, w->f_phase, w->a_rec, w->a_pose1, w->a_qs, w->a_g[0],
-                  w->a_g[1], w->a_seg, w->a_flag};
+                  w->a_g[1], w->a_seg[0], w->a_seg[1], w->a_flag, w->a_words, w->a_pairs};
     for (void* p : fb)
         if (p) cudaFree(p);
+    if (w->a_stream) cudaStreamDestroy(w->a_stream);
+    if (w->a_free) cudaEventDestroy(w->a_free);
+    if (w->a_ready) cudaEventDestroy(w->a_ready);
     broadphase_destroy(w->bp);
     narrowphase_destroy(w->np);
     xpbd_destroy(w->sv);
@@ -488,6 +495,7 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     w->f_items = nullptr;
     const size_t pslots = pb[n_scenes], cslots = cb[n_scenes];
     w->f_contact_slots = static_cast<uint32_t>(cslots);
+    w->f_pair_slots = static_cast<uint32_t>(pslots);
     w->f_words_stride = static_cast<uint32_t>(cslots + n_scenes);
     const size_t sizes[] = {n_scenes + 1ull, n_scenes + 1ull, pslots, 9 * cslots, cslots, 4ull * n_scenes,
                             static_cast<size_t>(kSceneWords) * w->f_words_stride, 2ull * n_scenes};
@@ -902,17 +910,38 @@ dyph_status adjoint_buffers(dyph_world* w, uint32_t seg_frames) {
         if (cudaMalloc(&w->a_rec, static_cast<size_t>(kRecWords) * w->f_contact_slots * 4) != cudaSuccess ||
             cudaMalloc(&w->a_pose1, 7 * n * 4) != cudaSuccess || cudaMalloc(&w->a_qs, 4 * n * 4) != cudaSuccess ||
             cudaMalloc(&w->a_g[0], 13 * n * 4) != cudaSuccess || cudaMalloc(&w->a_g[1], 13 * n * 4) != cudaSuccess ||
-            cudaMalloc(&w->a_flag, 4) != cudaSuccess)
+            cudaMalloc(&w->a_flag, 4) != cudaSuccess ||
+            cudaMalloc(&w->a_words, static_cast<size_t>(kSceneWords) * w->f_words_stride * 4) != cudaSuccess ||
+            cudaMalloc(&w->a_pairs, static_cast<size_t>(std::max(w->f_pair_slots, 1u)) * 4) != cudaSuccess)
             return DYPH_ERR_NOMEM;
+        DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->a_stream, cudaStreamNonBlocking));
+        DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->a_free, cudaEventDisableTiming));
+        DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->a_ready, cudaEventDisableTiming));
         DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(w->frame_smem)));
     }
     if (seg_frames > w->a_seg_frames) {
-        if (w->a_seg) cudaFree(w->a_seg);
-        w->a_seg = nullptr;
+        for (float*& b : w->a_seg) {
+            if (b) cudaFree(b);
+            b = nullptr;
+        }
         w->a_seg_frames = 0;
-        if (cudaMalloc(&w->a_seg, static_cast<size_t>(seg_frames) * 13 * n * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
+        for (float*& b : w->a_seg)
+            if (cudaMalloc(&b, static_cast<size_t>(seg_frames) * 13 * n * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
         w->a_seg_frames = seg_frames;
+    }
+    return DYPH_OK;
+}
+
+// The states at frames f0 .. f0 + len - 1 of a rollout, re-stepped from the
+// checkpoint at f0 into `out` on stream s.
+dyph_status restep_segment(dyph_world* w, const float* ckpt, int32_t len, float* out, cudaStream_t s) {
+    const size_t n = w->desc.bodies.n;
+    dyph_status st = unpack_state(w, ckpt, s);
+    if (st != DYPH_OK) return st;
+    for (int32_t j = 0; j < len; ++j) {
+        if ((st = pack_state(w, out + static_cast<size_t>(j) * 13 * n, s)) != DYPH_OK) return st;
+        if (j + 1 < len && (st = dyph_world_step(w, 1, reinterpret_cast<dyph_stream>(s))) != DYPH_OK) return st;
     }
     return DYPH_OK;
 }
@@ -954,21 +983,30 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     const float sub_dt = ip.dt / static_cast<float>(ip.n_substeps);
     SceneBufs S{w->bp->body_offset, w->bp->bvh.scene_of, w->sv->scene_order, nullptr, nullptr, 0, w->bp->n_scenes,
                 w->frame_smem};
-    FrameBufs F{w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                w->f_words, w->f_words_stride, w->f_contact_slots};
+    // The adjoint's recomputed frames spill into their own words and pair
+    // slots, so the next segment can be re-stepped at the same time.
+    FrameBufs F{w->f_pair_base, w->f_contact_base, w->a_pairs, w->f_contact_raw, w->f_color_raw, w->f_counts,
+                w->a_words, w->f_words_stride, w->f_contact_slots};
     AdjRun A{w->a_rec, w->f_contact_slots, w->a_pose1, w->a_qs, static_cast<uint32_t>(n), w->a_flag};
-    int cur = 0;
+    int cur = 0, buf = 0;
     const int32_t n_seg = (n_frames + every - 1) / every;
+    auto seg_len = [&](int32_t seg) { return std::min(every, n_frames - seg * every); };
+    auto ckpt = [&](int32_t seg) { return d_ckpt + static_cast<size_t>(seg) * 13 * n; };
+    if ((st = restep_segment(w, ckpt(n_seg - 1), seg_len(n_seg - 1), w->a_seg[buf], cs)) != DYPH_OK) return st;
     for (int32_t seg = n_seg - 1; seg >= 0; --seg) {
-        const int32_t f0 = seg * every, len = std::min(every, n_frames - f0);
-        // states at frames f0 .. f0 + len - 1, recomputed from the checkpoint
-        if ((st = unpack_state(w, d_ckpt + static_cast<size_t>(seg) * 13 * n, cs)) != DYPH_OK) return st;
-        for (int32_t j = 0; j < len; ++j) {
-            if ((st = pack_state(w, w->a_seg + static_cast<size_t>(j) * 13 * n, cs)) != DYPH_OK) return st;
-            if (j + 1 < len && (st = dyph_world_step(w, 1, s)) != DYPH_OK) return st;
+        const int32_t len = seg_len(seg);
+        if (seg > 0) {
+            // segment seg - 1 is re-stepped on the side stream into the other
+            // buffer (free once the adjoint of segment seg + 1 is done) while
+            // the adjoint of segment seg runs
+            DYPH_CUDA_TRY(cudaEventRecord(w->a_free, cs));
+            DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_free, 0));
+            if ((st = restep_segment(w, ckpt(seg - 1), seg_len(seg - 1), w->a_seg[buf ^ 1], w->a_stream)) != DYPH_OK)
+                return st;
+            DYPH_CUDA_TRY(cudaEventRecord(w->a_ready, w->a_stream));
         }
         for (int32_t j = len - 1; j >= 0; --j) {
-            FrameParams P{state_view(w, w->a_seg + static_cast<size_t>(j) * 13 * n), d.shapes, ip.gravity[0],
+            FrameParams P{state_view(w, w->a_seg[buf] + static_cast<size_t>(j) * 13 * n), d.shapes, ip.gravity[0],
                           ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt, w->sv->friction, ip.dt,
                           ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->meta,
                           w->bp->counts, w->np->counts, w->stats + 4, nullptr};
@@ -978,6 +1016,8 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
             DYPH_CUDA_TRY(cudaGetLastError());
             cur ^= 1;
         }
+        if (seg > 0) DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_ready, 0));
+        buf ^= 1;
     }
     DYPH_CUDA_TRY(cudaMemcpyAsync(d_grad_init, w->a_g[cur], 13 * n * 4, cudaMemcpyDeviceToDevice, cs));
     uint32_t flag = 0;
