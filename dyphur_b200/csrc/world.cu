@@ -992,10 +992,13 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     const int32_t n_seg = (n_frames + every - 1) / every;
     auto seg_len = [&](int32_t seg) { return std::min(every, n_frames - seg * every); };
     auto ckpt = [&](int32_t seg) { return d_ckpt + static_cast<size_t>(seg) * 13 * n; };
-    if ((st = restep_segment(w, ckpt(n_seg - 1), seg_len(n_seg - 1), w->a_seg[buf], cs)) != DYPH_OK) return st;
+    // With a checkpoint at every frame the checkpoints are the states: nothing is re-stepped.
+    const bool restep = every > 1;
+    if (restep && (st = restep_segment(w, ckpt(n_seg - 1), seg_len(n_seg - 1), w->a_seg[buf], cs)) != DYPH_OK)
+        return st;
     for (int32_t seg = n_seg - 1; seg >= 0; --seg) {
         const int32_t len = seg_len(seg);
-        if (seg > 0) {
+        if (restep && seg > 0) {
             // segment seg - 1 is re-stepped on the side stream into the other
             // buffer (free once the adjoint of segment seg + 1 is done) while
             // the adjoint of segment seg runs
@@ -1006,7 +1009,8 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
             DYPH_CUDA_TRY(cudaEventRecord(w->a_ready, w->a_stream));
         }
         for (int32_t j = len - 1; j >= 0; --j) {
-            FrameParams P{state_view(w, w->a_seg[buf] + static_cast<size_t>(j) * 13 * n), d.shapes, ip.gravity[0],
+            float* state = restep ? w->a_seg[buf] + static_cast<size_t>(j) * 13 * n : const_cast<float*>(ckpt(seg));
+            FrameParams P{state_view(w, state), d.shapes, ip.gravity[0],
                           ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt, w->sv->friction, ip.dt,
                           ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->meta,
                           w->bp->counts, w->np->counts, w->stats + 4, nullptr};
@@ -1016,7 +1020,7 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
             DYPH_CUDA_TRY(cudaGetLastError());
             cur ^= 1;
         }
-        if (seg > 0) DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_ready, 0));
+        if (restep && seg > 0) DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_ready, 0));
         buf ^= 1;
     }
     DYPH_CUDA_TRY(cudaMemcpyAsync(d_grad_init, w->a_g[cur], 13 * n * 4, cudaMemcpyDeviceToDevice, cs));
