@@ -1,15 +1,18 @@
 // Adjoint of one fused frame of batched scenes (included by world.cu after
-// scene_frame.cuh). One thread block per scene:
-//   1. recompute the frame from its starting state (frame_scene with an
-//      AdjRun), recording the pose after integrate, every contact's
-//      narrowphase branch, every acting contact's pre-solve body states and
-//      the quaternions before the renormalisations — the contact set and all
-//      branches are those of the forward frame;
-//   2. reverse the renormalisations, then the contact solves group by group
-//      in descending order (a group's contacts share no dynamic body), each
-//      with solve_contact_adj on its recorded pre-solve state;
-//   3. reverse the narrowphase (contact geometry -> the two bodies' poses
-//      after integrate) and the integration.
+// scene_frame.cuh), in two kernels so that frame f - 1's recomputation runs
+// while frame f's reverse pass does (they touch different buffers):
+//   record:  recompute the frame from its starting state (frame_scene with an
+//            AdjRun), recording the pose after integrate, every contact's
+//            narrowphase branch, every acting contact's pre-solve body states
+//            and the quaternions before the renormalisations — the contact
+//            set and all branches are those of the forward frame — and keep
+//            the scene's contact words (pairs, groups, geometry) in global
+//            memory;
+//   reverse: reverse the renormalisations, then the contact solves group by
+//            group in descending order (a group's contacts share no dynamic
+//            body), each with solve_contact_adj on its recorded pre-solve
+//            state, then the narrowphase (contact geometry -> the two bodies'
+//            poses after integrate) and the integration.
 // The adjoint of the state at the frame's end comes in, the adjoint of the
 // state at its start goes out, and the inverse masses' adjoints accumulate.
 #pragma once
@@ -46,23 +49,70 @@ __device__ __forceinline__ float& grow(float* g, uint32_t stride, int r, uint32_
     return g[static_cast<size_t>(r) * stride + i];
 }
 
-// The adjoint of scene s's frame by team T (`smem_bytes` of shared memory at smem).
+// A recorded frame's contact words and counts, kept for the reverse pass.
+struct AdjKeep {
+    uint32_t* words;  // [kSceneWords][words_stride], the layout of FrameBufs::words
+    uint32_t* mg;     // [2 n_scenes] contacts and groups of every scene
+};
+
+// Recomputation of scene s's frame with recording (team T, `smem_bytes` of
+// shared memory at smem); F.words is K.words, so a scene whose words spill
+// writes them in place and the others copy theirs out.
 template <class Team>
-__device__ void adjoint_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
-                              const SceneBufs& S, const FrameBufs& F, const FrameParams& P_, const AdjRun& A,
+__device__ void record_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
+                             const SceneBufs& S, const FrameBufs& F, const FrameParams& P_, const AdjRun& A,
+                             const AdjKeep& K) {
+    FrameOut fo{};
+    const bool ok = frame_scene(T, s, smem, smem_bytes, sh, S, F, P_, &A, &fo);
+    const uint32_t m = ok ? fo.m : 0u, groups = ok ? fo.groups : 0u;
+    const SceneContacts dst{K.words + F.contact_base[s] + s, F.words_stride};
+    const SceneContacts& SC = fo.SC;
+    if (ok && m > 0 && SC.w != dst.w) {
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
+            dst.ab(k) = SC.ab(k);
+            dst.ent(k) = SC.ent(k);
+#pragma unroll
+            for (int r = 0; r < 7; ++r) dst.g(r, k) = SC.g(r, k);
+        }
+        for (uint32_t g = T.rank(); g <= groups; g += T.size()) dst.pa(g) = SC.pa(g);
+    }
+    if (T.leader()) {
+        K.mg[2 * s] = m;
+        K.mg[2 * s + 1] = groups;
+    }
+    T.sync();
+}
+
+// The reverse pass of scene s's recorded frame by team T.
+template <class Team>
+__device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, SceneShared& sh, const SceneBufs& S,
+                              const FrameBufs& F, const FrameParams& P_, const AdjRun& A, const AdjKeep& K,
                               const AdjFrame& G) {
     const uint32_t ns = A.n_stride, rs = A.rec_stride;
     const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
-    FrameOut fo{};
-    if (!frame_scene(T, s, smem, smem_bytes, sh, S, F, P_, &A, &fo)) return;
     const uint32_t ldb = (nb + 3u) & ~3u;
     float* fb = reinterpret_cast<float*>(smem);
     const SceneBodies SB{fb, ldb};
     const SceneSolverRows R = scene_solver_rows(fb, ldb);
-    const uint32_t* info = R.cnt + ldb;
-    const float* half = reinterpret_cast<const float*>(info + ldb);
-    const SceneContacts& SC = fo.SC;
-    const uint32_t m = fo.m, cbase = F.contact_base[s];
+    uint32_t* info = R.cnt + ldb;
+    float* half = reinterpret_cast<float*>(info + ldb);
+    // the bodies' constant rows, shape types, flags and half extents
+    {
+        const GlobalBodies B{P_.gb};
+        for (uint32_t i = T.rank(); i < nb; i += T.size()) {
+            const uint32_t g = b0 + i, sh_i = P_.gb.shape[g];
+            fb[13 * ldb + i] = B.im(g);
+            fb[14 * ldb + i] = B.ixx(g); fb[15 * ldb + i] = B.iyy(g); fb[16 * ldb + i] = B.izz(g);
+            fb[17 * ldb + i] = B.ixy(g); fb[18 * ldb + i] = B.ixz(g); fb[19 * ldb + i] = B.iyz(g);
+            info[i] = P_.gs.type[sh_i] | (P_.gb.flags[g] << 8);
+            half[i] = P_.gs.half_x[sh_i];
+            half[ldb + i] = P_.gs.half_y[sh_i];
+            half[2 * ldb + i] = P_.gs.half_z[sh_i];
+        }
+    }
+    const SceneContacts SC{K.words + F.contact_base[s] + s, F.words_stride};
+    const uint32_t m = K.mg[2 * s], n_groups = K.mg[2 * s + 1], cbase = F.contact_base[s];
+    T.sync();
     // ── adjoint of the frame's end state ──
     for (uint32_t i = T.rank(); i < nb; i += T.size())
         for (int r = 0; r < 13; ++r) grow(G.gout, ns, r, b0 + i) = G.gin[static_cast<size_t>(r) * ns + b0 + i];
@@ -91,7 +141,7 @@ __device__ void adjoint_scene(const Team& T, uint32_t s, unsigned char* smem, ui
         }
         T.sync();
         // ── contact solves, last group first ──
-        for (int g = static_cast<int>(fo.groups) - 1; g >= 0; --g) {
+        for (int g = static_cast<int>(n_groups) - 1; g >= 0; --g) {
             const uint32_t end = SC.pa(g + 1);
             for (uint32_t idx = SC.pa(g) + T.rank(); idx < end; idx += T.size()) {
                 const uint32_t k = SC.ent(idx);
@@ -272,33 +322,48 @@ __device__ void adjoint_scene(const Team& T, uint32_t s, unsigned char* smem, ui
     T.sync();
 }
 
-// Work items as for scene_frame_kernel: a large scene per block, or up to
-// four small scenes, one per warp.
-__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_adjoint_kernel(SceneBufs S, FrameBufs F,
-                                                                               FrameParams P_, AdjRun A,
-                                                                               AdjFrame G,
-                                                                               const uint32_t* __restrict__ items,
-                                                                               uint32_t n_items) {
+// Work items as for scene_frame_kernel: a large scene per block, two
+// mid-size scenes on two warps each, or up to four small scenes, one per warp.
+template <class Fn>
+__device__ __forceinline__ void for_each_item(const uint32_t* items, uint32_t n_items, uint32_t smem_bytes, Fn&& fn) {
     extern __shared__ __align__(16) unsigned char scene_smem[];
     __shared__ SceneShared sh[kSceneThreads / 32];
     const uint32_t warp = threadIdx.x >> 5;
-    const uint32_t share = (S.smem_bytes / 4u) & ~15u;
+    const uint32_t share = (smem_bytes / 4u) & ~15u;
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
         const uint32_t kind = items[4 * it + 1];
         if (kind == kItemBlock) {
-            adjoint_scene(BlockTeam{}, items[4 * it], scene_smem, S.smem_bytes, sh[0], S, F, P_, A, G);
+            fn(BlockTeam{}, items[4 * it], scene_smem, smem_bytes, sh[0]);
         } else if (kind == kItemHalf) {
             const uint32_t half = warp >> 1, s = items[4 * it + 2 * half];
-            if (s != kItemEmpty)
-                adjoint_scene(HalfTeam{half}, s, scene_smem + half * 2u * share, 2u * share, sh[2 * half], S, F, P_,
-                              A, G);
+            if (s != kItemEmpty) fn(HalfTeam{half}, s, scene_smem + half * 2u * share, 2u * share, sh[2 * half]);
         } else {
             const uint32_t s = items[4 * it + warp];
-            if (s != kItemEmpty)
-                adjoint_scene(WarpTeam{}, s, scene_smem + warp * share, share, sh[warp], S, F, P_, A, G);
+            if (s != kItemEmpty) fn(WarpTeam{}, s, scene_smem + warp * share, share, sh[warp]);
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(kSceneThreads, 4) scene_frame_record_kernel(SceneBufs S, FrameBufs F,
+                                                                              FrameParams P_, AdjRun A, AdjKeep K,
+                                                                              const uint32_t* __restrict__ items,
+                                                                              uint32_t n_items) {
+    for_each_item(items, n_items, S.smem_bytes,
+                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t bytes, SceneShared& sh) {
+                      record_scene(T, s, smem, bytes, sh, S, F, P_, A, K);
+                  });
+}
+
+__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_reverse_kernel(SceneBufs S, FrameBufs F,
+                                                                               FrameParams P_, AdjRun A, AdjKeep K,
+                                                                               AdjFrame G,
+                                                                               const uint32_t* __restrict__ items,
+                                                                               uint32_t n_items) {
+    for_each_item(items, n_items, S.smem_bytes,
+                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t, SceneShared& sh) {
+                      reverse_scene(T, s, smem, sh, S, F, P_, A, K, G);
+                  });
 }
 
 }  // namespace

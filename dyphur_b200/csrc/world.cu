@@ -57,16 +57,21 @@ struct dyph_world {
     uint32_t f_n_items = 0;
     unsigned long long* f_phase = nullptr;  // [kFramePhases] phase timing of fused frames (null = off)
     // Adjoint of fused frames (dyph_world_rollout_backward), allocated on first use.
-    float* a_rec = nullptr;              // [kRecWords][f_contact_slots]
-    float* a_pose1 = nullptr;            // [7][n]
-    float* a_qs = nullptr;               // [4][n]
+    // per recorded frame, two sets (frame parity): contact records, poses
+    // after integrate, quaternions before renormalisation, contact words, counts
+    float* a_rec[2] = {nullptr, nullptr};      // [kRecWords][f_contact_slots]
+    float* a_pose1[2] = {nullptr, nullptr};    // [7][n]
+    float* a_qs[2] = {nullptr, nullptr};       // [4][n]
+    uint32_t* a_words[2] = {nullptr, nullptr}; // [kSceneWords][f_words_stride]
+    uint32_t* a_mg[2] = {nullptr, nullptr};    // [2 n_scenes]
     float* a_g[2] = {nullptr, nullptr};  // [13][n] adjoint ping-pong
     float* a_seg[2] = {nullptr, nullptr};  // [a_seg_frames][13][n] states of a checkpoint segment (double buffer)
     uint32_t a_seg_frames = 0;
-    uint32_t* a_words = nullptr;         // contact words of spilled scenes, the adjoint's own
-    uint32_t* a_pairs = nullptr;         // pair slots of spilled scenes, the adjoint's own
-    cudaStream_t a_stream = nullptr;     // re-steps the next segment while the adjoint runs
-    cudaEvent_t a_free = nullptr, a_ready = nullptr;
+    uint32_t* a_pairs = nullptr;         // pair slots of spilled scenes, the recording's own
+    cudaStream_t a_stream = nullptr;     // re-steps the next checkpoint segment
+    cudaStream_t a_rstream = nullptr;    // records frame f - 1 while frame f is reversed
+    cudaEvent_t a_seg_ready = nullptr, a_rtail = nullptr;
+    cudaEvent_t a_rec_done[2] = {nullptr, nullptr}, a_rev_done[2] = {nullptr, nullptr};
     uint32_t* a_flag = nullptr;
     uint32_t f_words_stride = 0, f_contact_slots = 0, f_pair_slots = 0;
     // Knobs of the fused kernel (dyph_world_set_fused_config / dyph_world_autotune).
@@ -235,13 +240,21 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     }
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                  w->f_words, w->f_pos, w->f_items, w->f_phase, w->a_rec, w->a_pose1, w->a_qs, w->a_g[0],
-                  w->a_g[1], w->a_seg[0], w->a_seg[1], w->a_flag, w->a_words, w->a_pairs};
+                  w->f_words, w->f_pos, w->f_items, w->f_phase, w->a_g[0], w->a_g[1], w->a_seg[0], w->a_seg[1],
+                  w->a_flag, w->a_pairs};
     for (void* p : fb)
         if (p) cudaFree(p);
+    for (int k = 0; k < 2; ++k) {
+        void* pk[] = {w->a_rec[k], w->a_pose1[k], w->a_qs[k], w->a_words[k], w->a_mg[k]};
+        for (void* p : pk)
+            if (p) cudaFree(p);
+        if (w->a_rec_done[k]) cudaEventDestroy(w->a_rec_done[k]);
+        if (w->a_rev_done[k]) cudaEventDestroy(w->a_rev_done[k]);
+    }
     if (w->a_stream) cudaStreamDestroy(w->a_stream);
-    if (w->a_free) cudaEventDestroy(w->a_free);
-    if (w->a_ready) cudaEventDestroy(w->a_ready);
+    if (w->a_rstream) cudaStreamDestroy(w->a_rstream);
+    if (w->a_seg_ready) cudaEventDestroy(w->a_seg_ready);
+    if (w->a_rtail) cudaEventDestroy(w->a_rtail);
     broadphase_destroy(w->bp);
     narrowphase_destroy(w->np);
     xpbd_destroy(w->sv);
@@ -483,7 +496,9 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
                           reinterpret_cast<const void*>(scene_frame_kernel<5>),
                           reinterpret_cast<const void*>(scene_frame_kernel<6>)})
         DYPH_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_record_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem)));
     uint32_t** bufs[] = {&w->f_pair_base, &w->f_contact_base, &w->f_pair_raw, &w->f_contact_raw, &w->f_color_raw,
                          &w->f_counts, &w->f_words, &w->f_pos};
@@ -906,19 +921,21 @@ dyph_bodies state_view(const dyph_world* w, float* st) {
 
 dyph_status adjoint_buffers(dyph_world* w, uint32_t seg_frames) {
     const size_t n = w->desc.bodies.n;
-    if (!w->a_rec) {
-        if (cudaMalloc(&w->a_rec, static_cast<size_t>(kRecWords) * w->f_contact_slots * 4) != cudaSuccess ||
-            cudaMalloc(&w->a_pose1, 7 * n * 4) != cudaSuccess || cudaMalloc(&w->a_qs, 4 * n * 4) != cudaSuccess ||
-            cudaMalloc(&w->a_g[0], 13 * n * 4) != cudaSuccess || cudaMalloc(&w->a_g[1], 13 * n * 4) != cudaSuccess ||
-            cudaMalloc(&w->a_flag, 4) != cudaSuccess ||
-            cudaMalloc(&w->a_words, static_cast<size_t>(kSceneWords) * w->f_words_stride * 4) != cudaSuccess ||
-            cudaMalloc(&w->a_pairs, static_cast<size_t>(std::max(w->f_pair_slots, 1u)) * 4) != cudaSuccess)
-            return DYPH_ERR_NOMEM;
+    if (!w->a_g[0]) {
+        bool ok = cudaMalloc(&w->a_g[0], 13 * n * 4) == cudaSuccess && cudaMalloc(&w->a_g[1], 13 * n * 4) == cudaSuccess &&
+                  cudaMalloc(&w->a_flag, 4) == cudaSuccess &&
+                  cudaMalloc(&w->a_pairs, static_cast<size_t>(std::max(w->f_pair_slots, 1u)) * 4) == cudaSuccess;
+        for (int k = 0; k < 2 && ok; ++k)
+            ok = cudaMalloc(&w->a_rec[k], static_cast<size_t>(kRecWords) * w->f_contact_slots * 4) == cudaSuccess &&
+                 cudaMalloc(&w->a_pose1[k], 7 * n * 4) == cudaSuccess && cudaMalloc(&w->a_qs[k], 4 * n * 4) == cudaSuccess &&
+                 cudaMalloc(&w->a_words[k], static_cast<size_t>(kSceneWords) * w->f_words_stride * 4) == cudaSuccess &&
+                 cudaMalloc(&w->a_mg[k], 2 * static_cast<size_t>(std::max(w->bp->n_scenes, 1u)) * 4) == cudaSuccess;
+        if (!ok) return DYPH_ERR_NOMEM;
         DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->a_stream, cudaStreamNonBlocking));
-        DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->a_free, cudaEventDisableTiming));
-        DYPH_CUDA_TRY(cudaEventCreateWithFlags(&w->a_ready, cudaEventDisableTiming));
-        DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(w->frame_smem)));
+        DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->a_rstream, cudaStreamNonBlocking));
+        cudaEvent_t* evs[] = {&w->a_seg_ready, &w->a_rtail, &w->a_rec_done[0], &w->a_rec_done[1], &w->a_rev_done[0],
+                              &w->a_rev_done[1]};
+        for (cudaEvent_t* e : evs) DYPH_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
     if (seg_frames > w->a_seg_frames) {
         for (float*& b : w->a_seg) {
@@ -983,46 +1000,85 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     const float sub_dt = ip.dt / static_cast<float>(ip.n_substeps);
     SceneBufs S{w->bp->body_offset, w->bp->bvh.scene_of, w->sv->scene_order, nullptr, nullptr, 0, w->bp->n_scenes,
                 w->frame_smem};
-    // The adjoint's recomputed frames spill into their own words and pair
-    // slots, so the next segment can be re-stepped at the same time.
-    FrameBufs F{w->f_pair_base, w->f_contact_base, w->a_pairs, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                w->a_words, w->f_words_stride, w->f_contact_slots};
-    AdjRun A{w->a_rec, w->f_contact_slots, w->a_pose1, w->a_qs, static_cast<uint32_t>(n), w->a_flag};
-    int cur = 0, buf = 0;
+    // Three streams: the next checkpoint segment is re-stepped on a_stream,
+    // frame f - 1 is recorded on a_rstream while frame f is reversed on the
+    // caller's stream. Per-frame buffers alternate with the frame's parity; the
+    // recordings spill into their own pair slots and keep their contact words.
     const int32_t n_seg = (n_frames + every - 1) / every;
+    const bool restep = every > 1;  // with a checkpoint at every frame the checkpoints are the states
     auto seg_len = [&](int32_t seg) { return std::min(every, n_frames - seg * every); };
     auto ckpt = [&](int32_t seg) { return d_ckpt + static_cast<size_t>(seg) * 13 * n; };
-    // With a checkpoint at every frame the checkpoints are the states: nothing is re-stepped.
-    const bool restep = every > 1;
-    if (restep && (st = restep_segment(w, ckpt(n_seg - 1), seg_len(n_seg - 1), w->a_seg[buf], cs)) != DYPH_OK)
-        return st;
-    for (int32_t seg = n_seg - 1; seg >= 0; --seg) {
-        const int32_t len = seg_len(seg);
-        if (restep && seg > 0) {
-            // segment seg - 1 is re-stepped on the side stream into the other
-            // buffer (free once the adjoint of segment seg + 1 is done) while
-            // the adjoint of segment seg runs
-            DYPH_CUDA_TRY(cudaEventRecord(w->a_free, cs));
-            DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_free, 0));
-            if ((st = restep_segment(w, ckpt(seg - 1), seg_len(seg - 1), w->a_seg[buf ^ 1], w->a_stream)) != DYPH_OK)
-                return st;
-            DYPH_CUDA_TRY(cudaEventRecord(w->a_ready, w->a_stream));
-        }
-        for (int32_t j = len - 1; j >= 0; --j) {
-            float* state = restep ? w->a_seg[buf] + static_cast<size_t>(j) * 13 * n : const_cast<float*>(ckpt(seg));
-            FrameParams P{state_view(w, state), d.shapes, ip.gravity[0],
-                          ip.gravity[1], ip.gravity[2], sub_dt, 0.5f * sub_dt, w->sv->friction, ip.dt,
-                          ip.n_substeps, static_cast<int>(w->sv->mode), w->sv->n_iters, w->sv->meta,
-                          w->bp->counts, w->np->counts, w->stats + 4, nullptr};
-            AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
-            scene_frame_adjoint_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, cs>>>(S, F, P, A, G, w->f_items,
-                                                                                          w->f_n_items);
-            DYPH_CUDA_TRY(cudaGetLastError());
-            cur ^= 1;
-        }
-        if (restep && seg > 0) DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_ready, 0));
-        buf ^= 1;
+    auto state = [&](int32_t f) {
+        const int32_t seg = f / every, j = f % every;
+        return restep ? w->a_seg[seg & 1] + static_cast<size_t>(j) * 13 * n : const_cast<float*>(ckpt(seg));
+    };
+    auto params = [&](int32_t f) {
+        return FrameParams{state_view(w, state(f)), d.shapes, ip.gravity[0], ip.gravity[1], ip.gravity[2], sub_dt,
+                           0.5f * sub_dt, w->sv->friction, ip.dt, ip.n_substeps, static_cast<int>(w->sv->mode),
+                           w->sv->n_iters, w->sv->meta, w->bp->counts, w->np->counts, w->stats + 4, nullptr};
+    };
+    auto adj = [&](int32_t f) {
+        const int k = f & 1;
+        return AdjRun{w->a_rec[k], w->f_contact_slots, w->a_pose1[k], w->a_qs[k], static_cast<uint32_t>(n),
+                      w->a_flag};
+    };
+    auto keep = [&](int32_t f) { return AdjKeep{w->a_words[f & 1], w->a_mg[f & 1]}; };
+    auto frame_bufs = [&](int32_t f) {
+        return FrameBufs{w->f_pair_base, w->f_contact_base, w->a_pairs, w->f_contact_raw, w->f_color_raw,
+                         w->f_counts, w->a_words[f & 1], w->f_words_stride, w->f_contact_slots};
+    };
+    auto record = [&](int32_t f) -> dyph_status {
+        scene_frame_record_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, w->a_rstream>>>(
+            S, frame_bufs(f), params(f), adj(f), keep(f), w->f_items, w->f_n_items);
+        DYPH_CUDA_TRY(cudaGetLastError());
+        DYPH_CUDA_TRY(cudaEventRecord(w->a_rec_done[f & 1], w->a_rstream));
+        return DYPH_OK;
+    };
+    // everything below starts after the caller's stream
+    DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, cs));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rtail, 0));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_rtail, 0));
+    if (restep) {
+        st = restep_segment(w, ckpt(n_seg - 1), seg_len(n_seg - 1), w->a_seg[(n_seg - 1) & 1], w->a_stream);
+        if (st != DYPH_OK) return st;
+        DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
+        DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_seg_ready, 0));
     }
+    if ((st = record(n_frames - 1)) != DYPH_OK) return st;
+    int cur = 0;
+    for (int32_t f = n_frames - 1; f >= 0; --f) {
+        const int32_t seg = f / every;
+        // the previous segment is re-stepped as this one starts; its buffer was
+        // last read by the recordings of segment seg + 1 (all queued on
+        // a_rstream) and by their reverse passes (queued on cs, the last one
+        // being frame f + 1's)
+        if (restep && f % every == seg_len(seg) - 1 && seg > 0) {
+            DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, w->a_rstream));
+            DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rtail, 0));
+            if (f + 1 < n_frames) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rev_done[(f + 1) & 1], 0));
+            st = restep_segment(w, ckpt(seg - 1), seg_len(seg - 1), w->a_seg[(seg - 1) & 1], w->a_stream);
+            if (st != DYPH_OK) return st;
+            DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
+        }
+        if (f > 0) {
+            // frame f - 1's buffers were last used by the reverse pass of frame f + 1
+            if (restep && (f - 1) / every != seg) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_seg_ready, 0));
+            if (f + 1 < n_frames) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_rev_done[(f - 1) & 1], 0));
+            if ((st = record(f - 1)) != DYPH_OK) return st;
+        }
+        DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_rec_done[f & 1], 0));
+        AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
+        scene_frame_reverse_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, cs>>>(
+            S, frame_bufs(f), params(f), adj(f), keep(f), G, w->f_items, w->f_n_items);
+        DYPH_CUDA_TRY(cudaGetLastError());
+        DYPH_CUDA_TRY(cudaEventRecord(w->a_rev_done[f & 1], cs));
+        cur ^= 1;
+    }
+    // the side streams end before the caller's stream goes on
+    DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, w->a_rstream));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_rtail, 0));
+    DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
+    DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_seg_ready, 0));
     DYPH_CUDA_TRY(cudaMemcpyAsync(d_grad_init, w->a_g[cur], 13 * n * 4, cudaMemcpyDeviceToDevice, cs));
     uint32_t flag = 0;
     DYPH_CUDA_TRY(cudaMemcpyAsync(&flag, w->a_flag, 4, cudaMemcpyDeviceToHost, cs));
