@@ -85,9 +85,9 @@ __device__ void record_scene(const Team& T, uint32_t s, unsigned char* smem, uin
 
 // The reverse pass of scene s's recorded frame by team T.
 template <class Team>
-__device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, SceneShared& sh, const SceneBufs& S,
-                              const FrameBufs& F, const FrameParams& P_, const AdjRun& A, const AdjKeep& K,
-                              const AdjFrame& G) {
+__device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
+                              const SceneBufs& S, const FrameBufs& F, const FrameParams& P_, const AdjRun& A,
+                              const AdjKeep& K, const AdjFrame& G) {
     const uint32_t ns = A.n_stride, rs = A.rec_stride;
     const uint32_t b0 = S.body_offset[s], nb = S.body_offset[s + 1] - b0;
     const uint32_t ldb = (nb + 3u) & ~3u;
@@ -110,8 +110,22 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, Sc
             half[2 * ldb + i] = P_.gs.half_z[sh_i];
         }
     }
-    const SceneContacts SC{K.words + F.contact_base[s] + s, F.words_stride};
+    // the kept contact words, staged in shared memory after the bodies when
+    // they fit (the group loops below read them on their critical path)
+    const SceneContacts KC{K.words + F.contact_base[s] + s, F.words_stride};
     const uint32_t m = K.mg[2 * s], n_groups = K.mg[2 * s + 1], cbase = F.contact_base[s];
+    const uint32_t ldc = (m + 4u) & ~3u;
+    const bool staged = frame_body_bytes(nb) + kSceneWords * 4u * ldc <= smem_bytes;
+    const SceneContacts SC = staged ? SceneContacts{reinterpret_cast<uint32_t*>(smem + frame_body_bytes(nb)), ldc} : KC;
+    if (staged) {
+        for (uint32_t k = T.rank(); k < m; k += T.size()) {
+            SC.ab(k) = KC.ab(k);
+            SC.ent(k) = KC.ent(k);
+#pragma unroll
+            for (int r = 0; r < 7; ++r) SC.g(r, k) = KC.g(r, k);
+        }
+        for (uint32_t g = T.rank(); g <= n_groups; g += T.size()) SC.pa(g) = KC.pa(g);
+    }
     T.sync();
     // ── adjoint of the frame's end state ──
     for (uint32_t i = T.rank(); i < nb; i += T.size())
@@ -361,8 +375,8 @@ __global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_reverse_kernel(S
                                                                                const uint32_t* __restrict__ items,
                                                                                uint32_t n_items) {
     for_each_item(items, n_items, S.smem_bytes,
-                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t, SceneShared& sh) {
-                      reverse_scene(T, s, smem, sh, S, F, P_, A, K, G);
+                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t bytes, SceneShared& sh) {
+                      reverse_scene(T, s, smem, bytes, sh, S, F, P_, A, K, G);
                   });
 }
 
