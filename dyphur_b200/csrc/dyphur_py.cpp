@@ -271,6 +271,18 @@ PYBIND11_MODULE(dyphur_py, m) {
         .value("Colored", DYPH_SOLVER_COLORED)
         .value("ReferenceRounds", DYPH_SOLVER_REFERENCE_ROUNDS);
 
+    py::class_<dyph_fused_config>(m, "FusedConfig")
+        .def_readonly("smem_bytes", &dyph_fused_config::smem_bytes)
+        .def_readonly("teams", &dyph_fused_config::teams)
+        .def_readonly("warp_scenes", &dyph_fused_config::warp_scenes)
+        .def_readonly("half_scenes", &dyph_fused_config::half_scenes)
+        .def_readonly("block_scenes", &dyph_fused_config::block_scenes)
+        .def_readonly("blocks", &dyph_fused_config::blocks)
+        .def_readonly("blocks_per_sm", &dyph_fused_config::blocks_per_sm)
+        .def_readonly("register_blocks", &dyph_fused_config::register_blocks)
+        .def_readonly("ms_per_frame", &dyph_fused_config::ms_per_frame)
+        .def_readonly("candidates", &dyph_fused_config::candidates);
+
     py::class_<World>(m, "World")
         .def(py::init<Stream&, BodyStore&, ShapeStore&, const AABB&, const IntegratorParams&, uint32_t, uint32_t,
                       int, float, dyph_solver_mode>(),
@@ -279,6 +291,9 @@ PYBIND11_MODULE(dyphur_py, m) {
              py::keep_alive<1, 2>(), py::keep_alive<1, 3>(), py::keep_alive<1, 4>())
         .def("set_scenes", &World::set_scenes, "body_offset"_a, "bounds"_a)
         .def("step", &World::step, "s"_a, "n_frames"_a = 1)
+        .def("fused_config", &World::fused_config)
+        .def("set_fused_config", &World::set_fused_config, "smem_cap"_a, "teams"_a = 2, "register_blocks"_a = 0)
+        .def("autotune", &World::autotune, "s"_a, "frames"_a = 16)
         .def("hash", [](World& w, Stream& s) { return state_hash(s, w.bodies().view()); })
         .def("scene_hashes", &World::scene_hashes, "s"_a, "n_scenes"_a)
         .def("count", [](World& w) { return w.bodies().count(); })

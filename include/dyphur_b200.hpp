@@ -545,6 +545,21 @@ public:
         check(dyph_world_scene_hashes(h_, s.abi(), out.data(), n_scenes), "World::scene_hashes");
         return out;
     }
+    // Knobs of the fused batched frame (dyph_world_set_fused_config /
+    // dyph_world_autotune); every setting gives the same frames.
+    dyph_fused_config fused_config() {
+        dyph_fused_config c{};
+        check(dyph_world_fused_config(h_, &c), "World::fused_config");
+        return c;
+    }
+    void set_fused_config(uint32_t smem_cap, uint32_t teams = 2, uint32_t register_blocks = 0) {
+        check(dyph_world_set_fused_config(h_, smem_cap, teams, register_blocks), "World::set_fused_config");
+    }
+    dyph_fused_config autotune(Stream& s, int frames = 16) {
+        dyph_fused_config c{};
+        check(dyph_world_autotune(h_, frames, s.abi(), &c), "World::autotune");
+        return c;
+    }
     // State rows at creation ([13][capacity], device), the start of rollouts.
     const float* initial_rows() const noexcept { return initial_.data(); }
     BodyStore& bodies() noexcept { return *bodies_; }

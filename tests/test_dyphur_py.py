@@ -41,7 +41,7 @@ def test_module_has_reference_surface(dp):
         for m in members:
             assert hasattr(c, m), f"{cls}.{m}"
     assert hasattr(dp, "Box") and hasattr(dp, "Sphere")  # export_values
-    for extra in ("World", "ray_query", "rollout", "integrate", "XpbdSolver"):
+    for extra in ("World", "ray_query", "rollout", "integrate", "XpbdSolver", "FusedConfig"):
         assert hasattr(dp, extra)
 
 
@@ -197,6 +197,8 @@ def test_rollout_through_module_matches_ctypes_world(dp):
                  dp.SolverMode.Sequential)
     w.set_scenes([int(x) for x in scene.body_offset], [dp.AABB(*(float(x) for x in b)) for b in scene.bounds])
     s.wait()
+    cfg = w.autotune(s, 4)  # the configuration changes no frame
+    assert cfg.blocks >= 1 and cfg.warp_scenes + cfg.half_scenes + cfg.block_scenes == scene.n_scenes
     wc = device.World(scene, mode=1)
     target = torch.from_numpy(scene.targets).cuda()
     results = []
