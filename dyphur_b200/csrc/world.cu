@@ -1008,6 +1008,9 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     const bool restep = every > 1;  // with a checkpoint at every frame the checkpoints are the states
     auto seg_len = [&](int32_t seg) { return std::min(every, n_frames - seg * every); };
     auto ckpt = [&](int32_t seg) { return d_ckpt + static_cast<size_t>(seg) * 13 * n; };
+    // The frame's start state; the record and reverse kernels only read it
+    // (frame_scene with an AdjRun writes nothing back), so a checkpoint can
+    // serve directly.
     auto state = [&](int32_t f) {
         const int32_t seg = f / every, j = f % every;
         return restep ? w->a_seg[seg & 1] + static_cast<size_t>(j) * 13 * n : const_cast<float*>(ckpt(seg));
