@@ -9,7 +9,9 @@ bindings use, is not installed; pybind11 is.
 
 Numerics flags: ``--fmad=false -prec-div=true -prec-sqrt=true`` keep every
 float operation correctly rounded and uncontracted, which is what makes the
-kernels bit-identical to the reference's host arithmetic.
+kernels bit-identical to the reference's host arithmetic. The one exception is
+the adjoint's reverse kernel (``csrc/reverse.cu``, its own translation unit),
+built with approximate division and square root.
 """
 from __future__ import annotations
 
@@ -28,6 +30,12 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NV_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
                    "-ftz=false", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"), "-ccbin", "g++"]
+# The adjoint's reverse kernel (csrc/reverse.cu) alone: approximate division
+# and square root (it follows recorded branches; its gradients are checked
+# against FP64 within 1e-3 relative). Multiply-adds stay uncontracted, so every
+# team layout of a scene computes the same gradients bit for bit.
+REVERSE_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=false", "-prec-sqrt=false",
+                        "-ftz=false", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"), "-ccbin", "g++"]
 CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
 
@@ -59,14 +67,16 @@ def build_native(verbose_ptxas: bool = False) -> str:
     if not _newer(lib, deps):
         return lib
     cu_obj = os.path.join(BUILD_DIR, "dyphur_b200.o")
-    flags = NV_FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else [])
-    _run([NVCC] + flags + ["-c", os.path.join(CSRC, "dyphur_b200.cu"), "-o", cu_obj])
+    rev_obj = os.path.join(BUILD_DIR, "reverse.o")
+    ptxas = ["-Xptxas", "-v"] if verbose_ptxas else []
+    _run([NVCC] + NV_FLAGS + ptxas + ["-c", os.path.join(CSRC, "dyphur_b200.cu"), "-o", cu_obj])
+    _run([NVCC] + REVERSE_FLAGS + ptxas + ["-c", os.path.join(CSRC, "reverse.cu"), "-o", rev_obj])
     host_objs = []
     for src in ("scenes.cpp",):
         obj = os.path.join(BUILD_DIR, src.replace(".cpp", ".o"))
         _run(["g++"] + CXX_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj])
         host_objs.append(obj)
-    _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-ccbin", "g++", cu_obj] + host_objs +
+    _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-ccbin", "g++", cu_obj, rev_obj] + host_objs +
          ["-o", lib + ".tmp", "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
     os.replace(lib + ".tmp", lib)
     return lib

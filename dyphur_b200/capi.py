@@ -95,6 +95,8 @@ _PROTOS = {
     "dyph_world_fused_config": (_st, [_vp, C.POINTER(FusedConfig)]),
     "dyph_world_set_fused_config": (_st, [_vp, C.c_uint32, C.c_uint32, C.c_uint32]),
     "dyph_world_autotune": (_st, [_vp, C.c_int32, _vp, C.POINTER(FusedConfig)]),
+    "dyph_world_adjoint_config": (_st, [_vp, C.POINTER(FusedConfig)]),
+    "dyph_world_set_adjoint_config": (_st, [_vp, C.c_uint32, C.c_uint32]),
     "dyph_ray_query": (_st, [C.POINTER(BvhView), C.POINTER(Bodies), C.POINTER(Shapes), _vp, _vp, C.c_uint32, _vp]),
     "dyph_contact_sensor_create": (_st, [C.c_uint32, C.POINTER(_vp)]),
     "dyph_contact_sensor_destroy": (None, [_vp]),

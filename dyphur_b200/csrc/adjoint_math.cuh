@@ -1,6 +1,6 @@
 // Hand-written reverse-mode adjoints of the frame step's per-body, per-contact
-// and per-pair primitives (device code, included by the library's single
-// translation unit).
+// and per-pair primitives (device code of the adjoint's reverse kernel,
+// reverse.cu).
 //
 // Each *_adj routine takes the primal inputs of one primitive, the branch it
 // took in the forward pass (recorded there, so the adjoint differentiates the
@@ -29,22 +29,46 @@ __device__ __forceinline__ F3 operator-(F3 a) { return F3{-a.x, -a.y, -a.z}; }
 __device__ __forceinline__ F3 operator*(float s, F3 a) { return F3{s * a.x, s * a.y, s * a.z}; }
 __device__ __forceinline__ F3& operator+=(F3& a, F3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
 __device__ __forceinline__ F3& operator-=(F3& a, F3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
-__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// Sums of products with explicit fused multiply-adds. The reverse pass is
+// compiled without contraction, so the compiler fuses nothing by itself and
+// every team layout of a scene rounds alike; the fusions are written here,
+// where most of the adjoint's arithmetic is.
+__device__ __forceinline__ float fma2(float a0, float b0, float a1, float b1) {
+    return __fmaf_rn(a1, b1, a0 * b0);
+}
+__device__ __forceinline__ float fma3(float a0, float b0, float a1, float b1, float a2, float b2) {
+    return __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0));
+}
+__device__ __forceinline__ float dot(F3 a, F3 b) { return fma3(a.x, b.x, a.y, b.y, a.z, b.z); }
 __device__ __forceinline__ F3 cross(F3 a, F3 b) {
-    return F3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return F3{__fmaf_rn(a.y, b.z, -(a.z * b.y)), __fmaf_rn(a.z, b.x, -(a.x * b.z)), __fmaf_rn(a.x, b.y, -(a.y * b.x))};
+}
+// M^T v and M v for a 3x3 M.
+__device__ __forceinline__ F3 mtv(const float M[3][3], F3 v) {
+    return f3(fma3(M[0][0], v.x, M[1][0], v.y, M[2][0], v.z), fma3(M[0][1], v.x, M[1][1], v.y, M[2][1], v.z),
+              fma3(M[0][2], v.x, M[1][2], v.y, M[2][2], v.z));
+}
+__device__ __forceinline__ F3 mv(const float M[3][3], F3 v) {
+    return f3(fma3(M[0][0], v.x, M[0][1], v.y, M[0][2], v.z), fma3(M[1][0], v.x, M[1][1], v.y, M[1][2], v.z),
+              fma3(M[2][0], v.x, M[2][1], v.y, M[2][2], v.z));
+}
+// I v for the symmetric inertia I6 = ixx, iyy, izz, ixy, ixz, iyz.
+__device__ __forceinline__ F3 i6v(const float I6[6], F3 v) {
+    return f3(fma3(I6[0], v.x, I6[3], v.y, I6[4], v.z), fma3(I6[3], v.x, I6[1], v.y, I6[5], v.z),
+              fma3(I6[4], v.x, I6[5], v.y, I6[2], v.z));
 }
 
 // Adjoint of the rotation rows A(q) (make_axes; also the matrix of
 // world_inv_inertia): q̄ += Σ_ij Ā_ij ∂A_ij/∂q.
 __device__ __forceinline__ void rot_adj(const float q[4], const float Ab[3][3], float qb[4]) {
     const float w = q[0], x = q[1], y = q[2], z = q[3];
-    qb[0] += 2.f * (z * Ab[0][1] - y * Ab[0][2] - z * Ab[1][0] + x * Ab[1][2] + y * Ab[2][0] - x * Ab[2][1]);
-    qb[1] += 2.f * (y * Ab[0][1] + z * Ab[0][2] + y * Ab[1][0] - 2.f * x * Ab[1][1] + w * Ab[1][2] + z * Ab[2][0] -
-                    w * Ab[2][1] - 2.f * x * Ab[2][2]);
-    qb[2] += 2.f * (-2.f * y * Ab[0][0] + x * Ab[0][1] - w * Ab[0][2] + x * Ab[1][0] + z * Ab[1][2] + w * Ab[2][0] +
-                    z * Ab[2][1] - 2.f * y * Ab[2][2]);
-    qb[3] += 2.f * (-2.f * z * Ab[0][0] + w * Ab[0][1] + x * Ab[0][2] - w * Ab[1][0] - 2.f * z * Ab[1][1] +
-                    y * Ab[1][2] + x * Ab[2][0] + y * Ab[2][1]);
+    // sums of the products, grouped by the quaternion component they multiply
+    const float a01 = Ab[0][1] - Ab[1][0], a12 = Ab[1][2] - Ab[2][1], a20 = Ab[2][0] - Ab[0][2];
+    const float s01 = Ab[0][1] + Ab[1][0], s12 = Ab[1][2] + Ab[2][1], s20 = Ab[2][0] + Ab[0][2];
+    qb[0] += 2.f * fma3(z, a01, x, a12, y, a20);
+    qb[1] += 2.f * fma3(y, s01, z, s20, w, a12) - 4.f * x * (Ab[1][1] + Ab[2][2]);
+    qb[2] += 2.f * fma3(x, s01, z, s12, w, a20) - 4.f * y * (Ab[0][0] + Ab[2][2]);
+    qb[3] += 2.f * fma3(w, a01, x, s20, y, s12) - 4.f * z * (Ab[0][0] + Ab[1][1]);
 }
 
 __device__ __forceinline__ void rot_rows(const float q[4], float A[3][3]) { make_axes(q[0], q[1], q[2], q[3], A); }
@@ -53,49 +77,36 @@ __device__ __forceinline__ void rot_rows(const float q[4], float A[3][3]) { make
 __device__ __forceinline__ F3 winv(const float q[4], const float I6[6], F3 v) {
     float R[3][3];
     rot_rows(q, R);
-    const F3 l = f3(R[0][0] * v.x + R[1][0] * v.y + R[2][0] * v.z, R[0][1] * v.x + R[1][1] * v.y + R[2][1] * v.z,
-                    R[0][2] * v.x + R[1][2] * v.y + R[2][2] * v.z);
-    const F3 il = f3(I6[0] * l.x + I6[3] * l.y + I6[4] * l.z, I6[3] * l.x + I6[1] * l.y + I6[5] * l.z,
-                     I6[4] * l.x + I6[5] * l.y + I6[2] * l.z);
-    return f3(R[0][0] * il.x + R[0][1] * il.y + R[0][2] * il.z, R[1][0] * il.x + R[1][1] * il.y + R[1][2] * il.z,
-              R[2][0] * il.x + R[2][1] * il.y + R[2][2] * il.z);
+    return mv(R, i6v(I6, mtv(R, v)));
 }
 
 // Adjoint of y = winv(q, I, v): v̄ += W ȳ (W symmetric), q̄ += ∂(W v)/∂q^T ȳ.
 __device__ __forceinline__ void winv_adj(const float q[4], const float I6[6], F3 v, F3 yb, F3& vb, float qb[4]) {
     float R[3][3];
     rot_rows(q, R);
-    const F3 l = f3(R[0][0] * v.x + R[1][0] * v.y + R[2][0] * v.z, R[0][1] * v.x + R[1][1] * v.y + R[2][1] * v.z,
-                    R[0][2] * v.x + R[1][2] * v.y + R[2][2] * v.z);
-    const F3 il = f3(I6[0] * l.x + I6[3] * l.y + I6[4] * l.z, I6[3] * l.x + I6[1] * l.y + I6[5] * l.z,
-                     I6[4] * l.x + I6[5] * l.y + I6[2] * l.z);
-    // y = R il: il̄ = R^T ȳ, R̄ += ȳ il^T
-    const F3 ilb = f3(R[0][0] * yb.x + R[1][0] * yb.y + R[2][0] * yb.z, R[0][1] * yb.x + R[1][1] * yb.y + R[2][1] * yb.z,
-                      R[0][2] * yb.x + R[1][2] * yb.y + R[2][2] * yb.z);
-    // il = I l: l̄ = I il̄
-    const F3 lb = f3(I6[0] * ilb.x + I6[3] * ilb.y + I6[4] * ilb.z, I6[3] * ilb.x + I6[1] * ilb.y + I6[5] * ilb.z,
-                     I6[4] * ilb.x + I6[5] * ilb.y + I6[2] * ilb.z);
+    const F3 il = i6v(I6, mtv(R, v));
+    // y = R il: il̄ = R^T ȳ, R̄ += ȳ il^T; il = I l: l̄ = I il̄
+    const F3 lb = i6v(I6, mtv(R, yb));
     // l = R^T v: v̄ += R l̄, R̄ += v l̄^T
-    vb += f3(R[0][0] * lb.x + R[0][1] * lb.y + R[0][2] * lb.z, R[1][0] * lb.x + R[1][1] * lb.y + R[1][2] * lb.z,
-             R[2][0] * lb.x + R[2][1] * lb.y + R[2][2] * lb.z);
+    vb += mv(R, lb);
     const float yv[3] = {yb.x, yb.y, yb.z}, ilv[3] = {il.x, il.y, il.z};
     const float vv[3] = {v.x, v.y, v.z}, lbv[3] = {lb.x, lb.y, lb.z};
     float Rb[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) Rb[i][j] = yv[i] * ilv[j] + vv[i] * lbv[j];
+        for (int j = 0; j < 3; ++j) Rb[i][j] = fma2(yv[i], ilv[j], vv[i], lbv[j]);
     rot_adj(q, Rb, qb);
 }
 
 // Adjoint of y = q / |q|: q̄ = r ȳ - r^3 (q·ȳ) q.
 __device__ __forceinline__ void normalize_adj(const float q[4], const float yb[4], float qb[4]) {
-    const float s = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    const float s = __fmaf_rn(q[3], q[3], fma3(q[0], q[0], q[1], q[1], q[2], q[2]));
     const float r = 1.f / sqrtf(s);
-    const float qy = q[0] * yb[0] + q[1] * yb[1] + q[2] * yb[2] + q[3] * yb[3];
-    const float r3 = r * r * r;
+    const float qy = __fmaf_rn(q[3], yb[3], fma3(q[0], yb[0], q[1], yb[1], q[2], yb[2]));
+    const float r3qy = r * r * r * qy;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) qb[k] = r * yb[k] - r3 * qy * q[k];
+    for (int k = 0; k < 4; ++k) qb[k] = __fmaf_rn(r, yb[k], -(r3qy * q[k]));
 }
 
 // q' = q + h * Ω(a) q with the component formulas of integrate_body /
@@ -103,13 +114,13 @@ __device__ __forceinline__ void normalize_adj(const float q[4], const float yb[4
 __device__ __forceinline__ void quat_delta_adj(const float q[4], F3 a, float h, const float gb[4], float qb[4],
                                                F3& ab) {
     const float gw = gb[0], gx = gb[1], gy = gb[2], gz = gb[3];
-    qb[0] += gw + h * (a.x * gx + a.y * gy + a.z * gz);
-    qb[1] += gx + h * (-a.x * gw + a.z * gy - a.y * gz);
-    qb[2] += gy + h * (-a.y * gw - a.z * gx + a.x * gz);
-    qb[3] += gz + h * (-a.z * gw + a.y * gx - a.x * gy);
-    ab.x += h * (-q[1] * gw + q[0] * gx - q[3] * gy + q[2] * gz);
-    ab.y += h * (-q[2] * gw + q[3] * gx + q[0] * gy - q[1] * gz);
-    ab.z += h * (-q[3] * gw - q[2] * gx + q[1] * gy + q[0] * gz);
+    qb[0] += __fmaf_rn(h, fma3(a.x, gx, a.y, gy, a.z, gz), gw);
+    qb[1] += __fmaf_rn(h, fma3(-a.x, gw, a.z, gy, -a.y, gz), gx);
+    qb[2] += __fmaf_rn(h, fma3(-a.y, gw, -a.z, gx, a.x, gz), gy);
+    qb[3] += __fmaf_rn(h, fma3(-a.z, gw, a.y, gx, -a.x, gy), gz);
+    ab.x += h * __fmaf_rn(q[2], gz, fma3(-q[1], gw, q[0], gx, -q[3], gy));
+    ab.y += h * __fmaf_rn(-q[1], gz, fma3(-q[2], gw, q[3], gx, q[0], gy));
+    ab.z += h * __fmaf_rn(q[0], gz, fma3(-q[3], gw, -q[2], gx, q[1], gy));
 }
 
 // ── integrate (one body, n_substeps substeps of sub_dt) ─────────────────────

@@ -25,17 +25,24 @@ constexpr uint32_t kShapeSphere = 1u;
 // (dyph_set_spin_limit), so a test can make a wait give up quickly.
 constexpr uint32_t kSpinLimit = 1u << 24;
 
+// The device words below belong to dyphur_b200.cu, the library's main
+// translation unit (its kernels share them without relocatable device code).
+// reverse.cu, the second one, defines DYPH_DEVICE_GLOBAL as `static
+// __device__`: it gets private copies, which its one kernel never touches.
+#ifndef DYPH_DEVICE_GLOBAL
+#define DYPH_DEVICE_GLOBAL __device__
+#endif
+
 // Sticky device error word (DYPH_ERR_TIMEOUT ...), read by dyph_download_device_error.
-// Defined here: the library is compiled as one translation unit (dyphur_b200.cu).
-__device__ uint32_t g_device_error = 0u;
+DYPH_DEVICE_GLOBAL uint32_t g_device_error = 0u;
 
 // Where the first error was raised (1 look-back, 2 sort look-back, 3 grid
 // barrier, 5 sequential schedule, 6 / 7 tree walk, 8 narrowphase pair index).
-__device__ uint32_t g_device_error_site = 0u;
+DYPH_DEVICE_GLOBAL uint32_t g_device_error_site = 0u;
 
 // Iteration limit of the bounded waits in force (the default unless a
 // caller of dyph_set_spin_limit changed it).
-__device__ uint32_t g_spin_limit = kSpinLimit;
+DYPH_DEVICE_GLOBAL uint32_t g_spin_limit = kSpinLimit;
 
 __device__ __forceinline__ uint32_t spin_limit() { return __ldg(&g_spin_limit); }
 

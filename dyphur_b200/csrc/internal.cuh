@@ -140,6 +140,11 @@ dyph_status xpbd_set_scenes(dyph_xpbd* sv, uint32_t n_scenes, const uint32_t* h_
 // Pre-set kernel attributes of the sort (call once, outside graph capture).
 dyph_status sort_prepare();
 
+// The adjoint's reverse kernel (reverse.cu, its own translation unit), for
+// cudaLaunchKernel with the argument list (SceneBufs, FrameBufs, FrameParams,
+// AdjRun, AdjKeep, AdjFrame, const uint32_t* items, uint32_t n_items).
+const void* reverse_kernel();
+
 dyph_status integrate_launch(const dyph_bodies* bodies, const dyph_integrator_params* p, cudaStream_t s);
 
 }  // namespace dyph

@@ -1,5 +1,7 @@
-// Adjoint of one fused frame of batched scenes (included by world.cu after
-// scene_frame.cuh), in two kernels so that frame f - 1's recomputation runs
+// Adjoint of one fused frame of batched scenes (included after
+// scene_frame.cuh: by world.cu, whose scene_frame_record_kernel runs
+// record_scene, and by reverse.cu, whose scene_frame_reverse_kernel runs
+// reverse_scene), in two kernels so that frame f - 1's recomputation runs
 // while frame f's reverse pass does (they touch different buffers):
 //   record:  recompute the frame from its starting state (frame_scene with an
 //            AdjRun), recording the pose after integrate, every contact's
@@ -126,6 +128,19 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
         }
         for (uint32_t g = T.rank(); g <= n_groups; g += T.size()) SC.pa(g) = KC.pa(g);
     }
+    // The scene's contact records, staged after the contact words when both
+    // fit: rows 0-27 and 35 (poses before each solve, geometry, the solve's
+    // flags) are read once per contact, one dependency level after another;
+    // rows 28-34 and 0-13 are rewritten below and read back from there.
+    const uint32_t rec_off = frame_body_bytes(nb) + kSceneWords * 4u * ldc;
+    const bool rec_staged = staged && rec_off + kRecWords * 4u * ldc <= smem_bytes;
+    float* const recb = rec_staged ? reinterpret_cast<float*>(smem + rec_off) : A.rec + cbase;
+    const size_t rst = rec_staged ? ldc : rs;
+    if (rec_staged)
+        for (uint32_t e = T.rank(); e < 29u * m; e += T.size()) {
+            const uint32_t q = e / m, k = e - q * m, row = q < 28u ? q : 35u;
+            recb[static_cast<size_t>(row) * ldc + k] = A.rec[cbase + k + static_cast<size_t>(row) * rs];
+        }
     T.sync();
     // ── adjoint of the frame's end state ──
     for (uint32_t i = T.rank(); i < nb; i += T.size())
@@ -159,18 +174,18 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
             const uint32_t end = SC.pa(g + 1);
             for (uint32_t idx = SC.pa(g) + T.rank(); idx < end; idx += T.size()) {
                 const uint32_t k = SC.ent(idx);
-                const float* r = A.rec + cbase + k;
-                if (r[35ull * rs] == 0.f) continue;  // did not act
+                const float* r = recb + k;
+                if (r[35ull * rst] == 0.f) continue;  // did not act
                 const Contact ct = SC.contact(k);
                 const uint32_t ia = ct.a, ib = ct.b;
                 LocalPair L;
                 for (int j = 0; j < 2; ++j) {
                     const uint32_t bi = j ? ib : ia;
                     const int o = j ? 13 : 0;
-                    for (int c = 0; c < 3; ++c) L.p[j][c] = r[static_cast<size_t>(o + c) * rs];
-                    for (int c = 0; c < 4; ++c) L.q[j][c] = r[static_cast<size_t>(o + 3 + c) * rs];
-                    for (int c = 0; c < 3; ++c) L.v[j][c] = r[static_cast<size_t>(o + 7 + c) * rs];
-                    for (int c = 0; c < 3; ++c) L.w[j][c] = r[static_cast<size_t>(o + 10 + c) * rs];
+                    for (int c = 0; c < 3; ++c) L.p[j][c] = r[static_cast<size_t>(o + c) * rst];
+                    for (int c = 0; c < 4; ++c) L.q[j][c] = r[static_cast<size_t>(o + 3 + c) * rst];
+                    for (int c = 0; c < 3; ++c) L.v[j][c] = r[static_cast<size_t>(o + 7 + c) * rst];
+                    for (int c = 0; c < 3; ++c) L.w[j][c] = r[static_cast<size_t>(o + 10 + c) * rst];
                     L.m[j] = SB.im(bi);
                     L.I[j][0] = SB.ixx(bi); L.I[j][1] = SB.iyy(bi); L.I[j][2] = SB.izz(bi);
                     L.I[j][3] = SB.ixy(bi); L.I[j][4] = SB.ixz(bi); L.I[j][5] = SB.iyz(bi);
@@ -188,7 +203,7 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
                 }
                 F3 pb = f3(0.f, 0.f, 0.f), nb3 = pb;
                 float db = 0.f;
-                solve_contact_adj(L, ct, P_.mu, P_.dt, r[26ull * rs], __float_as_uint(r[35ull * rs]), G0, G1, pb,
+                solve_contact_adj(L, ct, P_.mu, P_.dt, r[26ull * rst], __float_as_uint(r[35ull * rst]), G0, G1, pb,
                                   nb3, db);
                 for (int j = 0; j < 2; ++j) {
                     if (L.m[j] == 0.f) continue;  // a static body's state is not a variable
@@ -203,10 +218,10 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
                     grow(G.gout, ns, 12, gi) = Gj.w.z;
                     G.gim[gi] += Gj.im;
                 }
-                float* w = A.rec + cbase + k;
-                w[28ull * rs] = pb.x; w[29ull * rs] = pb.y; w[30ull * rs] = pb.z;
-                w[31ull * rs] = nb3.x; w[32ull * rs] = nb3.y; w[33ull * rs] = nb3.z;
-                w[34ull * rs] = db;
+                float* w = recb + k;
+                w[28ull * rst] = pb.x; w[29ull * rst] = pb.y; w[30ull * rst] = pb.z;
+                w[31ull * rst] = nb3.x; w[32ull * rst] = nb3.y; w[33ull * rst] = nb3.z;
+                w[34ull * rst] = db;
             }
             T.sync();
         }
@@ -222,7 +237,7 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
         for (uint32_t i = T.rank(); i < nb; i += T.size()) R.cnt[i] = 0u;
         T.sync();
         for (uint32_t k = T.rank(); k < m; k += T.size()) {
-            if (A.rec[cbase + k + 35ull * rs] == 0.f) continue;
+            if (recb[k + 35ull * rst] == 0.f) continue;
             const uint32_t ab = SC.ab(k), a = ab & 0xFFFFu, b = ab >> 16;
             if (SB.im(a) != 0.f) atomicAdd(&R.cnt[a], 1u);
             if (SB.im(b) != 0.f) atomicAdd(&R.cnt[b], 1u);
@@ -244,7 +259,7 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
         if (T.leader()) R.off[nb] = sh.carry;
         T.sync();
         for (uint32_t k = T.rank(); k < m; k += T.size()) {
-            if (A.rec[cbase + k + 35ull * rs] == 0.f) continue;
+            if (recb[k + 35ull * rst] == 0.f) continue;
             const uint32_t ab = SC.ab(k), a = ab & 0xFFFFu, b = ab >> 16;
             if (SB.im(a) != 0.f) entry(R.off[a] + atomicAdd(&R.cnt[a], 1u)) = k;
             if (SB.im(b) != 0.f) entry(R.off[b] + atomicAdd(&R.cnt[b], 1u)) = k;
@@ -264,8 +279,8 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
         }
         // the contacts' geometry adjoints, into their records
         for (uint32_t k = T.rank(); k < m; k += T.size()) {
-            float* r = A.rec + cbase + k;
-            if (r[35ull * rs] == 0.f) continue;  // a contact that did not act has no effect
+            float* r = recb + k;
+            if (r[35ull * rst] == 0.f) continue;  // a contact that did not act has no effect
             const Contact ct = SC.contact(k);
             const uint32_t ia = ct.a, ib = ct.b;
             const uint32_t ga = b0 + ia, gbi = b0 + ib;
@@ -280,13 +295,13 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
             F3 xab = f3(0.f, 0.f, 0.f), xbb = xab;
             float qab[4] = {0.f, 0.f, 0.f, 0.f}, qbb[4] = {0.f, 0.f, 0.f, 0.f};
             process_pair_adj(info[ia] & 0xFFu, info[ib] & 0xFFu, xa, qa, ha, xb, qb, hb,
-                             __float_as_uint(r[27ull * rs]), f3(ct.nx, ct.ny, ct.nz),
-                             f3(r[28ull * rs], r[29ull * rs], r[30ull * rs]),
-                             f3(r[31ull * rs], r[32ull * rs], r[33ull * rs]), r[34ull * rs], xab, qab, xbb, qbb);
+                             __float_as_uint(r[27ull * rst]), f3(ct.nx, ct.ny, ct.nz),
+                             f3(r[28ull * rst], r[29ull * rst], r[30ull * rst]),
+                             f3(r[31ull * rst], r[32ull * rst], r[33ull * rst]), r[34ull * rst], xab, qab, xbb, qbb);
             const float out[14] = {xab.x, xab.y, xab.z, qab[0], qab[1], qab[2], qab[3],
                                    xbb.x, xbb.y, xbb.z, qbb[0], qbb[1], qbb[2], qbb[3]};
 #pragma unroll
-            for (int c = 0; c < 14; ++c) r[static_cast<size_t>(c) * rs] = out[c];
+            for (int c = 0; c < 14; ++c) r[static_cast<size_t>(c) * rst] = out[c];
         }
         T.sync();
         // every body's sum over its contacts, in contact order
@@ -300,9 +315,9 @@ __device__ void reverse_scene(const Team& T, uint32_t s, unsigned char* smem, ui
             for (uint32_t e = lo; e < hi; ++e) {
                 const uint32_t k = entry(e);
                 const uint32_t side = (SC.ab(k) & 0xFFFFu) == x ? 0u : 7u;
-                const float* r = A.rec + cbase + k;
+                const float* r = recb + k;
 #pragma unroll
-                for (int c = 0; c < 7; ++c) acc[c] += r[static_cast<size_t>(side + c) * rs];
+                for (int c = 0; c < 7; ++c) acc[c] += r[static_cast<size_t>(side + c) * rst];
             }
 #pragma unroll
             for (int c = 0; c < 7; ++c) grow(G.gout, ns, c, gx) = acc[c];
@@ -357,27 +372,6 @@ __device__ __forceinline__ void for_each_item(const uint32_t* items, uint32_t n_
         }
         __syncthreads();
     }
-}
-
-__global__ void __launch_bounds__(kSceneThreads, 4) scene_frame_record_kernel(SceneBufs S, FrameBufs F,
-                                                                              FrameParams P_, AdjRun A, AdjKeep K,
-                                                                              const uint32_t* __restrict__ items,
-                                                                              uint32_t n_items) {
-    for_each_item(items, n_items, S.smem_bytes,
-                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t bytes, SceneShared& sh) {
-                      record_scene(T, s, smem, bytes, sh, S, F, P_, A, K);
-                  });
-}
-
-__global__ void __launch_bounds__(kSceneThreads, 3) scene_frame_reverse_kernel(SceneBufs S, FrameBufs F,
-                                                                               FrameParams P_, AdjRun A, AdjKeep K,
-                                                                               AdjFrame G,
-                                                                               const uint32_t* __restrict__ items,
-                                                                               uint32_t n_items) {
-    for_each_item(items, n_items, S.smem_bytes,
-                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t bytes, SceneShared& sh) {
-                      reverse_scene(T, s, smem, bytes, sh, S, F, P_, A, K, G);
-                  });
 }
 
 }  // namespace

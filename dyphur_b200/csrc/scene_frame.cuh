@@ -21,6 +21,8 @@
 // (scene_gather_*).
 #pragma once
 
+#include "solver_scene.cuh"
+
 namespace dyph {
 namespace {
 

@@ -24,6 +24,8 @@
 // chain of dependent contacts is d long takes d waves.
 #pragma once
 
+#include "solver_common.cuh"
+
 namespace dyph {
 namespace {
 

@@ -80,6 +80,14 @@ struct dyph_world {
     uint32_t f_teams = 2;                 // 0 blocks only, 1 + small scenes one per warp, 2 + mid-size two warps
     uint32_t f_variant = 0;               // register budget: 4 (0), 5 (1) or 6 (2) blocks per SM
     uint32_t f_warp_scenes = 0, f_half_scenes = 0, f_block_scenes = 0;
+    // Work items of the adjoint's reverse kernel, laid out on their own: its
+    // levels are long dependent chains with a barrier each, which favours
+    // one-warp teams over the forward frame's choice.
+    uint32_t* r_items = nullptr;
+    uint32_t r_n_items = 0, r_smem = 0;
+    uint32_t r_smem_cap = 0;              // 0: what lets two blocks share an SM
+    uint32_t r_teams = 1;
+    uint32_t r_warp_scenes = 0, r_half_scenes = 0, r_block_scenes = 0;
     float f_tuned_ms = 0.f;
     uint32_t f_tuned_candidates = 0;
 };
@@ -88,6 +96,18 @@ namespace dyph {
 namespace {
 
 constexpr uint32_t kHistory = 4096;
+
+// Frame f's recomputation with recording for the adjoint (record_scene), on
+// the fused kernel's work items.
+__global__ void __launch_bounds__(kSceneThreads, 4) scene_frame_record_kernel(SceneBufs S, FrameBufs F,
+                                                                              FrameParams P_, AdjRun A, AdjKeep K,
+                                                                              const uint32_t* __restrict__ items,
+                                                                              uint32_t n_items) {
+    for_each_item(items, n_items, S.smem_bytes,
+                  [&](const auto& T, uint32_t s, unsigned char* smem, uint32_t bytes, SceneShared& sh) {
+                      record_scene(T, s, smem, bytes, sh, S, F, P_, A, K);
+                  });
+}
 constexpr size_t kStatsWords = 8 + 2 * kHistory;
 
 __global__ void frame_stats_kernel(const uint32_t* __restrict__ bp_counts, const uint32_t* __restrict__ np_counts,
@@ -240,7 +260,7 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     }
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                  w->f_words, w->f_pos, w->f_items, w->f_phase, w->a_g[0], w->a_g[1], w->a_seg[0], w->a_seg[1],
+                  w->f_words, w->f_pos, w->f_items, w->r_items, w->f_phase, w->a_g[0], w->a_g[1], w->a_seg[0], w->a_seg[1],
                   w->a_flag, w->a_pairs};
     for (void* p : fb)
         if (p) cudaFree(p);
@@ -478,6 +498,112 @@ uint32_t fused_smem_need(uint32_t max_nb) {
 }
 uint32_t fused_smem_floor(uint32_t max_nb) { return frame_body_bytes(max_nb) + 56u * 64u; }
 
+// Work items, largest scenes first: a scene whose estimated shared-memory
+// need fits a quarter of the block's (`share`) runs on one warp, four such
+// scenes to a block (teams >= 1); one that fits half of it on two warps, two
+// to a block (teams == 2); larger scenes take the whole block.
+template <class Est>
+void build_items(const uint32_t* body_offset, uint32_t n_scenes, uint32_t share, uint32_t teams, Est est,
+                 std::vector<uint32_t>& items, uint32_t& n_small, uint32_t& n_mid) {
+    std::vector<uint32_t> order(n_scenes);
+    for (uint32_t i = 0; i < n_scenes; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [body_offset](uint32_t x, uint32_t y) {
+        return body_offset[x + 1] - body_offset[x] > body_offset[y + 1] - body_offset[y];
+    });
+    items.clear();
+    std::vector<uint32_t> small, mid;
+    for (uint32_t s : order) {
+        const uint32_t e = est(body_offset[s + 1] - body_offset[s]);
+        if (teams >= 1 && e <= share) {
+            small.push_back(s);
+        } else if (teams >= 2 && e <= 2u * share) {
+            mid.push_back(s);
+        } else {
+            items.insert(items.end(), {s, kItemBlock, kItemEmpty, kItemEmpty});
+        }
+    }
+    for (size_t i = 0; i < mid.size(); i += 2)
+        items.insert(items.end(), {mid[i], kItemHalf, i + 1 < mid.size() ? mid[i + 1] : kItemEmpty, kItemHalf});
+    for (size_t i = 0; i < small.size(); i += 4)
+        for (size_t j = 0; j < 4; ++j) items.push_back(i + j < small.size() ? small[i + j] : kItemEmpty);
+    n_small = static_cast<uint32_t>(small.size());
+    n_mid = static_cast<uint32_t>(mid.size());
+}
+
+// The fused kernels may take up to kMaxSmem of dynamic shared memory, set
+// once per device: the attribute belongs to the kernel, not to a world, so a
+// world that lowered it would make another world's launches fail.
+constexpr int kFusedMaxDevices = 64;
+std::mutex g_fused_smem_mu;
+bool g_fused_smem[kFusedMaxDevices] = {};
+
+dyph_status fused_smem_prepare() {
+    int dev = 0;
+    DYPH_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kFusedMaxDevices) return DYPH_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_fused_smem_mu);
+    if (g_fused_smem[dev]) return DYPH_OK;
+    for (const void* k : {reinterpret_cast<const void*>(scene_frame_kernel<4>),
+                          reinterpret_cast<const void*>(scene_frame_kernel<5>),
+                          reinterpret_cast<const void*>(scene_frame_kernel<6>),
+                          reinterpret_cast<const void*>(scene_frame_record_kernel),
+                          reverse_kernel()})
+        DYPH_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem)));
+    g_fused_smem[dev] = true;
+    return DYPH_OK;
+}
+
+// Dynamic shared memory per block with which `blocks` blocks of `kernel`
+// share an SM, as the occupancy calculator counts it (static shared memory
+// and the per-block reservation included): the SM's share for one block,
+// lowered in 128-byte steps until that many blocks fit.
+uint32_t smem_for_blocks(const void* kernel, int blocks) {
+    int dev = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0u;
+    }
+    uint32_t bytes = std::min(kMaxSmem, static_cast<uint32_t>(per_sm / blocks)) & ~127u;
+    for (; bytes >= 128u; bytes -= 128u) {
+        int fit = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kernel, kSceneThreads, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return 0u;
+        }
+        if (fit >= blocks) return bytes;
+    }
+    return 0u;
+}
+
+// The reverse kernel's items and shared memory: per scene its bodies' rows
+// plus the contact words and records of about 2.5 contacts per body (a scene
+// with more reads them from global memory).
+dyph_status setup_reverse(dyph_world* w) {
+    const uint32_t n_scenes = static_cast<uint32_t>(w->h_body_offset.size() - 1);
+    const uint32_t* off = w->h_body_offset.data();
+    uint32_t max_nb = 0;
+    for (uint32_t i = 0; i < n_scenes; ++i) max_nb = std::max(max_nb, off[i + 1] - off[i]);
+    uint32_t smem = w->r_smem_cap ? std::min(kMaxSmem, w->r_smem_cap & ~15u)
+                                  : smem_for_blocks(reverse_kernel(), 2);
+    smem = std::max(smem, frame_body_bytes(max_nb) + kSceneWords * 4u * 64u);
+    if (smem > kMaxSmem) return DYPH_ERR_TOO_LARGE;
+    std::vector<uint32_t> items;
+    uint32_t n_small = 0, n_mid = 0;
+    build_items(off, n_scenes, (smem / 4u) & ~15u, w->r_teams,
+                [](uint32_t nb) { return frame_body_bytes(nb) + (kSceneWords + kRecWords) * 10u * nb; }, items, n_small, n_mid);
+    if (w->r_items) cudaFree(w->r_items);
+    w->r_items = nullptr;
+    if (cudaMalloc(&w->r_items, items.size() * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
+    DYPH_CUDA_TRY(cudaMemcpy(w->r_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice));
+    w->r_n_items = static_cast<uint32_t>(items.size() / 4);
+    w->r_smem = smem;
+    w->r_warp_scenes = n_small;
+    w->r_half_scenes = n_mid;
+    w->r_block_scenes = n_scenes - n_small - n_mid;
+    return DYPH_OK;
+}
+
 dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_offset) {
     w->fused = false;
     w->h_body_offset.assign(body_offset, body_offset + n_scenes + 1);
@@ -490,16 +616,23 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
         cb[i + 1] = cb[i] + std::max(64u, 16u * nb + 64u);
     }
     if (fused_smem_floor(max_nb) > kMaxSmem) return DYPH_ERR_TOO_LARGE;
+    dyph_status prep = fused_smem_prepare();
+    if (prep != DYPH_OK) return prep;
     uint32_t smem = fused_smem_need(max_nb);
-    if (w->f_smem_cap) smem = std::max(fused_smem_floor(max_nb), std::min(smem, w->f_smem_cap & ~15u));
-    for (const void* k : {reinterpret_cast<const void*>(scene_frame_kernel<4>),
-                          reinterpret_cast<const void*>(scene_frame_kernel<5>),
-                          reinterpret_cast<const void*>(scene_frame_kernel<6>)})
-        DYPH_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_record_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem)));
-    DYPH_CUDA_TRY(cudaFuncSetAttribute(scene_frame_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem)));
+    const void* variant = w->f_variant == 1   ? reinterpret_cast<const void*>(scene_frame_kernel<5>)
+                          : w->f_variant == 2 ? reinterpret_cast<const void*>(scene_frame_kernel<6>)
+                                              : reinterpret_cast<const void*>(scene_frame_kernel<4>);
+    if (w->f_smem_cap) {
+        smem = std::max(fused_smem_floor(max_nb), std::min(smem, w->f_smem_cap & ~15u));
+    } else {
+        // With more scenes than SMs, a block that leaves room for a second one
+        // on its SM beats one that holds the largest scene whole.
+        int dev = 0, sms = 0;
+        DYPH_CUDA_TRY(cudaGetDevice(&dev));
+        DYPH_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const uint32_t two = smem_for_blocks(variant, 2);
+        if (n_scenes > static_cast<uint32_t>(sms) && smem > two && two >= fused_smem_floor(max_nb)) smem = two;
+    }
     uint32_t** bufs[] = {&w->f_pair_base, &w->f_contact_base, &w->f_pair_raw, &w->f_contact_raw, &w->f_color_raw,
                          &w->f_counts, &w->f_words, &w->f_pos};
     for (uint32_t** b : bufs) {
@@ -516,34 +649,12 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
                             static_cast<size_t>(kSceneWords) * w->f_words_stride, 2ull * n_scenes};
     for (int k = 0; k < 8; ++k)
         if (cudaMalloc(bufs[k], sizes[k] * sizeof(uint32_t)) != cudaSuccess) return DYPH_ERR_NOMEM;
-    // Work items, largest scenes first: a scene whose frame is expected to fit
-    // a quarter of the block's shared memory (about 4 pairs and 2.5 contacts
-    // per body) runs on one warp, four such scenes to a block; one that fits
-    // half of it on two warps, two to a block; larger scenes take the whole
-    // block.
-    std::vector<uint32_t> order(n_scenes);
-    for (uint32_t i = 0; i < n_scenes; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [body_offset](uint32_t x, uint32_t y) {
-        return body_offset[x + 1] - body_offset[x] > body_offset[y + 1] - body_offset[y];
-    });
-    const uint32_t share = (smem / 4u) & ~15u;
+    // Work items: a scene's frame is expected to need its bodies' rows plus
+    // about 4 pairs and 2.5 contacts per body.
     std::vector<uint32_t> items;
-    std::vector<uint32_t> small, mid;
-    for (uint32_t s : order) {
-        const uint32_t nb = body_offset[s + 1] - body_offset[s];
-        const uint32_t est = frame_body_bytes(nb) + 146u * nb;
-        if (w->f_teams >= 1 && est <= share) {
-            small.push_back(s);
-        } else if (w->f_teams >= 2 && est <= 2u * share) {
-            mid.push_back(s);
-        } else {
-            items.insert(items.end(), {s, kItemBlock, kItemEmpty, kItemEmpty});
-        }
-    }
-    for (size_t i = 0; i < mid.size(); i += 2)
-        items.insert(items.end(), {mid[i], kItemHalf, i + 1 < mid.size() ? mid[i + 1] : kItemEmpty, kItemHalf});
-    for (size_t i = 0; i < small.size(); i += 4)
-        for (size_t j = 0; j < 4; ++j) items.push_back(i + j < small.size() ? small[i + j] : kItemEmpty);
+    uint32_t n_small = 0, n_mid = 0;
+    build_items(body_offset, n_scenes, (smem / 4u) & ~15u, w->f_teams,
+                [](uint32_t nb) { return frame_body_bytes(nb) + 146u * nb; }, items, n_small, n_mid);
     w->f_n_items = static_cast<uint32_t>(items.size() / 4);
     if (cudaMalloc(&w->f_items, items.size() * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
     DYPH_CUDA_TRY(cudaMemcpy(w->f_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice));
@@ -551,9 +662,11 @@ dyph_status setup_fused(dyph_world* w, uint32_t n_scenes, const uint32_t* body_o
     DYPH_CUDA_TRY(cudaMemcpy(w->f_contact_base, cb.data(), cb.size() * 4, cudaMemcpyHostToDevice));
     DYPH_CUDA_TRY(cudaMemset(w->f_counts, 0, 4ull * n_scenes * sizeof(uint32_t)));
     w->frame_smem = smem;
-    w->f_warp_scenes = static_cast<uint32_t>(small.size());
-    w->f_half_scenes = static_cast<uint32_t>(mid.size());
-    w->f_block_scenes = n_scenes - w->f_warp_scenes - w->f_half_scenes;
+    w->f_warp_scenes = n_small;
+    w->f_half_scenes = n_mid;
+    w->f_block_scenes = n_scenes - n_small - n_mid;
+    dyph_status st = setup_reverse(w);
+    if (st != DYPH_OK) return st;
     w->fused = true;
     return DYPH_OK;
 }
@@ -652,6 +765,31 @@ extern "C" dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_
     dyph_status st = setup_fused(w, static_cast<uint32_t>(off.size() - 1), off.data());
     drop_graphs(w);
     return st;
+}
+
+extern "C" dyph_status dyph_world_adjoint_config(dyph_world* w, dyph_fused_config* out) {
+    if (!w || !out) return DYPH_ERR_INVALID;
+    *out = dyph_fused_config{};
+    if (!w->fused) return DYPH_OK;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reverse_kernel(), kSceneThreads, w->r_smem);
+    out->smem_bytes = w->r_smem;
+    out->teams = w->r_teams;
+    out->warp_scenes = w->r_warp_scenes;
+    out->half_scenes = w->r_half_scenes;
+    out->block_scenes = w->r_block_scenes;
+    out->blocks = w->r_n_items;
+    out->blocks_per_sm = static_cast<uint32_t>(per_sm);
+    out->register_blocks = 3u;
+    return DYPH_OK;
+}
+
+extern "C" dyph_status dyph_world_set_adjoint_config(dyph_world* w, uint32_t smem_bytes, uint32_t teams) {
+    if (!w || !w->fused || teams > 2u) return DYPH_ERR_INVALID;
+    DYPH_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    w->r_smem_cap = smem_bytes;
+    w->r_teams = teams;
+    return setup_reverse(w);
 }
 
 extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out) {
@@ -1000,6 +1138,8 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     const float sub_dt = ip.dt / static_cast<float>(ip.n_substeps);
     SceneBufs S{w->bp->body_offset, w->bp->bvh.scene_of, w->sv->scene_order, nullptr, nullptr, 0, w->bp->n_scenes,
                 w->frame_smem};
+    SceneBufs S_rev = S;
+    S_rev.smem_bytes = w->r_smem;
     // Three streams: the next checkpoint segment is re-stepped on a_stream,
     // frame f - 1 is recorded on a_rstream while frame f is reversed on the
     // caller's stream. Per-frame buffers alternate with the frame's parity; the
@@ -1071,9 +1211,12 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
         }
         DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_rec_done[f & 1], 0));
         AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
-        scene_frame_reverse_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, cs>>>(
-            S, frame_bufs(f), params(f), adj(f), keep(f), G, w->f_items, w->f_n_items);
-        DYPH_CUDA_TRY(cudaGetLastError());
+        FrameBufs fb = frame_bufs(f);
+        FrameParams pf = params(f);
+        AdjRun af = adj(f);
+        AdjKeep kf = keep(f);
+        void* args[] = {&S_rev, &fb, &pf, &af, &kf, &G, &w->r_items, &w->r_n_items};
+        DYPH_CUDA_TRY(cudaLaunchKernel(reverse_kernel(), dim3(w->r_n_items), dim3(kSceneThreads), args, w->r_smem, cs));
         DYPH_CUDA_TRY(cudaEventRecord(w->a_rev_done[f & 1], cs));
         cur ^= 1;
     }

@@ -548,6 +548,17 @@ class World:
         check(capi.lib().dyph_world_set_fused_config(self.h, int(smem_cap), int(teams), int(register_blocks)),
               "dyph_world_set_fused_config")
 
+    def adjoint_config(self) -> dict:
+        """Layout of the adjoint's reverse kernel (dyph_world_adjoint_config)."""
+        c = capi.FusedConfig()
+        check(capi.lib().dyph_world_adjoint_config(self.h, C.byref(c)), "dyph_world_adjoint_config")
+        return {k: getattr(c, k) for k, _ in capi.FusedConfig._fields_}
+
+    def set_adjoint_config(self, smem_bytes: int = 0, teams: int = 1) -> None:
+        """smem_bytes 0: what lets two reverse blocks share an SM; teams as set_fused_config."""
+        check(capi.lib().dyph_world_set_adjoint_config(self.h, int(smem_bytes), int(teams)),
+              "dyph_world_set_adjoint_config")
+
     def autotune(self, frames: int = 16, stream=None) -> dict:
         """Time the fused kernel's configurations from the current state and keep
         the fastest (dyph_world_autotune); returns the chosen configuration."""

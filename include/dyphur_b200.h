@@ -399,7 +399,8 @@ dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
  * many blocks fit an SM:
  *   smem_bytes     dynamic shared memory per block: what the largest scene
  *                  needs, or less (smem_cap), down to its bodies plus 64
- *                  contacts' words;
+ *                  contacts' words; with no cap and more scenes than SMs, at
+ *                  most what lets two blocks share an SM;
  *   teams          0: every scene takes a block; 1: scenes whose frame fits
  *                  a quarter of that run one per warp, four to a block; 2: also
  *                  scenes that fit half of it on two warps, two to a block;
@@ -428,6 +429,17 @@ typedef struct dyph_fused_config {
 dyph_status dyph_world_fused_config(dyph_world* w, dyph_fused_config* out);
 dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, uint32_t teams, uint32_t register_blocks);
 dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out);
+/* The reverse kernel of dyph_world_rollout_backward lays out its own work
+ * items (same results bit for bit, whatever the setting): smem_bytes of
+ * dynamic shared memory per block (0: what lets two blocks share an SM; at
+ * least the largest scene's bodies plus 64 contacts' words, at most 200 KB)
+ * and the same team policies, a scene's need being its bodies plus the words
+ * and records of about 2.5 contacts per body (default teams 1). Its levels are dependent chains
+ * with a barrier each, so one-warp teams pay off there for scenes that the
+ * forward frame runs faster on whole blocks. dyph_world_adjoint_config reports
+ * it in a dyph_fused_config (register_blocks 3, ms_per_frame and candidates 0). */
+dyph_status dyph_world_adjoint_config(dyph_world* w, dyph_fused_config* out);
+dyph_status dyph_world_set_adjoint_config(dyph_world* w, uint32_t smem_bytes, uint32_t teams);
 /* Phase timing of fused batched frames, the per-stage table of the
  * reference's --profile mode (examples/stress_test_blocks/main.cpp:199-254)
  * for a frame that is one kernel: with it on, every scene's team leader adds

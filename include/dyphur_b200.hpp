@@ -560,6 +560,15 @@ public:
         check(dyph_world_autotune(h_, frames, s.abi(), &c), "World::autotune");
         return c;
     }
+    // The adjoint's reverse kernel layout (dyph_world_set_adjoint_config).
+    dyph_fused_config adjoint_config() {
+        dyph_fused_config c{};
+        check(dyph_world_adjoint_config(h_, &c), "World::adjoint_config");
+        return c;
+    }
+    void set_adjoint_config(uint32_t smem_bytes, uint32_t teams = 1) {
+        check(dyph_world_set_adjoint_config(h_, smem_bytes, teams), "World::set_adjoint_config");
+    }
     // State rows at creation ([13][capacity], device), the start of rollouts.
     const float* initial_rows() const noexcept { return initial_.data(); }
     BodyStore& bodies() noexcept { return *bodies_; }

@@ -137,3 +137,35 @@ def test_checkpoint_spacing_does_not_change_the_gradient(dev):
         out.append(np.concatenate([vel.grad.cpu().numpy().ravel(), im.grad.cpu().numpy()]))
     for o in out[1:]:
         assert np.allclose(o, out[0], rtol=1e-5, atol=1e-6 * np.abs(out[0]).max())
+
+
+def test_reverse_layout_does_not_change_the_gradient(dev):
+    """The reverse kernel's work items and shared memory
+    (dyph_world_set_adjoint_config) move only where a scene's adjoint runs and
+    where its contact words live: the gradients are the same bit for bit."""
+    import torch
+    from dyphur_b200.autograd import rollout
+    s = scenes.batch_mixed(40, 16, 512, seed=5)
+    n = s.n_bodies
+    dyn = torch.from_numpy((s.mass > 0).astype(np.float32)).cuda()
+    out, layouts = [], set()
+    for smem, teams in ((0, 1), (0, 0), (0, 2), (1, 0), (1, 1), (200 << 10, 1), (64 << 10, 2)):
+        w = dev.World(s, mode=1)
+        w.set_adjoint_config(smem, teams)
+        cfg = w.adjoint_config()
+        assert cfg["warp_scenes"] + cfg["half_scenes"] + cfg["block_scenes"] == s.n_scenes
+        assert cfg["teams"] == teams and cfg["blocks_per_sm"] >= 1
+        layouts.add((cfg["smem_bytes"], cfg["warp_scenes"], cfg["half_scenes"]))
+        vel = w.initial[7:10, :n].T.clone().requires_grad_(True)
+        ang = w.initial[10:13, :n].T.clone().requires_grad_(True)
+        im = w.bodies.fbuf[13, :n].clone().requires_grad_(True)
+        fin = rollout(w, vel, ang, im, 12, every=4)
+        ((fin[:3].T ** 2).sum(1) * dyn).sum().backward()
+        torch.cuda.synchronize()
+        out.append([t.grad.cpu().numpy() for t in (vel, ang, im)])
+        assert dev.device_error() == 0
+    assert len(layouts) >= 5
+    assert np.abs(out[0][0]).sum() > 0
+    for o in out[1:]:
+        for a, b in zip(o, out[0]):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))

@@ -60,3 +60,20 @@ def test_autotune_keeps_state_and_caches(dev):
     again = dev.World(s, mode=capi.SOLVER_SEQUENTIAL).autotune(8)
     assert again["candidates"] == 0 and again["smem_bytes"] == cfg["smem_bytes"]
     assert dev.device_error() == 0
+
+
+def test_worlds_with_different_shared_memory_step_side_by_side(dev):
+    """The fused kernels' shared-memory limit is the kernel's, not the world's:
+    a world set up with less shared memory after another does not make the
+    other's launches fail."""
+    s = scenes.batch(160, 8, 256, seed=13)
+    big = dev.World(s, mode=capi.SOLVER_SEQUENTIAL)
+    big.step(3)
+    small = dev.World(s, mode=capi.SOLVER_SEQUENTIAL)
+    small.set_fused_config(1, 0, 4)  # the floor: bodies plus 64 contacts' words
+    assert small.fused_config()["smem_bytes"] < big.fused_config()["smem_bytes"]
+    small.step(3)
+    big.step(12)
+    small.step(12)
+    assert np.array_equal(bits(big.state()), bits(small.state()))
+    assert dev.device_error() == 0
