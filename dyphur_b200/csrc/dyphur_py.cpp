@@ -295,7 +295,7 @@ PYBIND11_MODULE(dyphur_py, m) {
         .def("set_fused_config", &World::set_fused_config, "smem_cap"_a, "teams"_a = 2, "register_blocks"_a = 0)
         .def("autotune", &World::autotune, "s"_a, "frames"_a = 16)
         .def("adjoint_config", &World::adjoint_config)
-        .def("set_adjoint_config", &World::set_adjoint_config, "smem_bytes"_a = 0, "teams"_a = 1)
+        .def("set_adjoint_config", &World::set_adjoint_config, "smem_bytes"_a = 0, "teams"_a = 2)
         .def("hash", [](World& w, Stream& s) { return state_hash(s, w.bodies().view()); })
         .def("scene_hashes", &World::scene_hashes, "s"_a, "n_scenes"_a)
         .def("count", [](World& w) { return w.bodies().count(); })

@@ -85,8 +85,8 @@ struct dyph_world {
     // one-warp teams over the forward frame's choice.
     uint32_t* r_items = nullptr;
     uint32_t r_n_items = 0, r_smem = 0;
-    uint32_t r_smem_cap = 0;              // 0: what lets two blocks share an SM
-    uint32_t r_teams = 1;
+    uint32_t r_smem_cap = 0;              // 0: a third of an SM's shared memory
+    uint32_t r_teams = 2;
     uint32_t r_warp_scenes = 0, r_half_scenes = 0, r_block_scenes = 0;
     float f_tuned_ms = 0.f;
     uint32_t f_tuned_candidates = 0;
@@ -576,6 +576,23 @@ uint32_t smem_for_blocks(const void* kernel, int blocks) {
     return 0u;
 }
 
+// Dynamic shared memory per block when `blocks` blocks of `kernel` split an
+// SM's shared memory (its static shared memory and the per-block reservation
+// counted), whatever its registers allow.
+uint32_t smem_share(const void* kernel, uint32_t blocks) {
+    int dev = 0, per_sm = 0, reserved = 0;
+    cudaFuncAttributes fa{};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) {
+        cudaGetLastError();
+        return 0u;
+    }
+    const int64_t bytes = static_cast<int64_t>(per_sm) / blocks - reserved - static_cast<int64_t>(fa.sharedSizeBytes);
+    return bytes > 0 ? std::min(kMaxSmem, static_cast<uint32_t>(bytes) & ~127u) : 0u;
+}
+
 // The reverse kernel's items and shared memory: per scene its bodies' rows
 // plus the contact words and records of about 2.5 contacts per body (a scene
 // with more reads them from global memory).
@@ -584,8 +601,10 @@ dyph_status setup_reverse(dyph_world* w) {
     const uint32_t* off = w->h_body_offset.data();
     uint32_t max_nb = 0;
     for (uint32_t i = 0; i < n_scenes; ++i) max_nb = std::max(max_nb, off[i + 1] - off[i]);
-    uint32_t smem = w->r_smem_cap ? std::min(kMaxSmem, w->r_smem_cap & ~15u)
-                                  : smem_for_blocks(reverse_kernel(), 2);
+    // Default: a third of an SM's shared memory. The kernel's registers allow
+    // two blocks per SM; the smaller blocks leave shared memory to the
+    // recording and re-stepping kernels that run beside it.
+    uint32_t smem = w->r_smem_cap ? std::min(kMaxSmem, w->r_smem_cap & ~15u) : smem_share(reverse_kernel(), 3u);
     smem = std::max(smem, frame_body_bytes(max_nb) + kSceneWords * 4u * 64u);
     if (smem > kMaxSmem) return DYPH_ERR_TOO_LARGE;
     std::vector<uint32_t> items;
@@ -780,7 +799,7 @@ extern "C" dyph_status dyph_world_adjoint_config(dyph_world* w, dyph_fused_confi
     out->block_scenes = w->r_block_scenes;
     out->blocks = w->r_n_items;
     out->blocks_per_sm = static_cast<uint32_t>(per_sm);
-    out->register_blocks = 3u;
+    out->register_blocks = 2u;
     return DYPH_OK;
 }
 

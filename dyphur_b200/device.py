@@ -554,8 +554,8 @@ class World:
         check(capi.lib().dyph_world_adjoint_config(self.h, C.byref(c)), "dyph_world_adjoint_config")
         return {k: getattr(c, k) for k, _ in capi.FusedConfig._fields_}
 
-    def set_adjoint_config(self, smem_bytes: int = 0, teams: int = 1) -> None:
-        """smem_bytes 0: what lets two reverse blocks share an SM; teams as set_fused_config."""
+    def set_adjoint_config(self, smem_bytes: int = 0, teams: int = 2) -> None:
+        """smem_bytes 0: a third of an SM's shared memory; teams as set_fused_config."""
         check(capi.lib().dyph_world_set_adjoint_config(self.h, int(smem_bytes), int(teams)),
               "dyph_world_set_adjoint_config")
 

@@ -431,13 +431,14 @@ dyph_status dyph_world_set_fused_config(dyph_world* w, uint32_t smem_cap, uint32
 dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_stream s, dyph_fused_config* out);
 /* The reverse kernel of dyph_world_rollout_backward lays out its own work
  * items (same results bit for bit, whatever the setting): smem_bytes of
- * dynamic shared memory per block (0: what lets two blocks share an SM; at
- * least the largest scene's bodies plus 64 contacts' words, at most 200 KB)
+ * dynamic shared memory per block (0: a third of an SM's; at least the
+ * largest scene's bodies plus 64 contacts' words, at most 200 KB)
  * and the same team policies, a scene's need being its bodies plus the words
- * and records of about 2.5 contacts per body (default teams 1). Its levels are dependent chains
- * with a barrier each, so one-warp teams pay off there for scenes that the
- * forward frame runs faster on whole blocks. dyph_world_adjoint_config reports
- * it in a dyph_fused_config (register_blocks 3, ms_per_frame and candidates 0). */
+ * and records of about 2.5 contacts per body (default teams 2). The kernel
+ * takes 240 registers a thread, two blocks per SM; its levels are dependent
+ * chains with a barrier each, so teams smaller than a block leave fewer warps
+ * waiting. dyph_world_adjoint_config reports it in a dyph_fused_config
+ * (register_blocks 2, ms_per_frame and candidates 0). */
 dyph_status dyph_world_adjoint_config(dyph_world* w, dyph_fused_config* out);
 dyph_status dyph_world_set_adjoint_config(dyph_world* w, uint32_t smem_bytes, uint32_t teams);
 /* Phase timing of fused batched frames, the per-stage table of the

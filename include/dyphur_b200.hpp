@@ -566,7 +566,7 @@ public:
         check(dyph_world_adjoint_config(h_, &c), "World::adjoint_config");
         return c;
     }
-    void set_adjoint_config(uint32_t smem_bytes, uint32_t teams = 1) {
+    void set_adjoint_config(uint32_t smem_bytes, uint32_t teams = 2) {
         check(dyph_world_set_adjoint_config(h_, smem_bytes, teams), "World::set_adjoint_config");
     }
     // State rows at creation ([13][capacity], device), the start of rollouts.
