@@ -5,7 +5,7 @@ stress_test_blocks example (examples/stress_test_blocks/main.cpp).
                               [--spacing S] [--jitter J] [--profile]
                               [--workload blocks|pile|batch] [--mode M]
                               [--start-frame F] [--smem-cap B] [--teams T]
-                              [--autotune FRAMES]
+                              [--autotune FRAMES] [--adjoint EVERY]
 
 Writes <prefix>.scene, <prefix>.trajectory (poses every other frame),
 <prefix>.metrics.json and <prefix>.golden exactly as the example does. The
@@ -18,6 +18,12 @@ recorded inside the captured frames instead of host fences.
 --start-frame F steps F frames untimed and writes nothing before the run:
 with `ncu -k regex:<kernel> -s F -c 1` it captures frame F's launch of a
 kernel that runs once per frame.
+--adjoint EVERY runs one differentiable rollout of n_frames (checkpoints every
+EVERY frames) and its backward pass instead, loss = squared distance of the
+boxes to the scenes' targets (the push workload), and prints both times; the
+backward pass runs one record and one reverse launch per frame, last frame
+first, so `ncu -k regex:scene_frame_reverse -s F -c 1` captures frame
+n_frames - 1 - F's reverse launch.
 """
 from __future__ import annotations
 
@@ -36,9 +42,11 @@ def parse(argv=None):
     ap.add_argument("--spacing", type=float, default=1.0)
     ap.add_argument("--jitter", type=float, default=0.0)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--workload", default="blocks", choices=["blocks", "pile", "batch"])
+    ap.add_argument("--workload", default="blocks", choices=["blocks", "pile", "batch", "push"])
     ap.add_argument("--bodies", type=int, default=65536, help="pile: dynamic bodies")
-    ap.add_argument("--scenes", type=int, default=4096, help="batch: scenes")
+    ap.add_argument("--scenes", type=int, default=4096, help="batch, push: scenes")
+    ap.add_argument("--adjoint", type=int, default=0, metavar="EVERY",
+                    help="one rollout of n_frames and its backward pass, checkpoints every EVERY frames")
     ap.add_argument("--mode", default="reference", choices=["reference", "sequential", "colored"])
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--start-frame", type=int, default=0)
@@ -62,6 +70,8 @@ def build_scene(args):
         return scenes.random_pile(args.bodies, seed=args.seed)
     if args.workload == "batch":
         return scenes.batch(args.scenes, 8, 256, seed=args.seed)
+    if args.workload == "push":
+        return scenes.push(args.scenes, seed=args.seed)
     nx, ny, nz = args.grid
     return scenes.stress_blocks(spacing=args.spacing, jitter=args.jitter, seed=args.seed, grid=(nx, ny, nz))
 
@@ -133,6 +143,33 @@ def cast_rays(world, scene, n_rays: int, seed: int = 9) -> None:
     print(f"rays: {n_rays} cast, {hits} hit, {ms:.3f} ms ({n_rays / ms / 1e3:.1f} M rays/s)")
 
 
+def adjoint_run(world, scene, frames: int, every: int) -> None:
+    """One differentiable rollout (sequential order) and its backward pass:
+    loss = sum over the dynamic bodies of |x_final - target|^2 (targets of the
+    push workload; the origin otherwise). Prints the forward and backward
+    milliseconds and the gradient norm."""
+    import torch
+    from .autograd import rollout
+    n = scene.n_bodies
+    target = getattr(scene, "targets", None)
+    tgt = torch.zeros((n, 3), device="cuda") if target is None else torch.from_numpy(target).cuda()
+    dyn = torch.from_numpy((scene.mass > 0).astype(np.float32)).cuda()
+    vel = world.initial[7:10, :n].T.clone().requires_grad_(True)
+    ang = world.initial[10:13, :n].T.clone().requires_grad_(True)
+    im = world.bodies.fbuf[13, :n].clone().requires_grad_(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    final = rollout(world, vel, ang, im, frames, every=every)
+    ev[1].record()
+    ((((final[:3].T - tgt) ** 2).sum(1)) * dyn).sum().backward()
+    ev[2].record()
+    torch.cuda.synchronize()
+    g = float(torch.linalg.vector_norm(torch.cat([vel.grad.ravel(), ang.grad.ravel(), im.grad.ravel()])))
+    print(f"adjoint: {frames} frames, checkpoints every {every}: forward {ev[0].elapsed_time(ev[1]):.3f} ms, "
+          f"backward {ev[1].elapsed_time(ev[2]):.3f} ms, |gradient| {g:.6g}; reverse kernel layout "
+          f"{world.adjoint_config()}")
+
+
 def main(argv=None) -> int:
     import torch
 
@@ -153,6 +190,12 @@ def main(argv=None) -> int:
         world.bodies.fbuf.copy_(init)
         torch.cuda.synchronize()
         print(f"fused frame configuration: {cfg}")
+    if args.adjoint:
+        if mode != capi.SOLVER_SEQUENTIAL:
+            print("--adjoint needs --mode sequential", file=sys.stderr)
+            return 2
+        adjoint_run(world, scene, args.n_frames, args.adjoint)
+        return 0
     if args.start_frame:
         world.step(args.start_frame)
         world.step(args.n_frames)
