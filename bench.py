@@ -665,9 +665,14 @@ def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask,
         _, _, gv10, ga10, gm10 = once(10)
         err_10 = _dual_error(w, scene, 0, 10, gv10.cpu().numpy(), ga10.cpu().numpy(), gm10.cpu().numpy(), False,
                              loss_mask, scale)
+    # checkpoints, the states of two segments, one record set per frame of two
+    # segments (36 record and 13 word rows per contact slot, 11 rows per
+    # body), the two adjoint states
     n_ckpt = (frames + every - 1) // every
+    seg = min(every if every > 1 else 4, frames)
+    states = 2 * (seg - 1) * 13 * n if every > 1 else 0
     slots = int(sum(max(64, 16 * int(b) + 64) for b in np.diff(scene.body_offset)))
-    act = 4 * (n_ckpt * 13 * n + every * 13 * n + 36 * slots + (7 + 4 + 26) * n)
+    act = 4 * (n_ckpt * 13 * n + states + 2 * seg * ((36 + 13) * slots + 11 * n) + 2 * 13 * n)
     w.close()
     return {"workload": label, "scenes": scene.n_scenes, "bodies": n, "frames": frames,
             "checkpoint_every": every, "solver_mode": "sequential",

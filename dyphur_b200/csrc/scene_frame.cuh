@@ -113,7 +113,8 @@ __device__ __forceinline__ void phase_mark(const Team& T, const FrameParams& P_,
 
 // Recording for the adjoint pass (frame_scene with `adj`): the frame is
 // recomputed from the given state, its branches and intermediates recorded,
-// and nothing is written back or reported.
+// and nothing is reported; the end state goes to `store` when it is set (the
+// given state is left as it was).
 struct AdjRun {
     float* rec;          // [kRecWords][rec_stride] per-contact records, slot = contact slot of the scene
     uint32_t rec_stride;
@@ -121,6 +122,7 @@ struct AdjRun {
     float* qs;           // [4][n_stride] quaternions after the sweeps, before the renormalisations
     uint32_t n_stride;
     uint32_t* flag;      // unsupported paths
+    float* store;        // [13][n_stride] the frame's end state (x, q, v, w), or null
 };
 
 // What the adjoint pass needs of a recomputed frame.
@@ -340,7 +342,16 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
     }
     if (out) *out = FrameOut{SC, m, groups};
     phase_mark(T, P_, 4, t0);
-    if (!adj) scene_store_bodies(T, B, b0, nb, SB);
+    if (!adj) {
+        scene_store_bodies(T, B, b0, nb, SB);
+    } else if (adj->store) {
+        for (uint32_t i = T.rank(); i < nb; i += T.size()) {
+            const float v[13] = {SB.px(i), SB.py(i), SB.pz(i), SB.qw(i), SB.qx(i), SB.qy(i), SB.qz(i),
+                                 SB.vx(i), SB.vy(i), SB.vz(i), SB.wx(i), SB.wy(i), SB.wz(i)};
+#pragma unroll
+            for (int r = 0; r < 13; ++r) adj->store[static_cast<size_t>(r) * adj->n_stride + b0 + i] = v[r];
+        }
+    }
     T.sync();
     phase_mark(T, P_, 5, t0);
     return true;

@@ -57,22 +57,22 @@ struct dyph_world {
     uint32_t f_n_items = 0;
     unsigned long long* f_phase = nullptr;  // [kFramePhases] phase timing of fused frames (null = off)
     // Adjoint of fused frames (dyph_world_rollout_backward), allocated on first use.
-    // per recorded frame, two sets (frame parity): contact records, poses
-    // after integrate, quaternions before renormalisation, contact words, counts
-    float* a_rec[2] = {nullptr, nullptr};      // [kRecWords][f_contact_slots]
-    float* a_pose1[2] = {nullptr, nullptr};    // [7][n]
-    float* a_qs[2] = {nullptr, nullptr};       // [4][n]
-    uint32_t* a_words[2] = {nullptr, nullptr}; // [kSceneWords][f_words_stride]
-    uint32_t* a_mg[2] = {nullptr, nullptr};    // [2 n_scenes]
+    // Record sets, one per frame of two checkpoint segments: contact records,
+    // poses after integrate, quaternions before renormalisation, contact
+    // words, counts.
+    std::vector<float*> a_rec;       // [kRecWords][f_contact_slots]
+    std::vector<float*> a_pose1;     // [7][n]
+    std::vector<float*> a_qs;        // [4][n]
+    std::vector<uint32_t*> a_words;  // [kSceneWords][f_words_stride]
+    std::vector<uint32_t*> a_mg;     // [2 n_scenes]
     float* a_g[2] = {nullptr, nullptr};  // [13][n] adjoint ping-pong
-    float* a_seg[2] = {nullptr, nullptr};  // [a_seg_frames][13][n] states of a checkpoint segment (double buffer)
+    float* a_seg[2] = {nullptr, nullptr};  // [a_seg_frames][13][n] states of frames 1.. of a segment (double buffer)
     uint32_t a_seg_frames = 0;
     uint32_t* a_pairs = nullptr;         // pair slots of spilled scenes, the recording's own
-    cudaStream_t a_stream = nullptr;     // re-steps the next checkpoint segment
-    cudaStream_t a_rstream = nullptr;    // records frame f - 1 while frame f is reversed
-    cudaEvent_t a_seg_ready = nullptr, a_rtail = nullptr;
-    cudaEvent_t a_rec_done[2] = {nullptr, nullptr}, a_rev_done[2] = {nullptr, nullptr};
+    cudaStream_t a_stream = nullptr;     // records the next checkpoint segment while this one is reversed
+    cudaEvent_t a_seg_ready = nullptr, a_rtail = nullptr, a_rev_done = nullptr;
     uint32_t* a_flag = nullptr;
+    uint32_t a_sized[4] = {0, 0, 0, 0};  // contact slots, words stride, pair slots, scenes the sets were made for
     uint32_t f_words_stride = 0, f_contact_slots = 0, f_pair_slots = 0;
     // Knobs of the fused kernel (dyph_world_set_fused_config / dyph_world_autotune).
     std::vector<uint32_t> h_body_offset;  // host copy of the scenes' body ranges
@@ -264,17 +264,15 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
                   w->a_flag, w->a_pairs};
     for (void* p : fb)
         if (p) cudaFree(p);
-    for (int k = 0; k < 2; ++k) {
+    for (size_t k = 0; k < w->a_rec.size(); ++k) {
         void* pk[] = {w->a_rec[k], w->a_pose1[k], w->a_qs[k], w->a_words[k], w->a_mg[k]};
         for (void* p : pk)
             if (p) cudaFree(p);
-        if (w->a_rec_done[k]) cudaEventDestroy(w->a_rec_done[k]);
-        if (w->a_rev_done[k]) cudaEventDestroy(w->a_rev_done[k]);
     }
     if (w->a_stream) cudaStreamDestroy(w->a_stream);
-    if (w->a_rstream) cudaStreamDestroy(w->a_rstream);
     if (w->a_seg_ready) cudaEventDestroy(w->a_seg_ready);
     if (w->a_rtail) cudaEventDestroy(w->a_rtail);
+    if (w->a_rev_done) cudaEventDestroy(w->a_rev_done);
     broadphase_destroy(w->bp);
     narrowphase_destroy(w->np);
     xpbd_destroy(w->sv);
@@ -1076,46 +1074,74 @@ dyph_bodies state_view(const dyph_world* w, float* st) {
     return v;
 }
 
-dyph_status adjoint_buffers(dyph_world* w, uint32_t seg_frames) {
+// Frames per recorded segment of a backward pass with a checkpoint at every
+// frame: enough to record the next segment while one is reversed, with one
+// wait between the two streams per segment.
+constexpr int32_t kRecordGroup = 4;
+
+// The adjoint's buffers: `sets` record sets and two segment buffers of
+// `seg_states` states each. The record sets and the recording's pair slots
+// are sized by the scenes' slots, so they are made again after the scenes
+// change (dyph_world_set_scenes).
+dyph_status adjoint_buffers(dyph_world* w, uint32_t sets, uint32_t seg_states) {
     const size_t n = w->desc.bodies.n;
+    const uint32_t n_sc = std::max(w->bp->n_scenes, 1u);
     if (!w->a_g[0]) {
-        bool ok = cudaMalloc(&w->a_g[0], 13 * n * 4) == cudaSuccess && cudaMalloc(&w->a_g[1], 13 * n * 4) == cudaSuccess &&
-                  cudaMalloc(&w->a_flag, 4) == cudaSuccess &&
-                  cudaMalloc(&w->a_pairs, static_cast<size_t>(std::max(w->f_pair_slots, 1u)) * 4) == cudaSuccess;
-        for (int k = 0; k < 2 && ok; ++k)
-            ok = cudaMalloc(&w->a_rec[k], static_cast<size_t>(kRecWords) * w->f_contact_slots * 4) == cudaSuccess &&
-                 cudaMalloc(&w->a_pose1[k], 7 * n * 4) == cudaSuccess && cudaMalloc(&w->a_qs[k], 4 * n * 4) == cudaSuccess &&
-                 cudaMalloc(&w->a_words[k], static_cast<size_t>(kSceneWords) * w->f_words_stride * 4) == cudaSuccess &&
-                 cudaMalloc(&w->a_mg[k], 2 * static_cast<size_t>(std::max(w->bp->n_scenes, 1u)) * 4) == cudaSuccess;
+        const bool ok = cudaMalloc(&w->a_g[0], 13 * n * 4) == cudaSuccess &&
+                        cudaMalloc(&w->a_g[1], 13 * n * 4) == cudaSuccess && cudaMalloc(&w->a_flag, 4) == cudaSuccess;
         if (!ok) return DYPH_ERR_NOMEM;
         DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->a_stream, cudaStreamNonBlocking));
-        DYPH_CUDA_TRY(cudaStreamCreateWithFlags(&w->a_rstream, cudaStreamNonBlocking));
-        cudaEvent_t* evs[] = {&w->a_seg_ready, &w->a_rtail, &w->a_rec_done[0], &w->a_rec_done[1], &w->a_rev_done[0],
-                              &w->a_rev_done[1]};
-        for (cudaEvent_t* e : evs) DYPH_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        for (cudaEvent_t* e : {&w->a_seg_ready, &w->a_rtail, &w->a_rev_done})
+            DYPH_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
-    if (seg_frames > w->a_seg_frames) {
+    const uint32_t sized[4] = {w->f_contact_slots, w->f_words_stride, w->f_pair_slots, n_sc};
+    if (!std::equal(sized, sized + 4, w->a_sized)) {
+        for (size_t k = 0; k < w->a_rec.size(); ++k) {
+            void* pk[] = {w->a_rec[k], w->a_pose1[k], w->a_qs[k], w->a_words[k], w->a_mg[k]};
+            for (void* p : pk)
+                if (p) cudaFree(p);
+        }
+        w->a_rec.clear();
+        w->a_pose1.clear();
+        w->a_qs.clear();
+        w->a_words.clear();
+        w->a_mg.clear();
+        if (w->a_pairs) cudaFree(w->a_pairs);
+        w->a_pairs = nullptr;
+        std::fill(w->a_sized, w->a_sized + 4, 0u);
+        if (cudaMalloc(&w->a_pairs, static_cast<size_t>(std::max(w->f_pair_slots, 1u)) * 4) != cudaSuccess)
+            return DYPH_ERR_NOMEM;
+        std::copy(sized, sized + 4, w->a_sized);
+    }
+    while (w->a_rec.size() < sets) {
+        float *rec = nullptr, *pose1 = nullptr, *qs = nullptr;
+        uint32_t *words = nullptr, *mg = nullptr;
+        const bool ok =
+            cudaMalloc(&rec, static_cast<size_t>(kRecWords) * w->f_contact_slots * 4) == cudaSuccess &&
+            cudaMalloc(&pose1, 7 * n * 4) == cudaSuccess && cudaMalloc(&qs, 4 * n * 4) == cudaSuccess &&
+            cudaMalloc(&words, static_cast<size_t>(kSceneWords) * w->f_words_stride * 4) == cudaSuccess &&
+            cudaMalloc(&mg, 2ull * n_sc * 4) == cudaSuccess;
+        if (!ok) {
+            void* pk[] = {rec, pose1, qs, words, mg};
+            for (void* p : pk)
+                if (p) cudaFree(p);
+            return DYPH_ERR_NOMEM;
+        }
+        w->a_rec.push_back(rec);
+        w->a_pose1.push_back(pose1);
+        w->a_qs.push_back(qs);
+        w->a_words.push_back(words);
+        w->a_mg.push_back(mg);
+    }
+    if (seg_states > w->a_seg_frames) {
         for (float*& b : w->a_seg) {
             if (b) cudaFree(b);
             b = nullptr;
         }
         w->a_seg_frames = 0;
         for (float*& b : w->a_seg)
-            if (cudaMalloc(&b, static_cast<size_t>(seg_frames) * 13 * n * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
-        w->a_seg_frames = seg_frames;
-    }
-    return DYPH_OK;
-}
-
-// The states at frames f0 .. f0 + len - 1 of a rollout, re-stepped from the
-// checkpoint at f0 into `out` on stream s.
-dyph_status restep_segment(dyph_world* w, const float* ckpt, int32_t len, float* out, cudaStream_t s) {
-    const size_t n = w->desc.bodies.n;
-    dyph_status st = unpack_state(w, ckpt, s);
-    if (st != DYPH_OK) return st;
-    for (int32_t j = 0; j < len; ++j) {
-        if ((st = pack_state(w, out + static_cast<size_t>(j) * 13 * n, s)) != DYPH_OK) return st;
-        if (j + 1 < len && (st = dyph_world_step(w, 1, reinterpret_cast<dyph_stream>(s))) != DYPH_OK) return st;
+            if (cudaMalloc(&b, static_cast<size_t>(seg_states) * 13 * n * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
+        w->a_seg_frames = seg_states;
     }
     return DYPH_OK;
 }
@@ -1145,8 +1171,25 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     if (!w || !w->fused || n_frames <= 0 || every <= 0 || !d_ckpt || !d_grad_final || !d_grad_init ||
         !d_grad_inv_mass)
         return DYPH_ERR_INVALID;
-    dyph_status st = adjoint_buffers(w, static_cast<uint32_t>(every));
+    // Frames are recorded in segments on a_stream, one record set per frame;
+    // sets alternate between two segments, so segment seg - 1 is recorded
+    // while segment seg is reversed on the caller's stream, last frame first.
+    // With checkpoints every `every` > 1 frames a segment is a checkpoint's
+    // frames, each recorded from the state the one before stored; with a
+    // checkpoint at every frame it is kRecordGroup frames, each recorded from
+    // its own checkpoint (one frame when that many sets do not fit).
+    int32_t group = every > 1 ? every : kRecordGroup;
+    dyph_status st = DYPH_ERR_NOMEM;
+    for (;;) {
+        const uint32_t seg_frames = static_cast<uint32_t>(std::min(group, n_frames));
+        st = adjoint_buffers(w, 2u * seg_frames, every > 1 ? seg_frames - 1u : 0u);
+        if (st != DYPH_ERR_NOMEM || every > 1 || group == 1) break;
+        cudaGetLastError();  // the failed allocation
+        group = 1;
+    }
     if (st != DYPH_OK) return st;
+    const int32_t seg_frames = std::min(group, n_frames);
+    const int32_t n_seg = (n_frames + group - 1) / group;
     const size_t n = w->desc.bodies.n;
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(s);
     DYPH_CUDA_TRY(cudaMemsetAsync(w->a_flag, 0, 4, cs));
@@ -1159,91 +1202,74 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
                 w->frame_smem};
     SceneBufs S_rev = S;
     S_rev.smem_bytes = w->r_smem;
-    // Three streams: the next checkpoint segment is re-stepped on a_stream,
-    // frame f - 1 is recorded on a_rstream while frame f is reversed on the
-    // caller's stream. Per-frame buffers alternate with the frame's parity; the
-    // recordings spill into their own pair slots and keep their contact words.
-    const int32_t n_seg = (n_frames + every - 1) / every;
-    const bool restep = every > 1;  // with a checkpoint at every frame the checkpoints are the states
-    auto seg_len = [&](int32_t seg) { return std::min(every, n_frames - seg * every); };
-    auto ckpt = [&](int32_t seg) { return d_ckpt + static_cast<size_t>(seg) * 13 * n; };
-    // The frame's start state; the record and reverse kernels only read it
-    // (frame_scene with an AdjRun writes nothing back), so a checkpoint can
-    // serve directly.
+    auto seg_len = [&](int32_t seg) { return std::min(group, n_frames - seg * group); };
+    auto ckpt = [&](int32_t c) { return d_ckpt + static_cast<size_t>(c) * 13 * n; };
+    // Frame f's start state: its segment's checkpoint, or the state its
+    // predecessor's recording stored. The record and reverse kernels only
+    // read it, so a checkpoint serves directly.
     auto state = [&](int32_t f) {
         const int32_t seg = f / every, j = f % every;
-        return restep ? w->a_seg[seg & 1] + static_cast<size_t>(j) * 13 * n : const_cast<float*>(ckpt(seg));
+        return j == 0 ? const_cast<float*>(ckpt(seg)) : w->a_seg[seg & 1] + static_cast<size_t>(j - 1) * 13 * n;
     };
+    auto set_of = [&](int32_t f) { return static_cast<size_t>(((f / group) & 1) * seg_frames + f % group); };
     auto params = [&](int32_t f) {
         return FrameParams{state_view(w, state(f)), d.shapes, ip.gravity[0], ip.gravity[1], ip.gravity[2], sub_dt,
                            0.5f * sub_dt, w->sv->friction, ip.dt, ip.n_substeps, static_cast<int>(w->sv->mode),
                            w->sv->n_iters, w->sv->meta, w->bp->counts, w->np->counts, w->stats + 4, nullptr};
     };
-    auto adj = [&](int32_t f) {
-        const int k = f & 1;
+    auto adj = [&](int32_t f, float* store) {
+        const size_t k = set_of(f);
         return AdjRun{w->a_rec[k], w->f_contact_slots, w->a_pose1[k], w->a_qs[k], static_cast<uint32_t>(n),
-                      w->a_flag};
+                      w->a_flag, store};
     };
-    auto keep = [&](int32_t f) { return AdjKeep{w->a_words[f & 1], w->a_mg[f & 1]}; };
+    auto keep = [&](int32_t f) { return AdjKeep{w->a_words[set_of(f)], w->a_mg[set_of(f)]}; };
     auto frame_bufs = [&](int32_t f) {
         return FrameBufs{w->f_pair_base, w->f_contact_base, w->a_pairs, w->f_contact_raw, w->f_color_raw,
-                         w->f_counts, w->a_words[f & 1], w->f_words_stride, w->f_contact_slots};
+                         w->f_counts, w->a_words[set_of(f)], w->f_words_stride, w->f_contact_slots};
     };
-    auto record = [&](int32_t f) -> dyph_status {
-        scene_frame_record_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, w->a_rstream>>>(
-            S, frame_bufs(f), params(f), adj(f), keep(f), w->f_items, w->f_n_items);
-        DYPH_CUDA_TRY(cudaGetLastError());
-        DYPH_CUDA_TRY(cudaEventRecord(w->a_rec_done[f & 1], w->a_rstream));
+    // The recordings spill into their own pair slots and keep their contact
+    // words; each but a segment's last stores the next frame's start state.
+    auto record_segment = [&](int32_t seg) -> dyph_status {
+        const int32_t f0 = seg * group, len = seg_len(seg);
+        for (int32_t j = 0; j < len; ++j) {
+            const int32_t f = f0 + j;
+            scene_frame_record_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, w->a_stream>>>(
+                S, frame_bufs(f), params(f), adj(f, every > 1 && j + 1 < len ? state(f + 1) : nullptr), keep(f), w->f_items,
+                w->f_n_items);
+            DYPH_CUDA_TRY(cudaGetLastError());
+        }
+        DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
         return DYPH_OK;
     };
     // everything below starts after the caller's stream
     DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, cs));
     DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rtail, 0));
-    DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_rtail, 0));
-    if (restep) {
-        st = restep_segment(w, ckpt(n_seg - 1), seg_len(n_seg - 1), w->a_seg[(n_seg - 1) & 1], w->a_stream);
-        if (st != DYPH_OK) return st;
-        DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
-        DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_seg_ready, 0));
-    }
-    if ((st = record(n_frames - 1)) != DYPH_OK) return st;
+    if ((st = record_segment(n_seg - 1)) != DYPH_OK) return st;
     int cur = 0;
-    for (int32_t f = n_frames - 1; f >= 0; --f) {
-        const int32_t seg = f / every;
-        // the previous segment is re-stepped as this one starts; its buffer was
-        // last read by the recordings of segment seg + 1 (all queued on
-        // a_rstream) and by their reverse passes (queued on cs, the last one
-        // being frame f + 1's)
-        if (restep && f % every == seg_len(seg) - 1 && seg > 0) {
-            DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, w->a_rstream));
-            DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rtail, 0));
-            if (f + 1 < n_frames) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rev_done[(f + 1) & 1], 0));
-            st = restep_segment(w, ckpt(seg - 1), seg_len(seg - 1), w->a_seg[(seg - 1) & 1], w->a_stream);
-            if (st != DYPH_OK) return st;
-            DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
+    for (int32_t seg = n_seg - 1; seg >= 0; --seg) {
+        DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_seg_ready, 0));
+        if (seg > 0) {
+            // segment seg - 1's sets and states were last read by segment
+            // seg + 1's reverse passes, queued on cs before this point
+            if (seg + 1 < n_seg) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_stream, w->a_rev_done, 0));
+            if ((st = record_segment(seg - 1)) != DYPH_OK) return st;
         }
-        if (f > 0) {
-            // frame f - 1's buffers were last used by the reverse pass of frame f + 1
-            if (restep && (f - 1) / every != seg) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_seg_ready, 0));
-            if (f + 1 < n_frames) DYPH_CUDA_TRY(cudaStreamWaitEvent(w->a_rstream, w->a_rev_done[(f - 1) & 1], 0));
-            if ((st = record(f - 1)) != DYPH_OK) return st;
+        for (int32_t f = seg * group + seg_len(seg) - 1; f >= seg * group; --f) {
+            AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
+            FrameBufs fb = frame_bufs(f);
+            FrameParams pf = params(f);
+            AdjRun af = adj(f, nullptr);
+            AdjKeep kf = keep(f);
+            void* args[] = {&S_rev, &fb, &pf, &af, &kf, &G, &w->r_items, &w->r_n_items};
+            DYPH_CUDA_TRY(
+                cudaLaunchKernel(reverse_kernel(), dim3(w->r_n_items), dim3(kSceneThreads), args, w->r_smem, cs));
+            cur ^= 1;
         }
-        DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_rec_done[f & 1], 0));
-        AdjFrame G{w->a_g[cur], w->a_g[cur ^ 1], d_grad_inv_mass};
-        FrameBufs fb = frame_bufs(f);
-        FrameParams pf = params(f);
-        AdjRun af = adj(f);
-        AdjKeep kf = keep(f);
-        void* args[] = {&S_rev, &fb, &pf, &af, &kf, &G, &w->r_items, &w->r_n_items};
-        DYPH_CUDA_TRY(cudaLaunchKernel(reverse_kernel(), dim3(w->r_n_items), dim3(kSceneThreads), args, w->r_smem, cs));
-        DYPH_CUDA_TRY(cudaEventRecord(w->a_rev_done[f & 1], cs));
-        cur ^= 1;
+        DYPH_CUDA_TRY(cudaEventRecord(w->a_rev_done, cs));
     }
-    // the side streams end before the caller's stream goes on
-    DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, w->a_rstream));
+    // the side stream ends before the caller's stream goes on
+    DYPH_CUDA_TRY(cudaEventRecord(w->a_rtail, w->a_stream));
     DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_rtail, 0));
-    DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
-    DYPH_CUDA_TRY(cudaStreamWaitEvent(cs, w->a_seg_ready, 0));
     DYPH_CUDA_TRY(cudaMemcpyAsync(d_grad_init, w->a_g[cur], 13 * n * 4, cudaMemcpyDeviceToDevice, cs));
     uint32_t flag = 0;
     DYPH_CUDA_TRY(cudaMemcpyAsync(&flag, w->a_flag, 4, cudaMemcpyDeviceToHost, cs));

@@ -464,17 +464,24 @@ dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s, uint64_t*
  * after the rollout ([13][n]), and returns d_grad_init, the adjoint of the
  * state at frame 0 ([13][n]), and d_grad_inv_mass, the adjoint of every
  * body's inverse mass ([n], overwritten; the inverse inertia is held fixed).
- * Each checkpoint segment is recomputed forward, then every frame is reversed
- * by one kernel launch (one thread block per scene) that recomputes the
- * frame, records its contact set, narrowphase branches and pre-solve states,
- * and applies the hand-written adjoints of the renormalisations, the contact
- * solves (in reverse colour / level order), the narrowphase and the
- * integration. The contact set and every branch are those of the forward
- * frames. Static bodies get zero adjoints. Returns DYPH_ERR_UNSUPPORTED (the
- * gradients are then incomplete) when a frame took a path the adjoint does
- * not differentiate: a contact that first acted after a renormalisation
- * (deferred at w_total < 1e-10), more than 8 substeps or 10 iterations.
- * Fused batched worlds only; the world's body state is scratch afterwards. */
+ * Each checkpoint segment is recomputed forward once, from its checkpoint, by
+ * a recording kernel (one launch per frame) that keeps every frame's contact
+ * set, narrowphase branches and pre-solve states and stores the next frame's
+ * start state; every frame is then reversed by one launch of the reverse
+ * kernel, which applies the hand-written adjoints of the renormalisations,
+ * the contact solves (in reverse level order), the narrowphase and the
+ * integration. Segment seg - 1 is recorded on a side stream while segment
+ * seg is reversed on s (with every = 1, a segment is 4 frames, each recorded
+ * from its own checkpoint; 1 frame when 8 record sets do not fit). The contact set and every branch are those of the
+ * forward frames. Static bodies get zero adjoints. Returns
+ * DYPH_ERR_UNSUPPORTED (the gradients are then incomplete) when a frame took
+ * a path the adjoint does not differentiate: a contact that first acted after
+ * a renormalisation (deferred at w_total < 1e-10), more than 8 substeps or 10
+ * iterations. Device memory beyond the checkpoints: one record set per frame
+ * of two segments (2 min(L, n_frames) sets, L = every or 4 when every = 1,
+ * of 4 (36 + 13) bytes per contact slot plus 44 bytes per body) and, when
+ * every > 1, 2 (min(every, n_frames) - 1) states. Fused batched worlds only; the world's body state is left as it
+ * was. */
 dyph_status dyph_world_rollout(dyph_world* w, int32_t n_frames, int32_t every, float* d_ckpt, dyph_stream s);
 dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_frames, int32_t every, const float* d_ckpt,
                                         const float* d_grad_final, float* d_grad_init, float* d_grad_inv_mass,
