@@ -216,3 +216,55 @@ def test_rollout_through_module_matches_ctypes_world(dp):
     for a, b in zip(*results):
         assert torch.equal(a, b)
     assert results[0][1].abs().sum() > 0
+
+
+@pytest.mark.gpu
+def test_backward_after_the_scenes_change(dp):
+    """The adjoint's record sets are sized by the scenes' slots: after
+    set_scenes changes them, a backward pass equals, bit for bit, that of a
+    world set up with the new scenes from the start."""
+    import torch
+
+    from dyphur_b200 import device
+    device.require_device()
+    scene = scenes.push(4)
+    n = scene.n_bodies
+    off = [int(x) for x in scene.body_offset]
+    merged = [off[0], off[2], off[4]]  # two scenes of two pushes each
+
+    def aabb(lo, hi):
+        b = np.concatenate([scene.bounds[lo:hi, :3].min(0), scene.bounds[lo:hi, 3:].max(0)])
+        return dp.AABB(*(float(x) for x in b))
+
+    def world(s):
+        ss, bs = _stores(dp, s, scene)
+        w = dp.World(s, bs, ss, aabb(0, 4), _params(dp, scene), 48 * n + 256, 16 * n + 256, scene.n_iters,
+                     scene.friction, dp.SolverMode.Sequential)
+        return w, (ss, bs)
+
+    def grads(w):
+        rows = torch.as_tensor(w.device_rows(), device="cuda")
+        init = torch.as_tensor(w.initial_rows(), device="cuda")
+        vel = init[7:10, :n].T.clone().requires_grad_(True)
+        ang = init[10:13, :n].T.clone().requires_grad_(True)
+        im = rows[13, :n].clone().requires_grad_(True)
+        final = dp.rollout(w, vel, ang, im, 12, 4)
+        (final[:3] ** 2).sum().backward()
+        torch.cuda.synchronize()
+        return [t.grad.cpu().numpy() for t in (vel, ang, im)]
+
+    s = dp.Device.default_gpu().make_stream()
+    w, keep = world(s)
+    w.set_scenes(off, [aabb(i, i + 1) for i in range(4)])
+    s.wait()
+    grads(w)
+    w.set_scenes(merged, [aabb(0, 2), aabb(2, 4)])
+    s.wait()
+    got = grads(w)
+    w2, keep2 = world(s)
+    w2.set_scenes(merged, [aabb(0, 2), aabb(2, 4)])
+    s.wait()
+    want = grads(w2)
+    assert np.abs(want[0]).sum() > 0
+    for a, b in zip(got, want):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
