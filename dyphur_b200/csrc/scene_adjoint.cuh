@@ -65,7 +65,7 @@ __device__ void record_scene(const Team& T, uint32_t s, unsigned char* smem, uin
                              const SceneBufs& S, const FrameBufs& F, const FrameParams& P_, const AdjRun& A,
                              const AdjKeep& K) {
     FrameOut fo{};
-    const bool ok = frame_scene(T, s, smem, smem_bytes, sh, S, F, P_, &A, &fo);
+    const bool ok = frame_scene<true>(T, s, smem, smem_bytes, sh, S, F, P_, &A, &fo);
     const uint32_t m = ok ? fo.m : 0u, groups = ok ? fo.groups : 0u;
     const SceneContacts dst{K.words + F.contact_base[s] + s, F.words_stride};
     const SceneContacts& SC = fo.SC;

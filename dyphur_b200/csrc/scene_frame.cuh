@@ -132,11 +132,13 @@ struct FrameOut {
 };
 
 // One frame of scene s by team T with `smem_bytes` of shared memory at smem.
-// Returns false after raising an error.
-template <class Team>
+// Returns false after raising an error. kRecord compiles the adjoint's
+// recording in (`adj_in`, `out`); the forward frame is built without it.
+template <bool kRecord = false, class Team>
 __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint32_t smem_bytes, SceneShared& sh,
                             const SceneBufs& S, const FrameBufs& F, const FrameParams& P_,
-                            const AdjRun* adj = nullptr, FrameOut* out = nullptr) {
+                            const AdjRun* adj_in = nullptr, FrameOut* out = nullptr) {
+    const AdjRun* const adj = kRecord ? adj_in : nullptr;
     const GlobalBodies B{P_.gb};
     const uint32_t lane = threadIdx.x & 31u;
     uint64_t t0 = P_.phase_ns ? global_ns() : 0u;
@@ -327,7 +329,7 @@ __device__ bool frame_scene(const Team& T, uint32_t s, unsigned char* smem, uint
         SolveRecord rec{};
         if (adj) rec = SolveRecord{adj->rec, adj->rec_stride, cbase, adj->qs, adj->n_stride, b0, adj->flag};
         uint64_t t_sweep = 0;
-        if (!scene_solve(T, nb, m, SB, R, SC, P_.mode, P_.n_iters, P_.mu, P_.dt, sh, colored, n_colors, rounds,
+        if (!scene_solve<kRecord>(T, nb, m, SB, R, SC, P_.mode, P_.n_iters, P_.mu, P_.dt, sh, colored, n_colors, rounds,
                          adj ? &rec : nullptr, &groups, P_.phase_ns ? &t_sweep : nullptr))
             return false;
         if (P_.phase_ns && T.leader()) {

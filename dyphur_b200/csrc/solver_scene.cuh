@@ -300,10 +300,12 @@ __device__ __forceinline__ void record_state(float* r, uint32_t stride, const Sc
 }
 
 // One sweep over the groups in ascending order, one contact per thread at a
-// time inside a group (no two of a group share a dynamic body).
-template <class Team>
+// time inside a group (no two of a group share a dynamic body). kRecord
+// compiles the recording in; without it `rec` is ignored.
+template <bool kRecord, class Team>
 __device__ void scene_sweep(const Team& T, uint32_t groups, const SceneBodies& SB, const SceneContacts& SC, float mu,
-                            float dt, int* s_flag, const SolveRecord* rec = nullptr, int iter = 0) {
+                            float dt, int* s_flag, const SolveRecord* rec_in = nullptr, int iter = 0) {
+    const SolveRecord* const rec = kRecord ? rec_in : nullptr;
     for (uint32_t g = 0; g < groups; ++g) {
         const uint32_t end = SC.pa(g + 1);
         for (uint32_t i = SC.pa(g) + T.rank(); i < end; i += T.size()) {
@@ -390,12 +392,13 @@ __device__ __forceinline__ void scene_store_bodies(const Team& T, const GlobalBo
 // lambda = 0, geometry; pb = none) with R.cnt[b] = the b-side contact count of
 // every dynamic body b. Leaves the bodies solved and renormalised in SB and
 // the colours (or UINT32_MAX) in SC.done. Returns false after raising an error.
-template <class Team>
+template <bool kRecord = false, class Team>
 __device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneBodies& SB, const SceneSolverRows& R,
                             const SceneContacts& SC, int mode, int n_iters, float mu, float dt, SceneShared& sh,
                             bool& colored_out, uint32_t& n_colors_out, uint32_t& rounds_out,
-                            const SolveRecord* rec = nullptr, uint32_t* groups_out = nullptr,
+                            const SolveRecord* rec_in = nullptr, uint32_t* groups_out = nullptr,
                             uint64_t* sweep_start = nullptr) {
+    const SolveRecord* const rec = kRecord ? rec_in : nullptr;
     // ── predecessors in contact order: b-side lists (scan, fill, sort) ──
     if (T.leader()) {
         sh.carry = 0u;
@@ -514,7 +517,7 @@ __device__ bool scene_solve(const Team& T, uint32_t nb, uint32_t m, const SceneB
     if (groups_out) *groups_out = groups;
     for (int iter = 0; iter < n_iters; ++iter) {
         if (iter == 0 || deferred) {
-            scene_sweep(T, groups, SB, SC, mu, dt, &sh.flag, rec, iter);
+            scene_sweep<kRecord>(T, groups, SB, SC, mu, dt, &sh.flag, rec, iter);
             deferred = sh.flag != 0;
         }
         if (rec && iter == 0)
