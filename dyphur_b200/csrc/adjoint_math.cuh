@@ -43,6 +43,11 @@ __device__ __forceinline__ float dot(F3 a, F3 b) { return fma3(a.x, b.x, a.y, b.
 __device__ __forceinline__ F3 cross(F3 a, F3 b) {
     return F3{__fmaf_rn(a.y, b.z, -(a.z * b.y)), __fmaf_rn(a.z, b.x, -(a.x * b.z)), __fmaf_rn(a.x, b.y, -(a.y * b.x))};
 }
+// a + s b, fused per component.
+__device__ __forceinline__ F3 fmav(float s, F3 b, F3 a) {
+    return F3{__fmaf_rn(s, b.x, a.x), __fmaf_rn(s, b.y, a.y), __fmaf_rn(s, b.z, a.z)};
+}
+__device__ __forceinline__ float fmav(float s, float b, float a) { return __fmaf_rn(s, b, a); }
 // M^T v and M v for a 3x3 M.
 __device__ __forceinline__ F3 mtv(const float M[3][3], F3 v) {
     return f3(fma3(M[0][0], v.x, M[1][0], v.y, M[2][0], v.z), fma3(M[0][1], v.x, M[1][1], v.y, M[2][1], v.z),
@@ -471,14 +476,14 @@ __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Cont
         F3 tb = f3(0.f, 0.f, 0.f), fab = tb, fbb = tb;
         if (da) {
             jtb += -wa * dot(G0.v, t) - dot(G0.w, fa);
-            tb += (-wa * jt) * G0.v;
-            fab += (-jt) * G0.w;
+            tb = fmav((-wa * jt), G0.v, tb);
+            fab = fmav((-jt), G0.w, fab);
             wab += -jt * dot(G0.v, t);
         }
         if (dbn) {
             jtb += wb * dot(G1.v, t) + dot(G1.w, fb);
-            tb += (wb * jt) * G1.v;
-            fbb += jt * G1.w;
+            tb = fmav((wb * jt), G1.v, tb);
+            fbb = fmav(jt, G1.w, fbb);
             wbb += jt * dot(G1.v, t);
         }
         float Ltb = 0.f, wtb = 0.f;
@@ -493,8 +498,8 @@ __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Cont
         wab += wtb;
         wbb += wtb;
         F3 eab = wtb * fa, ebb = wtb * fb;
-        fab += wtb * ea;
-        fbb += wtb * eb;
+        fab = fmav(wtb, ea, fab);
+        fbb = fmav(wtb, eb, fbb);
         winv_adj(qa1, L.I[0], ea, fab, eab, qa1b);
         winv_adj(qb1, L.I[1], eb, fbb, ebb, qb1b);
         rab += cross(t, eab);
@@ -503,12 +508,12 @@ __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Cont
         tb += cross(ebb, rb);
         F3 vtb = (1.f / Lt) * tb;
         Ltb += -dot(tb, vt) / (Lt * Lt);
-        vtb += (Ltb / Lt) * vt;
+        vtb = fmav((Ltb / Lt), vt, vtb);
         const F3 rvb0 = vtb;
         const float rvnb = -dot(vtb, n);
-        nb += (-rvn) * vtb;
+        nb = fmav((-rvn), vtb, nb);
         const F3 rvb = rvb0 + rvnb * n;
-        nb += rvnb * rv;
+        nb = fmav(rvnb, rv, nb);
         va1b += rvb;
         oa1b += cross(ra, rvb);
         rab += cross(rvb, oa1);
@@ -522,22 +527,22 @@ __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Cont
         F3 dAb = f3(0.f, 0.f, 0.f), dBb = dAb;
         if (da) {
             jnb += wa * dot(va1b, n) + dot(oa1b, dA);
-            nb += (wa * jn) * va1b;
+            nb = fmav((wa * jn), va1b, nb);
             wab += jn * dot(va1b, n);
-            dAb += jn * oa1b;
+            dAb = fmav(jn, oa1b, dAb);
         }
         if (dbn) {
             jnb += -wb * dot(vb1b, n) - dot(ob1b, dB);
-            nb += (-wb * jn) * vb1b;
+            nb = fmav((-wb * jn), vb1b, nb);
             wbb += -jn * dot(vb1b, n);
-            dBb += (-jn) * ob1b;
+            dBb = fmav((-jn), ob1b, dBb);
         }
         winv_adj(qa1, L.I[0], ca, dAb, cab, qa1b);
         winv_adj(qb1, L.I[1], cb, dBb, cbb, qb1b);
         const float vrelnb = -jnb / w;
         wbar += -jnb * jn / w;
         const F3 vrelb = vrelnb * n;
-        nb += vrelnb * vrel;
+        nb = fmav(vrelnb, vrel, nb);
         vab += vrelb;
         oab += cross(ra, vrelb);
         rab += cross(vrelb, oa);
@@ -553,10 +558,10 @@ __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Cont
         quat_delta_adj(qa, aa, 0.5f, qa1b, qin, aab);
         for (int k = 0; k < 4; ++k) qab[k] = qin[k];
         dlb += dot(aab, ua);
-        uab += dl * aab;
+        uab = fmav(dl, aab, uab);
         dlb += wa * dot(G0.x, n);
         wab += dl * dot(G0.x, n);
-        nb += (wa * dl) * G0.x;
+        nb = fmav((wa * dl), G0.x, nb);
     }
     if (dbn) {
         F3 abb = f3(0.f, 0.f, 0.f);
@@ -564,19 +569,19 @@ __device__ __forceinline__ void solve_contact_adj(const LocalPair& L, const Cont
         quat_delta_adj(qbq, ab, 0.5f, qb1b, qin, abb);
         for (int k = 0; k < 4; ++k) qbb[k] = qin[k];
         dlb += -dot(abb, ub);
-        ubb += (-dl) * abb;
+        ubb = fmav((-dl), abb, ubb);
         dlb += -wb * dot(G1.x, n);
         wbb += -dl * dot(G1.x, n);
-        nb += (-wb * dl) * G1.x;
+        nb = fmav((-wb * dl), G1.x, nb);
     }
     remb += dlb / w;
     wbar += -dlb * dl / w;
     wab += wbar;
     wbb += wbar;
-    cab += wbar * ua;
-    uab += wbar * ca;
-    cbb += wbar * ub;
-    ubb += wbar * cb;
+    cab = fmav(wbar, ua, cab);
+    uab = fmav(wbar, ca, uab);
+    cbb = fmav(wbar, ub, cbb);
+    ubb = fmav(wbar, cb, ubb);
     winv_adj(qa, L.I[0], ca, uab, cab, qab);
     winv_adj(qbq, L.I[1], cb, ubb, cbb, qbb);
     rab += cross(n, cab);
