@@ -669,10 +669,12 @@ def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask,
     # segments (36 record and 13 word rows per contact slot, 11 rows per
     # body), the two adjoint states
     n_ckpt = (frames + every - 1) // every
-    seg = min(every if every > 1 else 4, frames)
-    states = 2 * (seg - 1) * 13 * n if every > 1 else 0
     slots = int(sum(max(64, 16 * int(b) + 64) for b in np.diff(scene.body_offset)))
-    act = 4 * (n_ckpt * 13 * n + states + 2 * seg * ((36 + 13) * slots + 11 * n) + 2 * 13 * n)
+    set_bytes = 4 * ((36 + 13) * slots + 11 * n)
+    group = every if every > 1 else max(1, min(4, (2 << 30) // (2 * set_bytes)))
+    seg = min(group, frames)
+    states = 2 * (seg - 1) * 13 * n if every > 1 else 0
+    act = 4 * (n_ckpt * 13 * n + states + 2 * 13 * n) + 2 * seg * set_bytes
     w.close()
     return {"workload": label, "scenes": scene.n_scenes, "bodies": n, "frames": frames,
             "checkpoint_every": every, "solver_mode": "sequential",

@@ -1076,8 +1076,17 @@ dyph_bodies state_view(const dyph_world* w, float* st) {
 
 // Frames per recorded segment of a backward pass with a checkpoint at every
 // frame: enough to record the next segment while one is reversed, with one
-// wait between the two streams per segment.
+// wait between the two streams per segment; fewer when the two segments'
+// record sets would pass kRecordBudget bytes.
 constexpr int32_t kRecordGroup = 4;
+constexpr size_t kRecordBudget = size_t(2) << 30;
+
+// Bytes of one record set (records, poses after integrate, quaternions before
+// renormalisation, contact words, counts).
+size_t record_set_bytes(const dyph_world* w) {
+    return 4 * (static_cast<size_t>(kRecWords) * w->f_contact_slots + 11ull * w->desc.bodies.n +
+                static_cast<size_t>(kSceneWords) * w->f_words_stride + 2ull * std::max(w->bp->n_scenes, 1u));
+}
 
 // The adjoint's buffers: `sets` record sets and two segment buffers of
 // `seg_states` states each. The record sets and the recording's pair slots
@@ -1176,9 +1185,13 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
     // while segment seg is reversed on the caller's stream, last frame first.
     // With checkpoints every `every` > 1 frames a segment is a checkpoint's
     // frames, each recorded from the state the one before stored; with a
-    // checkpoint at every frame it is kRecordGroup frames, each recorded from
-    // its own checkpoint (one frame when that many sets do not fit).
-    int32_t group = every > 1 ? every : kRecordGroup;
+    // checkpoint at every frame it is up to kRecordGroup frames, each recorded
+    // from its own checkpoint (one frame when that many sets do not fit).
+    int32_t group = every;
+    if (every == 1) {
+        const size_t sets = kRecordBudget / (2 * record_set_bytes(w));
+        group = static_cast<int32_t>(std::max<size_t>(1, std::min<size_t>(kRecordGroup, sets)));
+    }
     dyph_status st = DYPH_ERR_NOMEM;
     for (;;) {
         const uint32_t seg_frames = static_cast<uint32_t>(std::min(group, n_frames));

@@ -471,16 +471,17 @@ dyph_status dyph_world_download_phase_ns(dyph_world* w, dyph_stream s, uint64_t*
  * kernel, which applies the hand-written adjoints of the renormalisations,
  * the contact solves (in reverse level order), the narrowphase and the
  * integration. Segment seg - 1 is recorded on a side stream while segment
- * seg is reversed on s (with every = 1, a segment is 4 frames, each recorded
- * from its own checkpoint; 1 frame when 8 record sets do not fit). The contact set and every branch are those of the
+ * seg is reversed on s (with every = 1, a segment is up to 4 frames, each
+ * recorded from its own checkpoint, as many as keep two segments' record
+ * sets within 2 GiB; 1 frame when they do not fit the device). The contact set and every branch are those of the
  * forward frames. Static bodies get zero adjoints. Returns
  * DYPH_ERR_UNSUPPORTED (the gradients are then incomplete) when a frame took
  * a path the adjoint does not differentiate: a contact that first acted after
  * a renormalisation (deferred at w_total < 1e-10), more than 8 substeps or 10
  * iterations. Device memory beyond the checkpoints: one record set per frame
- * of two segments (2 min(L, n_frames) sets, L = every or 4 when every = 1,
- * of 4 (36 + 13) bytes per contact slot plus 44 bytes per body) and, when
- * every > 1, 2 (min(every, n_frames) - 1) states. Fused batched worlds only; the world's body state is left as it
+ * of two segments (2 min(L, n_frames) sets, L = every, or up to 4 when
+ * every = 1, of 4 (36 + 13) bytes per contact slot plus 44 bytes per body)
+ * and, when every > 1, 2 (min(every, n_frames) - 1) states. Fused batched worlds only; the world's body state is left as it
  * was. */
 dyph_status dyph_world_rollout(dyph_world* w, int32_t n_frames, int32_t every, float* d_ckpt, dyph_stream s);
 dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_frames, int32_t every, const float* d_ckpt,
