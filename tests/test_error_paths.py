@@ -28,6 +28,10 @@ def test_host_argument_checks():
     assert L.dyph_world_check_finite(None, None, None) == capi.ERR_INVALID
     assert L.dyph_contact_sensor_filter(None, None, None, 0, None) == capi.ERR_INVALID
     assert L.dyph_contact_sensor_count(None) == 0
+    assert L.dyph_world_adjoint_config(None, None) == capi.ERR_INVALID
+    assert L.dyph_world_set_adjoint_config(None, 0, 1) == capi.ERR_INVALID
+    assert L.dyph_world_set_fused_config(None, 0, 1, 0) == capi.ERR_INVALID
+    assert L.dyph_world_rollout_backward(None, 1, 1, None, None, None, None, None) == capi.ERR_INVALID
     for code in range(11):
         assert capi.lib().dyph_status_string(code) not in (None, b"unknown status")
 
