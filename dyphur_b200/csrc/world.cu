@@ -1246,9 +1246,9 @@ extern "C" dyph_status dyph_world_rollout_backward(dyph_world* w, int32_t n_fram
         const int32_t f0 = seg * group, len = seg_len(seg);
         for (int32_t j = 0; j < len; ++j) {
             const int32_t f = f0 + j;
+            float* store = every > 1 && j + 1 < len ? state(f + 1) : nullptr;
             scene_frame_record_kernel<<<w->f_n_items, kSceneThreads, w->frame_smem, w->a_stream>>>(
-                S, frame_bufs(f), params(f), adj(f, every > 1 && j + 1 < len ? state(f + 1) : nullptr), keep(f), w->f_items,
-                w->f_n_items);
+                S, frame_bufs(f), params(f), adj(f, store), keep(f), w->f_items, w->f_n_items);
             DYPH_CUDA_TRY(cudaGetLastError());
         }
         DYPH_CUDA_TRY(cudaEventRecord(w->a_seg_ready, w->a_stream));
