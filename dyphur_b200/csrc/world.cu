@@ -260,7 +260,8 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     }
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
-                  w->f_words, w->f_pos, w->f_items, w->r_items, w->f_phase, w->a_g[0], w->a_g[1], w->a_seg[0], w->a_seg[1],
+                  w->f_words, w->f_pos, w->f_items, w->r_items, w->f_phase, w->a_g[0], w->a_g[1], w->a_seg[0],
+                  w->a_seg[1],
                   w->a_flag, w->a_pairs};
     for (void* p : fb)
         if (p) cudaFree(p);
@@ -608,7 +609,8 @@ dyph_status setup_reverse(dyph_world* w) {
     std::vector<uint32_t> items;
     uint32_t n_small = 0, n_mid = 0;
     build_items(off, n_scenes, (smem / 4u) & ~15u, w->r_teams,
-                [](uint32_t nb) { return frame_body_bytes(nb) + (kSceneWords + kRecWords) * 10u * nb; }, items, n_small, n_mid);
+                [](uint32_t nb) { return frame_body_bytes(nb) + (kSceneWords + kRecWords) * 10u * nb; }, items,
+                n_small, n_mid);
     if (w->r_items) cudaFree(w->r_items);
     w->r_items = nullptr;
     if (cudaMalloc(&w->r_items, items.size() * 4) != cudaSuccess) return DYPH_ERR_NOMEM;
