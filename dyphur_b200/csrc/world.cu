@@ -261,8 +261,7 @@ extern "C" void dyph_world_destroy(dyph_world* w) {
     if (w->traj_stream) cudaStreamDestroy(w->traj_stream);
     void* fb[] = {w->f_pair_base, w->f_contact_base, w->f_pair_raw, w->f_contact_raw, w->f_color_raw, w->f_counts,
                   w->f_words, w->f_pos, w->f_items, w->r_items, w->f_phase, w->a_g[0], w->a_g[1], w->a_seg[0],
-                  w->a_seg[1],
-                  w->a_flag, w->a_pairs};
+                  w->a_seg[1], w->a_flag, w->a_pairs};
     for (void* p : fb)
         if (p) cudaFree(p);
     for (size_t k = 0; k < w->a_rec.size(); ++k) {
