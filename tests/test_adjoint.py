@@ -127,16 +127,20 @@ def test_adjoint_matches_central_differences(dev):
 
 
 def test_checkpoint_spacing_does_not_change_the_gradient(dev):
+    """Segments re-recorded from their checkpoints (every > 1, the last one
+    shorter, or one segment longer than the rollout) give the gradient of a
+    checkpoint at every frame, bit for bit."""
     import torch
     from dyphur_b200.autograd import rollout
     out = []
-    for every in (1, 7, 15):
+    for every in (1, 7, 15, 20):
         s, w, vel, ang, im, tgt, mask = _setup(dev, n_scenes=2)
         _loss(rollout(w, vel, ang, im, 15, every=every), tgt, mask).backward()
         torch.cuda.synchronize()
         out.append(np.concatenate([vel.grad.cpu().numpy().ravel(), im.grad.cpu().numpy()]))
+    assert np.abs(out[0]).sum() > 0
     for o in out[1:]:
-        assert np.allclose(o, out[0], rtol=1e-5, atol=1e-6 * np.abs(out[0]).max())
+        assert np.array_equal(o.view(np.uint32), out[0].view(np.uint32))
 
 
 def test_reverse_layout_does_not_change_the_gradient(dev):
