@@ -487,11 +487,8 @@ def gpu_workload(scene, mode, frames, args, torch, barrier, clocks=None, rooflin
     from dyphur_b200 import device
     w = device.World(scene, mode=mode)
     tuned = None
-    if scene.n_scenes > 1:  # tuned on settled frames, before the episode is captured
-        init = w.bodies.fbuf.clone()
-        w.step(min(120, frames))
-        tuned = w.autotune(16)
-        w.bodies.fbuf.copy_(init)
+    if scene.n_scenes > 1:  # tuned on the episode's first half from its initial state, before it is captured
+        tuned = w.autotune(max(16, frames // 2))
         torch.cuda.synchronize()
     w.capture_episode(frames, -1)
     ms, ck, init = timed_episodes(w, args.steps, args.warmup, torch, barrier, clocks)

@@ -853,9 +853,11 @@ extern "C" dyph_status dyph_world_autotune(dyph_world* w, int32_t frames, dyph_s
     w->f_phase = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     const uint32_t need = fused_smem_need(max_nb), floor_ = fused_smem_floor(max_nb);
+    // caps below the need down to the floor itself (the least a block can hold)
     std::vector<uint32_t> caps = {need};
-    for (uint32_t c : {96u << 10, 72u << 10, 56u << 10, 48u << 10, 40u << 10, 32u << 10})
+    for (uint32_t c : {96u << 10, 72u << 10, 56u << 10, 48u << 10, 44u << 10, 40u << 10, 32u << 10})
         if (c < need && c >= floor_) caps.push_back(c);
+    if (floor_ < need && std::find(caps.begin(), caps.end(), floor_) == caps.end()) caps.push_back(floor_);
     TunedConfig best{need, 2u, 0u, 1e30f};
     uint32_t tried = 0;
     const uint32_t cap0 = w->f_smem_cap, variant0 = w->f_variant;

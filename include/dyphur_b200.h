@@ -407,8 +407,8 @@ dyph_status dyph_world_sync_lists(dyph_world* w, dyph_stream s);
  *   register_blocks the kernel's register budget: 4, 5 or 6 resident blocks
  *                  per SM (128, 96 or 80 registers a thread; 0 = 4).
  * dyph_world_autotune times `frames` frames of each candidate (smem caps
- * 96/72/56/48/40/32 KB below the need, each team policy, each register
- * budget) from the
+ * 96/72/56/48/44/40/32 KB below the need and the floor itself, each team
+ * policy, each register budget) from the
  * world's current state, keeps the fastest, and puts the state and the
  * statistics back; the choice is cached per device and batch profile (scene
  * sizes, solver mode, iterations, substeps) for the life of the process, so
