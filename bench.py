@@ -619,6 +619,7 @@ def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask,
     from dyphur_b200 import device
     from dyphur_b200.autograd import rollout
     w = device.World(scene, mode=1)
+    tuned = w.autotune(frames)  # the fused frame's configuration (no frame changes); records use it too
     n = scene.n_bodies
     stream = torch.cuda.current_stream()
     dyn = torch.from_numpy(loss_mask.astype(np.float32)).cuda()
@@ -672,9 +673,11 @@ def adjoint_report(torch, scene, frames: int, every: int, label: str, loss_mask,
     seg = min(group, frames)
     states = 2 * (seg - 1) * 13 * n if every > 1 else 0
     act = 4 * (n_ckpt * 13 * n + states + 2 * 13 * n) + 2 * seg * set_bytes
+    reverse = w.adjoint_config()
     w.close()
     return {"workload": label, "scenes": scene.n_scenes, "bodies": n, "frames": frames,
-            "checkpoint_every": every, "solver_mode": "sequential",
+            "checkpoint_every": every, "solver_mode": "sequential", "fused_config": tuned,
+            "reverse_config": reverse,
             "fwd": {"value": n * frames / (fwd_ms / 1e3), "unit": METRIC, "ms": fwd_ms},
             "fwd_bwd": {"value": n * frames / ((fwd_ms + bwd_ms) / 1e3), "unit": METRIC, "ms": fwd_ms + bwd_ms},
             "fwd_bwd_over_fwd": (fwd_ms + bwd_ms) / fwd_ms,
