@@ -1,15 +1,16 @@
 // Adjoint of one fused frame of batched scenes (included after
 // scene_frame.cuh: by world.cu, whose scene_frame_record_kernel runs
 // record_scene, and by reverse.cu, whose scene_frame_reverse_kernel runs
-// reverse_scene), in two kernels so that frame f - 1's recomputation runs
-// while frame f's reverse pass does (they touch different buffers):
+// reverse_scene), in two kernels so that one checkpoint segment's recording
+// runs while the next one's reverse pass does (they touch different record
+// sets):
 //   record:  recompute the frame from its starting state (frame_scene with an
 //            AdjRun), recording the pose after integrate, every contact's
 //            narrowphase branch, every acting contact's pre-solve body states
 //            and the quaternions before the renormalisations — the contact
-//            set and all branches are those of the forward frame — and keep
-//            the scene's contact words (pairs, groups, geometry) in global
-//            memory;
+//            set and all branches are those of the forward frame — keep the
+//            scene's contact words (pairs, groups, geometry) in global
+//            memory, and store the frame's end state when asked;
 //   reverse: reverse the renormalisations, then the contact solves group by
 //            group in descending order (a group's contacts share no dynamic
 //            body), each with solve_contact_adj on its recorded pre-solve

@@ -601,7 +601,8 @@ dyph_status setup_reverse(dyph_world* w) {
     for (uint32_t i = 0; i < n_scenes; ++i) max_nb = std::max(max_nb, off[i + 1] - off[i]);
     // Default: a third of an SM's shared memory. The kernel's registers allow
     // two blocks per SM; the smaller blocks leave shared memory to the
-    // recording and re-stepping kernels that run beside it.
+    // recording kernel that runs beside it. At least the largest scene's
+    // bodies plus 64 contacts' words.
     uint32_t smem = w->r_smem_cap ? std::min(kMaxSmem, w->r_smem_cap & ~15u) : smem_share(reverse_kernel(), 3u);
     smem = std::max(smem, frame_body_bytes(max_nb) + kSceneWords * 4u * 64u);
     if (smem > kMaxSmem) return DYPH_ERR_TOO_LARGE;
