@@ -313,11 +313,17 @@ __device__ void scene_sweep(const Team& T, uint32_t groups, const SceneBodies& S
             const Contact ct = SC.contact(k);
             float lc = SC.lam(k);
             if (rec) {
-                // the pre-solve state is written first and marked as acted only if it did
+                // The pre-solve state of the first sweep, the one the adjoint
+                // differentiates, marked as acted only if it did. A later sweep
+                // (after a deferral) must not overwrite it: it re-solves only the
+                // deferred contacts, and one of those that acts there is
+                // reported as a path the adjoint does not cover.
                 float* r = rec->rec + rec->base + k;
                 const float lc0 = lc;
-                record_state(r, rec->stride, SB, ct.a, 0);
-                record_state(r, rec->stride, SB, ct.b, 13);
+                if (iter == 0) {
+                    record_state(r, rec->stride, SB, ct.a, 0);
+                    record_state(r, rec->stride, SB, ct.b, 13);
+                }
                 uint32_t fl = 0u;
                 if (solve_contact(SB, ct, mu, lc, dt, &fl) == kSolveDeferred) *s_flag = 1;
                 if (fl & kSfActive) {

@@ -173,3 +173,56 @@ def test_reverse_layout_does_not_change_the_gradient(dev):
     for o in out[1:]:
         for a, b in zip(o, out[0]):
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_adjoint_with_deferred_contacts_matches_fp64_dual(dev):
+    """Two push setups merged into one scene overlap: their static grounds
+    make contacts that are deferred (w_total < 1e-10) every iteration, so every
+    frame runs further sweeps in which nothing acts. The adjoint still
+    differentiates the first sweep at its own pre-solve states."""
+    import dataclasses
+
+    import torch
+    from dyphur_b200.autograd import rollout
+    s0 = scenes.push(4, seed=4)
+    o, so, b = s0.body_offset, s0.shape_offset, s0.bounds
+    bounds = np.stack([np.concatenate([b[i:i + 2, :3].min(0), b[i:i + 2, 3:].max(0)]) for i in (0, 2)])
+    s = dataclasses.replace(s0, body_offset=np.array([o[0], o[2], o[4]], np.uint32),
+                            shape_offset=np.array([so[0], so[2], so[4]], np.uint32),
+                            bounds=bounds.astype(np.float32))
+    w = dev.World(s, mode=1)
+    n = s.n_bodies
+    vel = w.initial[7:10, :n].T.clone().requires_grad_(True)
+    ang = w.initial[10:13, :n].T.clone().requires_grad_(True)
+    im = w.bodies.fbuf[13, :n].clone().requires_grad_(True)
+    box = np.zeros(n, bool)
+    for i in range(s.n_scenes):
+        box[s.body_offset[i]:s.body_offset[i] + 64] = True
+    tgt = torch.from_numpy(s.targets).cuda()
+    frames = 4
+    final = rollout(w, vel, ang, im, frames, every=2)
+    _loss(final, tgt, torch.from_numpy(box.astype(np.float32)).cuda()).backward()
+    torch.cuda.synchronize()
+    g_v, g_w, g_m = vel.grad.cpu().numpy(), ang.grad.cpu().numpy(), im.grad.cpu().numpy()
+    from oracle import oracle
+    fb = w.bodies.fbuf.cpu().numpy()
+    for i in range(s.n_scenes):
+        b0, b1 = int(s.body_offset[i]), int(s.body_offset[i + 1])
+        sh = s.shape[b0:b1]
+        mask = np.zeros(b1 - b0, np.uint8)
+        mask[:64] = 1
+        # the first setup's pusher and its 64 boxes' inverse masses (the oracle takes at most 96 parameters)
+        params = [(k, 64) for k in range(6)] + [(6, j) for j in range(64)]
+        loss, g_dual, ff, fv = oracle.dual_rollout(
+            np.ascontiguousarray(w.initial[:, b0:b1].cpu().numpy()), fb[13, b0:b1].copy(),
+            np.ascontiguousarray(fb[14:20, b0:b1]), s.shape_type[sh], np.ascontiguousarray(s.shape_half[sh].T),
+            s.flags[b0:b1], frames, s.dt, s.gravity, s.n_substeps, s.n_iters, s.friction, params,
+            s.targets[b0:b1], mask, at_float=True)
+        assert np.array_equal(final.detach().cpu().numpy()[:, b0:b1].view(np.uint32), ff.view(np.uint32)), i
+        p = b0 + 64
+        g_gpu = [g_v[p, 0], g_v[p, 1], g_v[p, 2], g_w[p, 0], g_w[p, 1], g_w[p, 2]]
+        g_gpu += [g_m[b0 + j] for k, j in params[6:]]
+        g_gpu = np.array(g_gpu, np.float64)
+        rel = np.linalg.norm(g_gpu - g_dual) / np.linalg.norm(g_dual)
+        print(f"\nmerged scene {i}, {frames} frames: |g| {np.linalg.norm(g_dual):.4g}, relative error {rel:.2e}")
+        assert rel <= 1e-3, (i, rel)
